@@ -1,0 +1,306 @@
+"""B200-native e-means engine: host-side mirror of the crate `emeans` API.
+
+The reference crate (andrewluetgers/e-means) exposes `Config`, `train`,
+`assign`, `resolve_recipe` and the `Assigner` / `AssignRows<T>` traits
+(src/lib.rs:75-163, 201-225, 348-520). This package offers the same names over
+the C ABI of libemb200.so (include/emb200.h), whose CUDA kernels do all of the
+work on one B200. There is no CPU fallback: without the built library or a
+B200 every call raises.
+"""
+import ctypes
+import enum
+import os
+import subprocess
+from dataclasses import dataclass, field
+from typing import List, Optional
+
+import numpy as np
+
+from . import datasets  # noqa: F401
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libemb200.so")
+
+EMB200_F32, EMB200_I8, EMB200_U8 = 0, 1, 2
+PREC_FP32, PREC_BF16, PREC_BF16X1 = 0, 1, 2
+CENTROIDS_F32, CENTROIDS_I8 = 0, 8
+MATCH = {"avx512": 0, "avx2": 1, "portable": 2}
+_DTYPES = {np.dtype(np.float32): EMB200_F32, np.dtype(np.int8): EMB200_I8, np.dtype(np.uint8): EMB200_U8}
+PRECISIONS = {"fp32": PREC_FP32, "bf16": PREC_BF16, "bf16x1": PREC_BF16X1}
+
+
+class EngineError(RuntimeError):
+    """A non-zero status from libemb200 (the reference returns Err or panics)."""
+
+
+class _Opts(ctypes.Structure):
+    _fields_ = [("precision", ctypes.c_int), ("centroid_bits", ctypes.c_int), ("match_kernel", ctypes.c_int),
+                ("reserved", ctypes.c_int * 5)]
+
+
+class _Config(ctypes.Structure):
+    _fields_ = [("nepochs", ctypes.c_double), ("batch_law", ctypes.c_int), ("batch_size", ctypes.c_uint64),
+                ("alpha0", ctypes.c_double), ("unused_threshold", ctypes.c_float), ("balance", ctypes.c_float),
+                ("seed", ctypes.c_uint64), ("verbose", ctypes.c_int), ("closing_f64", ctypes.c_int)]
+
+
+class _Recipe(ctypes.Structure):
+    _fields_ = [("batch_size", ctypes.c_uint64), ("alpha0", ctypes.c_double), ("n_epochs", ctypes.c_uint64),
+                ("total_steps", ctypes.c_uint64), ("unused_threshold", ctypes.c_float)]
+
+
+class _Stats(ctypes.Structure):
+    _fields_ = [("rows", ctypes.c_uint64), ("rows_certified", ctypes.c_uint64), ("rows_researched", ctypes.c_uint64),
+                ("kernel_launches", ctypes.c_uint64), ("ms_total", ctypes.c_double)]
+
+
+def build(force=False):
+    """Compile libemb200.so in-tree with nvcc for sm_100a."""
+    args = ["make", "-s", "-C", _HERE] + (["-B"] if force else [])
+    subprocess.run(args, check=True)
+
+
+_lib = None
+
+
+def lib():
+    """Load libemb200.so; raises if it is missing (no CPU fallback exists)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise EngineError(f"{LIB_PATH} is not built: run emeans_b200.build() (nvcc, sm_100a)")
+    L = ctypes.CDLL(LIB_PATH)
+    P, S, I = ctypes.c_void_p, ctypes.c_size_t, ctypes.c_int
+    L.emb200_create.argtypes = [I, ctypes.POINTER(_Opts), ctypes.POINTER(P)]
+    L.emb200_destroy.argtypes = [P]
+    L.emb200_last_error.restype = ctypes.c_char_p
+    L.emb200_last_error.argtypes = [P]
+    L.emb200_name.argtypes = [P, ctypes.c_char_p, S]
+    L.emb200_set_opts.argtypes = [P, ctypes.POINTER(_Opts)]
+    L.emb200_get_stats.argtypes = [P, ctypes.POINTER(_Stats)]
+    L.emb200_set_centroids.argtypes = [P, P, S, S]
+    L.emb200_set_bias.argtypes = [P, P, S]
+    for nm in ("emb200_assign_f32", "emb200_assign_i8", "emb200_assign_u8"):
+        getattr(L, nm).argtypes = [P, P, S, P, P]
+    L.emb200_assign_device.argtypes = [P, I, P, S, P, P, P]
+    L.emb200_load_rows.argtypes = [P, I, P, S, S]
+    L.emb200_assign_resident.argtypes = [P, P, P]
+    L.emb200_resolve_recipe.argtypes = [S, S, S, ctypes.POINTER(_Config), ctypes.POINTER(_Recipe), P, S]
+    L.emb200_scheduled_alpha.restype = ctypes.c_double
+    L.emb200_scheduled_alpha.argtypes = [ctypes.c_double, S, S]
+    L.emb200_train.argtypes = [P, ctypes.POINTER(_Config), S, P, P, P, P, ctypes.POINTER(_Recipe)]
+    _lib = L
+    return L
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(ctypes.c_void_p)
+
+
+class BatchLaw(enum.IntEnum):
+    """src/lib.rs:93-101."""
+
+    AUTO = 0
+    THROUGHPUT = 1
+    QUALITY = 2
+
+
+@dataclass
+class Config:
+    """src/lib.rs:103-139 (same fields and defaults)."""
+
+    nepochs: float = 5.0
+    batch_law: BatchLaw = BatchLaw.AUTO
+    batch_size: Optional[int] = None
+    alpha0: Optional[float] = None
+    unused_threshold: Optional[float] = None
+    balance: float = 0.0
+    seed: int = 1234
+    verbose: bool = False
+    closing_f64: bool = False  # FP64 last-pass sums instead of the reference's f32
+
+    def _c(self):
+        return _Config(self.nepochs, int(self.batch_law), self.batch_size or 0,
+                       self.alpha0 if self.alpha0 is not None else -1.0,
+                       self.unused_threshold if self.unused_threshold is not None else -1.0, self.balance, self.seed,
+                       int(self.verbose), int(self.closing_f64))
+
+
+@dataclass
+class Recipe:
+    """src/lib.rs:141-149."""
+
+    batch_size: int
+    alpha0: float
+    epoch_rows: List[int]
+    total_steps: int
+    unused_threshold: float
+
+
+@dataclass
+class Output:
+    """src/lib.rs:151-163."""
+
+    centroids: np.ndarray
+    labels: np.ndarray
+    objective: np.ndarray
+    n_splits: int
+    recipe: Recipe
+    stats: dict = field(default_factory=dict)
+
+
+def resolve_recipe(n, d, k, cfg: Optional[Config] = None) -> Recipe:
+    """resolve_recipe (src/lib.rs:201-225), computed by libemb200's host code."""
+    cfg = cfg or Config()
+    c = cfg._c()
+    r = _Recipe()
+    er = np.zeros(int(np.floor(cfg.nepochs)) + 2, np.uint64)
+    lib().emb200_resolve_recipe(n, d, k, ctypes.byref(c), ctypes.byref(r), _p(er), er.size)
+    return Recipe(int(r.batch_size), float(r.alpha0), [int(v) for v in er[:r.n_epochs]], int(r.total_steps),
+                  float(r.unused_threshold))
+
+
+def scheduled_alpha(alpha0, step, total):
+    """src/lib.rs:194-198."""
+    return lib().emb200_scheduled_alpha(alpha0, step, total)
+
+
+def balance_stats(labels, k):
+    """balance_stats (src/lib.rs:497-504): (imbalance factor, largest/mean size, empty clusters)."""
+    counts = np.bincount(np.asarray(labels, np.int64), minlength=k).astype(np.uint64)
+    n = float(len(labels))
+    squares = float((counts * counts).astype(np.float64).sum())
+    return k * squares / (n * n), float(counts.max()) * k / n, int((counts == 0).sum())
+
+
+class B200Assigner:
+    """Drop-in for the `Assigner` + `AssignRows<T>` traits (src/lib.rs:75-91),
+    beside CpuAssigner (src/cpu.rs) and CpuI8Assigner (src/cpu_i8.rs).
+
+    precision: "fp32" (SIMT), "bf16" (tcgen05, three-term split), "bf16x1".
+    centroid_bits: 0 (CpuAssigner semantics for every row type) or 8
+    (CpuI8Assigner(I8) semantics for i8 rows). match: which CpuAssigner SIMD
+    kernel's rounding the labels and distances reproduce.
+    """
+
+    def __init__(self, ordinal=0, precision="fp32", centroid_bits=0, match="avx512"):
+        self._h = ctypes.c_void_p()
+        self._opts = _Opts(PRECISIONS[precision], centroid_bits, MATCH[match])
+        rc = lib().emb200_create(ordinal, ctypes.byref(self._opts), ctypes.byref(self._h))
+        if rc != 0:
+            raise EngineError(f"emb200_create failed ({rc}): no usable B200 (sm_100) device")
+        self.k = 0
+        self.d = 0
+
+    def _check(self, rc):
+        if rc != 0:
+            raise EngineError(lib().emb200_last_error(self._h).decode())
+
+    def close(self):
+        if self._h:
+            lib().emb200_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_options(self, precision=None, centroid_bits=None, match=None):
+        if precision is not None:
+            self._opts.precision = PRECISIONS[precision]
+        if centroid_bits is not None:
+            self._opts.centroid_bits = centroid_bits
+        if match is not None:
+            self._opts.match_kernel = MATCH[match]
+        self._check(lib().emb200_set_opts(self._h, ctypes.byref(self._opts)))
+
+    def name(self):
+        buf = ctypes.create_string_buffer(256)
+        self._check(lib().emb200_name(self._h, buf, 256))
+        return buf.value.decode()
+
+    def set_centroids(self, centroids, k=None, d=None):
+        c = np.ascontiguousarray(centroids, np.float32)
+        if k is None:
+            k, d = c.shape
+        if c.size != k * d:
+            raise ValueError("centroids must be k x d")
+        self._check(lib().emb200_set_centroids(self._h, _p(c), k, d))
+        self.k, self.d = k, d
+
+    def set_bias(self, bias):
+        b = np.ascontiguousarray(bias, np.float32)
+        self._check(lib().emb200_set_bias(self._h, _p(b), b.size))
+
+    def assign(self, x, labels=None, dist=None):
+        """AssignRows::assign: rows (m x d, f32/i8/u8) -> (labels u32, dist f32)."""
+        x = np.ascontiguousarray(x)
+        if x.dtype not in _DTYPES:
+            raise TypeError(f"rows must be float32, int8 or uint8, got {x.dtype}")
+        m = x.size // max(self.d, 1)
+        labels = np.empty(m, np.uint32) if labels is None else labels
+        dist = np.empty(m, np.float32) if dist is None else dist
+        fn = {EMB200_F32: lib().emb200_assign_f32, EMB200_I8: lib().emb200_assign_i8,
+              EMB200_U8: lib().emb200_assign_u8}[_DTYPES[x.dtype]]
+        self._check(fn(self._h, _p(x), m, _p(labels), _p(dist)))
+        return labels, dist
+
+    def assign_device(self, x_ptr, dtype, m, labels_ptr, dist_ptr, stream=None):
+        """Device-pointer assign (torch tensors' data_ptr()), enqueued on `stream`."""
+        self._check(lib().emb200_assign_device(self._h, dtype, ctypes.c_void_p(x_ptr), m, ctypes.c_void_p(labels_ptr),
+                                               ctypes.c_void_p(dist_ptr), ctypes.c_void_p(stream or 0)))
+
+    def load_rows(self, x):
+        """Upload rows once; they stay resident in HBM for assign_resident / train."""
+        x = np.ascontiguousarray(x)
+        n, d = x.shape
+        self._check(lib().emb200_load_rows(self._h, _DTYPES[x.dtype], _p(x), n, d))
+        self.rows_shape = (n, d)
+
+    def assign_resident(self, want_host=True):
+        n = self.rows_shape[0]
+        labels = np.empty(n, np.uint32) if want_host else None
+        dist = np.empty(n, np.float32) if want_host else None
+        self._check(lib().emb200_assign_resident(self._h, _p(labels), _p(dist)))
+        return labels, dist
+
+    def stats(self):
+        s = _Stats()
+        self._check(lib().emb200_get_stats(self._h, ctypes.byref(s)))
+        return {f: getattr(s, f) for f, _ in _Stats._fields_}
+
+    def train_resident(self, k, cfg: Optional[Config] = None) -> Output:
+        """train (src/lib.rs:348-491) on the resident rows, entirely on the device."""
+        cfg = cfg or Config()
+        n, d = self.rows_shape
+        c = cfg._c()
+        rec = resolve_recipe(n, d, k, cfg)
+        cent = np.empty((k, d), np.float32)
+        labels = np.empty(n, np.uint32)
+        obj = np.empty(len(rec.epoch_rows), np.float64)
+        ns = np.zeros(1, np.uint64)
+        r = _Recipe()
+        self._check(lib().emb200_train(self._h, ctypes.byref(c), k, _p(cent), _p(labels), _p(obj), _p(ns),
+                                       ctypes.byref(r)))
+        self.k, self.d = k, d
+        return Output(cent, labels, obj, int(ns[0]), rec, self.stats())
+
+
+def train(x, d, k, cfg: Optional[Config] = None, assigner: Optional[B200Assigner] = None) -> Output:
+    """train (src/lib.rs:348-491): rows uploaded once, the whole loop on the B200."""
+    x = np.ascontiguousarray(x)
+    x = x.reshape(-1, d)
+    a = assigner or B200Assigner()
+    a.load_rows(x)
+    return a.train_resident(k, cfg)
+
+
+def assign(x, centroids, d, assigner: B200Assigner):
+    """assign (src/lib.rs:512-520): exact labels and squared distances."""
+    x = np.ascontiguousarray(x).reshape(-1, d)
+    c = np.ascontiguousarray(centroids, np.float32).reshape(-1, d)
+    assigner.set_centroids(c)
+    return assigner.assign(x)

@@ -1,0 +1,534 @@
+// libemb200: C ABI (include/emb200.h) and host orchestration of the B200
+// e-means engine. Every computation runs in the CUDA kernels included below;
+// host code only sizes buffers, launches and copies.
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/emb200.h"
+#include "common.cuh"
+#include "host_recipe.hpp"
+#include "kernels_exact.cuh"
+#include "kernels_i8.cuh"
+#include "kernels_simt.cuh"
+#include "kernels_tc.cuh"
+#include "kernels_update.cuh"
+
+using namespace emb;
+
+namespace {
+
+// Device buffer owned by a handle.
+template <typename T>
+struct DevBuf {
+    T* p = nullptr;
+    size_t n = 0;
+    cudaError_t ensure(size_t want) {
+        if (want <= n && p) return cudaSuccess;
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+        cudaError_t e = cudaMalloc((void**)&p, std::max(want, (size_t)1) * sizeof(T));
+        if (e == cudaSuccess) n = std::max(want, (size_t)1);
+        return e;
+    }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+};
+
+// Device state of a training run (filled by emb200_train).
+struct TrainState {
+    DevBuf<float> usage, sums;
+    DevBuf<uint32_t> counts, labels_all, order, batch_labels;
+    DevBuf<float> batch_dist;
+    void release() {
+        usage.release(); sums.release(); counts.release(); labels_all.release(); order.release();
+        batch_labels.release(); batch_dist.release();
+    }
+};
+
+}  // namespace
+
+struct emb200_handle {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    emb200_opts opts{};
+    std::string err;
+    emb200_stats stats{};
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    int sm_count = 148;
+
+    // centroids
+    size_t k = 0, d = 0;
+    bool have_centroids = false;
+    DevBuf<float> c, norms, bias;
+    DevBuf<Bounds> bounds;
+    DevBuf<__nv_bfloat16> c_hi, c_lo;  // K-major BF16 split, row stride kpad
+    size_t kpad = 0;
+    DevBuf<int8_t> c8;   // I8 centroids (CpuI8Assigner)
+    DevBuf<long long> off8;  // I8 offsets: sum c8^2 (+ bias)
+    bool bias_set = false;
+
+    // resident rows
+    DevBuf<uint8_t> rows;
+    int rows_dtype = -1;
+    size_t rows_n = 0, rows_d = 0;
+    DevBuf<uint32_t> res_labels;
+    DevBuf<float> res_dist;
+
+    // scratch for assign
+    DevBuf<uint8_t> stage;  // host-path staging of rows
+    DevBuf<uint32_t> st_labels;
+    DevBuf<float> st_dist;
+    DevBuf<float> part_s;
+    DevBuf<uint32_t> part_i;
+    DevBuf<uint32_t> redo_rows;
+    DevBuf<uint32_t> counters;  // [0] redo count, [1] certified count
+
+    // training state
+    TrainState train;
+};
+
+namespace {
+
+int fail(emb200_handle* h, int code, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    if (h) h->err = buf;
+    return code;
+}
+
+#define CK(call)                                                                                      \
+    do {                                                                                              \
+        cudaError_t e_ = (call);                                                                      \
+        if (e_ != cudaSuccess) return fail(h, e_ == cudaErrorMemoryAllocation ? EMB200_ENOMEM : EMB200_ECUDA, \
+                                           "%s: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__); \
+    } while (0)
+
+#define CKL()                                                                                         \
+    do {                                                                                              \
+        h->stats.kernel_launches++;                                                                   \
+        cudaError_t e_ = cudaGetLastError();                                                          \
+        if (e_ != cudaSuccess) return fail(h, EMB200_ECUDA, "kernel launch: %s (%s:%d)", cudaGetErrorString(e_), \
+                                           __FILE__, __LINE__);                                       \
+    } while (0)
+
+size_t elt_size(int dtype) { return dtype == EMB200_F32 ? 4 : 1; }
+
+// Error-bound coefficients of the certification, E = ka |x| cmax + kb nmax
+// (see k_certify). u = 2^-24 (f32 rounding), ub = 2^-9 (bf16 rounding); the
+// tensor-core accumulation is allowed one f32 truncation (2u) per product term.
+void bound_coefficients(int precision, int dtype, size_t d, float* ka, float* kb) {
+    const double u = std::ldexp(1.0, -24), ub = std::ldexp(1.0, -9);
+    auto gamma = [](double n, double unit) { return n * unit / (1.0 - n * unit); };
+    double g_ref = gamma((double)d + 2, u);  // reference dot vs exact
+    double a;
+    if (precision == EMB200_PREC_FP32) {
+        a = 2.0 * (gamma((double)d + 2, u) + g_ref) + 4.02 * u;
+    } else if (precision == EMB200_PREC_BF16) {
+        double terms = dtype == EMB200_F32 ? 3.0 : 2.0;
+        double rep = dtype == EMB200_F32 ? 3.2 * ub * ub : 1.1 * ub * ub;  // dropped split terms
+        a = 2.0 * (rep + 1.02 * gamma(terms * (double)d + 2, 2 * u) + g_ref) + 4.02 * u;
+    } else {
+        double rep = dtype == EMB200_F32 ? 2.0 * ub + ub * ub : ub;
+        a = 2.0 * (rep + 1.02 * gamma((double)d + 2, 2 * u) + g_ref) + 4.02 * u;
+    }
+    *ka = (float)(1.25 * a);
+    *kb = (float)(1.25 * 2.0 * u);
+}
+
+bool use_i8_mode(const emb200_handle* h, int dtype) {
+    return dtype == EMB200_I8 && h->opts.centroid_bits == EMB200_CENTROIDS_I8;
+}
+
+
+// set_centroids on the device: reference norms, certification bounds, and the
+// forms the selected search needs (BF16 split for tcgen05, i8 for I8 mode).
+int prepare_centroids(emb200_handle* h) {
+    cudaStream_t st = h->stream;
+    const int k = (int)h->k, d = (int)h->d;
+    CK(cudaMemsetAsync(h->bounds.p, 0, sizeof(Bounds), st));
+    __nv_bfloat16 *hi = nullptr, *lo = nullptr;
+    if (h->opts.precision != EMB200_PREC_FP32) {
+        h->kpad = (h->d + 63) / 64 * 64;
+        if (h->c_hi.ensure((size_t)k * h->kpad) || h->c_lo.ensure((size_t)k * h->kpad))
+            return fail(h, EMB200_ENOMEM, "BF16 centroid allocation failed");
+        hi = h->c_hi.p;
+        lo = h->c_lo.p;
+    } else {
+        h->kpad = (h->d + 63) / 64 * 64;
+    }
+    k_prep_centroids<<<(unsigned)((k + 7) / 8), 256, 0, st>>>(h->c.p, k, d, h->norms.p, h->bounds.p, hi, lo,
+                                                              (int)h->kpad);
+    CKL();
+    if (h->opts.centroid_bits == EMB200_CENTROIDS_I8) {
+        size_t kp = (h->d + 31) / 32 * 32;
+        if (h->c8.ensure((size_t)k * kp) || h->off8.ensure(k)) return fail(h, EMB200_ENOMEM, "i8 centroid allocation failed");
+        k_prep_i8<<<(unsigned)((k + 7) / 8), 256, 0, st>>>(h->c.p, k, d, (int)kp, h->c8.p, h->off8.p);
+        CKL();
+    }
+    h->bias_set = false;
+    return EMB200_OK;
+}
+
+// set_bias on the device (bias already in device memory).
+int apply_bias(emb200_handle* h, const float* bias_dev) {
+    cudaStream_t st = h->stream;
+    const int k = (int)h->k;
+    k_add_bias<<<(unsigned)((k + 255) / 256), 256, 0, st>>>(h->norms.p, bias_dev, k, h->bounds.p);
+    CKL();
+    if (h->opts.centroid_bits == EMB200_CENTROIDS_I8) {
+        k_bias_i8<<<(unsigned)((k + 255) / 256), 256, 0, st>>>(h->off8.p, bias_dev, k);
+        CKL();
+    }
+    h->bias_set = true;
+    return EMB200_OK;
+}
+
+// CpuI8Assigner(I8) semantics: exact integer search, no certification needed.
+int launch_i8_assign(emb200_handle* h, const int8_t* x, const uint32_t* gather, size_t m, uint32_t* labels,
+                     float* dist, cudaStream_t st) {
+    const int k = (int)h->k, d = (int)h->d;
+    int row_tiles = (int)((m + kI8BM - 1) / kI8BM);
+    int ntiles = (k + kI8BN - 1) / kI8BN;
+    int nsplit = 1, target = 2 * h->sm_count;
+    if (row_tiles < target) nsplit = std::min(ntiles, (target + row_tiles - 1) / row_tiles);
+    // part_s holds int64 scores here: 2 floats per entry.
+    if (h->part_s.ensure((size_t)nsplit * m * 2) || h->part_i.ensure((size_t)nsplit * m))
+        return fail(h, EMB200_ENOMEM, "scratch allocation failed for %zu rows", m);
+    size_t kp = (h->d + 31) / 32 * 32;
+    int xvec = (d % 16 == 0) ? 1 : 0;
+    dim3 grid(row_tiles, nsplit);
+    k_assign_i8<<<grid, 256, 0, st>>>(x, gather, (int)m, d, h->c8.p, (int)kp, h->off8.p, k,
+                                      (long long*)h->part_s.p, h->part_i.p, xvec);
+    CKL();
+    k_finish_i8<<<(unsigned)((m + 255) / 256), 256, 0, st>>>(x, gather, (int)m, d, (const long long*)h->part_s.p,
+                                                             h->part_i.p, nsplit, labels, dist);
+    CKL();
+    return EMB200_OK;
+}
+
+bool tc_supported(const emb200_handle* h, int dtype) {
+    (void)h; (void)dtype;
+    return false;
+}
+int tc_nsplit(const emb200_handle* h, size_t m) {
+    (void)h; (void)m;
+    return 1;
+}
+template <typename T>
+int launch_tc_assign(emb200_handle* h, const T* x, const uint32_t* gather, size_t m, int nsplit, cudaStream_t st) {
+    (void)x; (void)gather; (void)m; (void)nsplit; (void)st;
+    return fail(h, EMB200_ESTATE, "tensor-core path not available");
+}
+
+// Full pipeline of one assign over m rows already on the device (x_dev, or
+// gathered through `gather`), results to device labels/dist.
+template <typename T>
+int assign_rows_dev(emb200_handle* h, const T* x, const uint32_t* gather, size_t m, uint32_t* labels, float* dist,
+                    cudaStream_t st) {
+    const int dtype = std::is_same<T, float>::value ? EMB200_F32 : (std::is_same<T, int8_t>::value ? EMB200_I8 : EMB200_U8);
+    const int k = (int)h->k, d = (int)h->d;
+    if (m == 0) return EMB200_OK;
+    if (use_i8_mode(h, dtype)) {
+        return launch_i8_assign(h, (const int8_t*)x, gather, m, labels, dist, st);
+    }
+    int prec = h->opts.precision;
+    int row_tiles = (int)((m + kSimtBM - 1) / kSimtBM);
+    int ntiles = (k + kSimtBN - 1) / kSimtBN;
+    int nsplit = 1;
+    bool tc = prec != EMB200_PREC_FP32 && tc_supported(h, dtype);
+    if (tc) {
+        nsplit = tc_nsplit(h, m);
+    } else {
+        int target = 2 * h->sm_count;
+        if (row_tiles < target) nsplit = std::min(ntiles, (target + row_tiles - 1) / row_tiles);
+    }
+    size_t mm = m;
+    if (h->part_s.ensure((size_t)nsplit * mm * 2) || h->part_i.ensure((size_t)nsplit * mm * 2) ||
+        h->redo_rows.ensure(mm) || h->counters.ensure(4))
+        return fail(h, EMB200_ENOMEM, "scratch allocation failed for %zu rows", m);
+    CK(cudaMemsetAsync(h->counters.p, 0, 4 * sizeof(uint32_t), st));
+    if (tc) {
+        int rc = launch_tc_assign(h, x, gather, m, nsplit, st);
+        if (rc) return rc;
+    } else {
+        dim3 grid(row_tiles, nsplit);
+        int vec4 = (d % 4 == 0) ? 1 : 0;
+        k_assign_simt<T><<<grid, kSimtThreads, 0, st>>>(x, gather, (int)m, d, h->c.p, h->norms.p, k, h->part_s.p,
+                                                         h->part_i.p, vec4);
+        CKL();
+    }
+    float ka, kb;
+    bound_coefficients(tc ? prec : EMB200_PREC_FP32, dtype, h->d, &ka, &kb);
+    int match = h->opts.match_kernel;
+    k_certify<T><<<(unsigned)((m + 7) / 8), 256, 0, st>>>(x, gather, (int)m, d, h->c.p, h->norms.p, k, h->part_s.p,
+                                                           h->part_i.p, nsplit, h->bounds.p, ka, kb, match, labels,
+                                                           dist, h->redo_rows.p, h->counters.p, h->counters.p + 1);
+    CKL();
+    k_research<T><<<h->sm_count * 4, 256, 0, st>>>(x, gather, d, h->c.p, h->norms.p, k, match, h->redo_rows.p,
+                                                    h->counters.p, labels, dist);
+    CKL();
+    return EMB200_OK;
+}
+
+int assign_dispatch(emb200_handle* h, int dtype, const void* x, const uint32_t* gather, size_t m, uint32_t* labels,
+                    float* dist, cudaStream_t st) {
+    switch (dtype) {
+        case EMB200_F32: return assign_rows_dev(h, (const float*)x, gather, m, labels, dist, st);
+        case EMB200_I8: return assign_rows_dev(h, (const int8_t*)x, gather, m, labels, dist, st);
+        case EMB200_U8: return assign_rows_dev(h, (const uint8_t*)x, gather, m, labels, dist, st);
+    }
+    return fail(h, EMB200_EINVAL, "unknown dtype %d", dtype);
+}
+
+int check_ready(emb200_handle* h, int dtype) {
+    if (!h) return EMB200_EINVAL;
+    if (!h->have_centroids) return fail(h, EMB200_ESTATE, "set_centroids must be called first");
+    if (dtype < 0 || dtype > 2) return fail(h, EMB200_EINVAL, "unknown dtype %d", dtype);
+    if (use_i8_mode(h, dtype) && h->d > 32768)
+        return fail(h, EMB200_EINVAL, "integer assignment supports d <= 32768");
+    return EMB200_OK;
+}
+
+// Host-memory assign (the trait call): chunks of rows are copied in, searched
+// and copied out.
+int assign_host(emb200_handle* h, int dtype, const void* x, size_t m, uint32_t* labels, float* dist) {
+    int rc = check_ready(h, dtype);
+    if (rc) return rc;
+    if (m && (!x || !labels || !dist)) return fail(h, EMB200_EINVAL, "null buffer");
+    if (m > 0xFFFFFFFFull) return fail(h, EMB200_EINVAL, "more than 2^32 - 1 rows in one call");
+    h->stats = emb200_stats{};
+    cudaStream_t st = h->stream;
+    CK(cudaEventRecord(h->ev0, st));
+    const size_t esz = elt_size(dtype);
+    const size_t chunk = std::min(m, (size_t)1 << 20);
+    if (h->stage.ensure(chunk * h->d * esz) || h->st_labels.ensure(chunk) || h->st_dist.ensure(chunk))
+        return fail(h, EMB200_ENOMEM, "staging allocation failed");
+    uint32_t cert = 0, redo = 0;
+    for (size_t r0 = 0; r0 < m; r0 += chunk) {
+        size_t mc = std::min(chunk, m - r0);
+        CK(cudaMemcpyAsync(h->stage.p, (const uint8_t*)x + r0 * h->d * esz, mc * h->d * esz, cudaMemcpyHostToDevice, st));
+        rc = assign_dispatch(h, dtype, h->stage.p, nullptr, mc, h->st_labels.p, h->st_dist.p, st);
+        if (rc) return rc;
+        CK(cudaMemcpyAsync(labels + r0, h->st_labels.p, mc * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(dist + r0, h->st_dist.p, mc * sizeof(float), cudaMemcpyDeviceToHost, st));
+        uint32_t cnt[2] = {0, 0};
+        if (!use_i8_mode(h, dtype)) CK(cudaMemcpyAsync(cnt, h->counters.p, sizeof cnt, cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        redo += cnt[0];
+        cert += cnt[1];
+    }
+    CK(cudaEventRecord(h->ev1, st));
+    CK(cudaEventSynchronize(h->ev1));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, h->ev0, h->ev1);
+    h->stats.rows = m;
+    h->stats.rows_certified = use_i8_mode(h, dtype) ? m : cert;
+    h->stats.rows_researched = redo;
+    h->stats.ms_total = ms;
+    return EMB200_OK;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+extern "C" {
+
+int emb200_create(int ordinal, const emb200_opts* opts, emb200_handle** out) {
+    if (!out) return EMB200_EINVAL;
+    *out = nullptr;
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) return EMB200_EDEVICE;
+    if (ordinal < 0 || ordinal >= n) return EMB200_EINVAL;
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, ordinal) != cudaSuccess) return EMB200_EDEVICE;
+    if (prop.major != 10) return EMB200_EDEVICE;  // built for sm_100a only
+    emb200_handle* h = new emb200_handle();
+    h->device = ordinal;
+    h->sm_count = prop.multiProcessorCount;
+    if (opts) h->opts = *opts;
+    if (cudaSetDevice(ordinal) != cudaSuccess || cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) ||
+        cudaEventCreate(&h->ev0) || cudaEventCreate(&h->ev1) || h->bounds.ensure(1)) {
+        delete h;
+        return EMB200_ECUDA;
+    }
+    *out = h;
+    return EMB200_OK;
+}
+
+int emb200_destroy(emb200_handle* h) {
+    if (!h) return EMB200_OK;
+    cudaSetDevice(h->device);
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    h->c.release(); h->norms.release(); h->bias.release(); h->bounds.release();
+    h->c_hi.release(); h->c_lo.release(); h->c8.release(); h->off8.release();
+    h->rows.release(); h->res_labels.release(); h->res_dist.release();
+    h->stage.release(); h->st_labels.release(); h->st_dist.release();
+    h->part_s.release(); h->part_i.release(); h->redo_rows.release(); h->counters.release();
+    h->train.release();
+    if (h->ev0) cudaEventDestroy(h->ev0);
+    if (h->ev1) cudaEventDestroy(h->ev1);
+    if (h->stream) cudaStreamDestroy(h->stream);
+    delete h;
+    return EMB200_OK;
+}
+
+const char* emb200_last_error(const emb200_handle* h) {
+    if (!h) return "null handle";
+    return h->err.c_str();
+}
+
+int emb200_set_opts(emb200_handle* h, const emb200_opts* opts) {
+    if (!h || !opts) return EMB200_EINVAL;
+    if (opts->precision < 0 || opts->precision > 2 || opts->match_kernel < 0 || opts->match_kernel > 2 ||
+        (opts->centroid_bits != 0 && opts->centroid_bits != 8))
+        return fail(h, EMB200_EINVAL, "invalid options");
+    bool rebuild = h->opts.centroid_bits != opts->centroid_bits || h->opts.precision != opts->precision;
+    h->opts = *opts;
+    if (rebuild && h->have_centroids) h->have_centroids = false;  // centroid forms depend on the options
+    return EMB200_OK;
+}
+
+int emb200_get_stats(const emb200_handle* h, emb200_stats* out) {
+    if (!h || !out) return EMB200_EINVAL;
+    *out = h->stats;
+    return EMB200_OK;
+}
+
+int emb200_name(emb200_handle* h, char* buf, size_t len) {
+    if (!h || !buf || len == 0) return EMB200_EINVAL;
+    cudaDeviceProp prop;
+    cudaGetDeviceProperties(&prop, h->device);
+    const char* prec = h->opts.precision == EMB200_PREC_FP32 ? "FP32 SIMT"
+                       : h->opts.precision == EMB200_PREC_BF16 ? "BF16x3 tcgen05" : "BF16 tcgen05";
+    const char* match = h->opts.match_kernel == 0 ? "AVX-512" : h->opts.match_kernel == 1 ? "AVX2" : "portable";
+    snprintf(buf, len, "B200 fused assign (%s search, exact re-score in %s rounding%s), %s", prec, match,
+             h->opts.centroid_bits == 8 ? ", int8 centroids for i8 rows" : "", prop.name);
+    return EMB200_OK;
+}
+
+int emb200_set_centroids(emb200_handle* h, const float* centroids, size_t k, size_t d) {
+    if (!h) return EMB200_EINVAL;
+    if (!centroids || k == 0 || d == 0) return fail(h, EMB200_EINVAL, "centroids must be a non-empty k x d array");
+    if (k > 0x7FFFFFFF || d > 0x7FFFFFFF) return fail(h, EMB200_EINVAL, "k and d must fit in 31 bits");
+    CK(cudaSetDevice(h->device));
+    if (h->c.ensure(k * d) || h->norms.ensure(k) || h->bias.ensure(k))
+        return fail(h, EMB200_ENOMEM, "centroid allocation failed");
+    h->k = k;
+    h->d = d;
+    CK(cudaMemcpyAsync(h->c.p, centroids, k * d * sizeof(float), cudaMemcpyHostToDevice, h->stream));
+    int rc = prepare_centroids(h);
+    if (rc) return rc;
+    CK(cudaStreamSynchronize(h->stream));
+    h->have_centroids = true;
+    return EMB200_OK;
+}
+
+int emb200_set_bias(emb200_handle* h, const float* bias, size_t k) {
+    if (!h) return EMB200_EINVAL;
+    if (!h->have_centroids) return fail(h, EMB200_ESTATE, "set_centroids must be called first");
+    if (!bias || k != h->k) return fail(h, EMB200_EINVAL, "bias must have k = %zu entries", h->k);
+    CK(cudaMemcpyAsync(h->bias.p, bias, k * sizeof(float), cudaMemcpyHostToDevice, h->stream));
+    int rc = apply_bias(h, h->bias.p);
+    if (rc) return rc;
+    CK(cudaStreamSynchronize(h->stream));
+    return EMB200_OK;
+}
+
+int emb200_assign_f32(emb200_handle* h, const float* x, size_t m, uint32_t* labels, float* dist) {
+    return assign_host(h, EMB200_F32, x, m, labels, dist);
+}
+int emb200_assign_i8(emb200_handle* h, const int8_t* x, size_t m, uint32_t* labels, float* dist) {
+    return assign_host(h, EMB200_I8, x, m, labels, dist);
+}
+int emb200_assign_u8(emb200_handle* h, const uint8_t* x, size_t m, uint32_t* labels, float* dist) {
+    return assign_host(h, EMB200_U8, x, m, labels, dist);
+}
+
+int emb200_assign_device(emb200_handle* h, int dtype, const void* x_dev, size_t m, uint32_t* labels_dev,
+                         float* dist_dev, void* stream) {
+    int rc = check_ready(h, dtype);
+    if (rc) return rc;
+    if (m > 0xFFFFFFFFull) return fail(h, EMB200_EINVAL, "more than 2^32 - 1 rows in one call");
+    if (m && (!x_dev || !labels_dev || !dist_dev)) return fail(h, EMB200_EINVAL, "null buffer");
+    cudaStream_t st = stream ? (cudaStream_t)stream : h->stream;
+    return assign_dispatch(h, dtype, x_dev, nullptr, m, labels_dev, dist_dev, st);
+}
+
+int emb200_load_rows(emb200_handle* h, int dtype, const void* x, size_t n, size_t d) {
+    if (!h) return EMB200_EINVAL;
+    if (dtype < 0 || dtype > 2) return fail(h, EMB200_EINVAL, "unknown dtype %d", dtype);
+    if (!x || n == 0 || d == 0) return fail(h, EMB200_EINVAL, "x must be a non-empty row-major n x d array");
+    if (n > 0xFFFFFFFFull) return fail(h, EMB200_EINVAL, "more than 2^32 - 1 rows: subsample or shard the input");
+    CK(cudaSetDevice(h->device));
+    size_t bytes = n * d * elt_size(dtype);
+    if (h->rows.ensure(bytes)) return fail(h, EMB200_ENOMEM, "cannot hold %zu bytes of rows", bytes);
+    CK(cudaMemcpyAsync(h->rows.p, x, bytes, cudaMemcpyHostToDevice, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    h->rows_dtype = dtype;
+    h->rows_n = n;
+    h->rows_d = d;
+    return EMB200_OK;
+}
+
+int emb200_assign_resident(emb200_handle* h, uint32_t* labels, float* dist) {
+    if (!h) return EMB200_EINVAL;
+    if (h->rows_dtype < 0) return fail(h, EMB200_ESTATE, "load_rows must be called first");
+    int rc = check_ready(h, h->rows_dtype);
+    if (rc) return rc;
+    if (h->rows_d != h->d) return fail(h, EMB200_EINVAL, "rows have d = %zu, centroids d = %zu", h->rows_d, h->d);
+    if (h->res_labels.ensure(h->rows_n) || h->res_dist.ensure(h->rows_n))
+        return fail(h, EMB200_ENOMEM, "result allocation failed");
+    h->stats = emb200_stats{};
+    cudaStream_t st = h->stream;
+    CK(cudaEventRecord(h->ev0, st));
+    rc = assign_dispatch(h, h->rows_dtype, h->rows.p, nullptr, h->rows_n, h->res_labels.p, h->res_dist.p, st);
+    if (rc) return rc;
+    CK(cudaEventRecord(h->ev1, st));
+    uint32_t cnt[2] = {0, 0};
+    if (!use_i8_mode(h, h->rows_dtype)) CK(cudaMemcpyAsync(cnt, h->counters.p, sizeof cnt, cudaMemcpyDeviceToHost, st));
+    if (labels) CK(cudaMemcpyAsync(labels, h->res_labels.p, h->rows_n * 4, cudaMemcpyDeviceToHost, st));
+    if (dist) CK(cudaMemcpyAsync(dist, h->res_dist.p, h->rows_n * 4, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, h->ev0, h->ev1);
+    h->stats.rows = h->rows_n;
+    h->stats.rows_certified = use_i8_mode(h, h->rows_dtype) ? h->rows_n : cnt[1];
+    h->stats.rows_researched = cnt[0];
+    h->stats.ms_total = ms;
+    return EMB200_OK;
+}
+
+int emb200_resolve_recipe(size_t n, size_t d, size_t k, const emb200_config* cfg, emb200_recipe* out,
+                          uint64_t* epoch_rows, size_t max_epochs) {
+    if (!cfg || !out) return EMB200_EINVAL;
+    Recipe r = resolve_recipe(n, d, k, *cfg);
+    out->batch_size = r.batch_size;
+    out->alpha0 = r.alpha0;
+    out->n_epochs = r.epoch_rows.size();
+    out->total_steps = r.total_steps;
+    out->unused_threshold = r.unused_threshold;
+    if (epoch_rows)
+        for (size_t i = 0; i < r.epoch_rows.size() && i < max_epochs; i++) epoch_rows[i] = r.epoch_rows[i];
+    return EMB200_OK;
+}
+
+double emb200_scheduled_alpha(double alpha0, size_t step, size_t total) { return scheduled_alpha(alpha0, step, total); }
+
+}  // extern "C"
+
+#include "engine_train.inc"

@@ -1,0 +1,260 @@
+// Exact kernels: centroid preparation, certification of the fast top-2 and the
+// exact re-search, all in the reference CpuAssigner's own f32 rounding.
+#pragma once
+#include <cuda_bf16.h>
+#include "common.cuh"
+
+namespace emb {
+
+constexpr unsigned kFull = 0xffffffffu;
+
+// Device-side bounds used by the certification (filled by k_prep_centroids / k_bias).
+struct Bounds {
+    float cmax;  // >= max_j |c_j| (upper-rounded)
+    float nmax;  // >= max_j |norms_j| (norms include the bias)
+    float cmax_hi;  // >= max_j |bf16(c_j)| (three-term split bound)
+    float pad;
+};
+
+EMB_DEV void atomic_max_pos(float* addr, float v) {
+    // Non-negative floats order like their bit patterns.
+    atomicMax((unsigned int*)addr, __float_as_uint(v));
+}
+
+// Warp-cooperative sqnorm_ref (src/cpu.rs:169-180). All lanes return the value.
+template <typename T>
+EMB_DEV float warp_sqnorm_ref(const T* v, int d, int lane) {
+    int body = d & ~15;
+    float acc = 0.0f;
+    if (lane < 16)
+        for (int i = lane; i < body; i += 16) {
+            float a = to_f32(v[i]);
+            acc = __fadd_rn(acc, __fmul_rn(a, a));
+        }
+    float s = -0.0f;
+#pragma unroll
+    for (int q = 0; q < 16; q++) s = __fadd_rn(s, __shfl_sync(kFull, acc, q));
+    float t = -0.0f;
+    for (int i = body; i < d; i++) {
+        float a = to_f32(v[i]);
+        t = __fadd_rn(t, __fmul_rn(a, a));
+    }
+    return __fadd_rn(s, t);
+}
+
+// Group-cooperative reference dot product. The warp is split in groups of
+// G = 16 lanes (AVX-512 rounding) or 8 lanes (AVX2, portable); each group
+// computes x . cg for its own centroid pointer cg; every lane of the group
+// returns the group's value. Must be called by all 32 lanes.
+template <typename T>
+EMB_DEV float group_dot_ref(int match, const T* x, const float* cg, int d, int lane) {
+    if (match == kMatchAvx512) {
+        int l = lane & 15;
+        float acc = 0.0f;
+        int dr = (d + 15) & ~15;
+        for (int i = l; i < dr; i += 16) {
+            float a = i < d ? to_f32(x[i]) : 0.0f, b = i < d ? cg[i] : 0.0f;
+            acc = __fmaf_rn(a, b, acc);
+        }
+        // Lane l holds acc[l]; xor 8,4,2,1 is the tree of _mm512_reduce_add_ps.
+        acc = __fadd_rn(acc, __shfl_xor_sync(kFull, acc, 8));
+        acc = __fadd_rn(acc, __shfl_xor_sync(kFull, acc, 4));
+        acc = __fadd_rn(acc, __shfl_xor_sync(kFull, acc, 2));
+        acc = __fadd_rn(acc, __shfl_xor_sync(kFull, acc, 1));
+        return acc;
+    } else if (match == kMatchAvx2) {
+        int l = lane & 7;
+        int body = d & ~7;
+        float acc = 0.0f;
+        for (int i = l; i < body; i += 8) acc = __fmaf_rn(to_f32(x[i]), cg[i], acc);
+        acc = __fadd_rn(acc, __shfl_xor_sync(kFull, acc, 4));
+        acc = __fadd_rn(acc, __shfl_xor_sync(kFull, acc, 2));
+        acc = __fadd_rn(acc, __shfl_xor_sync(kFull, acc, 1));
+        for (int i = body; i < d; i++) acc = __fadd_rn(acc, __fmul_rn(to_f32(x[i]), cg[i]));
+        return acc;
+    } else {
+        int l = lane & 7;
+        int body = d & ~7;
+        float acc = 0.0f;
+        for (int i = l; i < body; i += 8) acc = __fadd_rn(acc, __fmul_rn(to_f32(x[i]), cg[i]));
+        float s = -0.0f;
+        int base = lane & ~7;
+#pragma unroll
+        for (int q = 0; q < 8; q++) s = __fadd_rn(s, __shfl_sync(kFull, acc, base | q));
+        float tail = -0.0f;
+        for (int i = body; i < d; i++) tail = __fadd_rn(tail, __fmul_rn(to_f32(x[i]), cg[i]));
+        return __fadd_rn(s, tail);
+    }
+}
+
+// set_centroids (src/cpu.rs:84-93): norms_j = sqnorm_ref(c_j); bounds for the
+// certification; optionally the BF16 hi/lo split (hi = bf16(c), lo = bf16(c - hi)),
+// written K-major into `split` with row stride `kpad` (hi at column t, lo at column kpad/2 + t).
+// One warp per centroid.
+__global__ void k_prep_centroids(const float* __restrict__ c, int k, int d, float* __restrict__ norms,
+                                 Bounds* __restrict__ bounds, __nv_bfloat16* __restrict__ hi,
+                                 __nv_bfloat16* __restrict__ lo, int kpad) {
+    int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    int lane = threadIdx.x & 31;
+    if (warp >= k) return;
+    const float* cj = c + (size_t)warp * d;
+    float nrm = warp_sqnorm_ref(cj, d, lane);
+    float ss = 0.0f, ssh = 0.0f;
+    for (int i = lane; i < kpad; i += 32) {
+        float v = i < d ? cj[i] : 0.0f;
+        ss = __fmaf_ru(v, v, ss);
+        if (hi) {
+            __nv_bfloat16 h = __float2bfloat16_rn(v);
+            float hf = __bfloat162float(h);
+            __nv_bfloat16 l = __float2bfloat16_rn(v - hf);
+            hi[(size_t)warp * kpad + i] = h;
+            lo[(size_t)warp * kpad + i] = l;
+            ssh = __fmaf_ru(hf, hf, ssh);
+        }
+    }
+    for (int o = 16; o; o >>= 1) {
+        ss = __fadd_ru(ss, __shfl_xor_sync(kFull, ss, o));
+        ssh = __fadd_ru(ssh, __shfl_xor_sync(kFull, ssh, o));
+    }
+    if (lane == 0) {
+        norms[warp] = nrm;
+        atomic_max_pos(&bounds->cmax, __fmul_ru(__fsqrt_ru(ss), 1.0000005f));
+        atomic_max_pos(&bounds->nmax, fabsf(nrm));
+        atomic_max_pos(&bounds->cmax_hi, __fmul_ru(__fsqrt_ru(ssh), 1.0000005f));
+    }
+}
+
+// set_bias (src/cpu.rs:95-99): norms_j += bias_j, and refresh nmax.
+__global__ void k_add_bias(float* __restrict__ norms, const float* __restrict__ bias, int k, Bounds* bounds) {
+    int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= k) return;
+    float v = __fadd_rn(norms[j], bias[j]);
+    norms[j] = v;
+    atomic_max_pos(&bounds->nmax, fabsf(v));
+}
+
+// Certification of the fast top-2 (one warp per row).
+//   part_s/part_i: nsplit partial top-2 lists per row, [split][row][2].
+//   The approximate score of every centroid is within E of its reference
+//   score, E = ka * |x| * cmax + kb * nmax. With j1, j2 re-scored exactly and
+//   b their better one, every other centroid j has s_j >= s^_2 - E; if
+//   b < s^_2 - E no other centroid can reach b, so b is the reference's label.
+//   Rows that fail go to the exact re-search list.
+template <typename T>
+__global__ void k_certify(const T* __restrict__ x, const uint32_t* __restrict__ gather, int m, int d,
+                          const float* __restrict__ c, const float* __restrict__ norms, int k,
+                          const float* __restrict__ part_s, const uint32_t* __restrict__ part_i, int nsplit,
+                          const Bounds* __restrict__ bounds, float ka, float kb, int match,
+                          uint32_t* __restrict__ labels, float* __restrict__ dist,
+                          uint32_t* __restrict__ redo_rows, uint32_t* __restrict__ redo_count,
+                          uint32_t* __restrict__ cert_count) {
+    int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    int lane = threadIdx.x & 31;
+    if (row >= m) return;
+    size_t src = gather ? gather[row] : (size_t)row;
+    const T* xr = x + src * (size_t)d;
+
+    Top2 t;
+    t.init();
+    for (int s = 0; s < nsplit; s++) {
+        size_t o = ((size_t)s * m + row) * 2;
+        t.push(part_s[o], part_i[o]);
+        t.push(part_s[o + 1], part_i[o + 1]);
+    }
+    float xn = warp_sqnorm_ref(xr, d, lane);
+    // Exact re-score of the two candidates: group 0 takes j1, group 1 takes j2.
+    uint32_t j1 = t.i1 < (uint32_t)k ? t.i1 : 0u;
+    uint32_t j2 = t.i2 < (uint32_t)k ? t.i2 : j1;
+    int gsz = match == kMatchAvx512 ? 16 : 8;
+    uint32_t jg = (lane / gsz) == 1 ? j2 : j1;
+    float dg = group_dot_ref(match, xr, c + (size_t)jg * d, d, lane);
+    float d1 = __shfl_sync(kFull, dg, 0);
+    float d2 = __shfl_sync(kFull, dg, gsz);
+    if (lane != 0) return;
+    bool ok = t.i1 < (uint32_t)k && (k < 2 || t.i2 < (uint32_t)k);
+    float s1 = score_ref(norms[j1], d1);
+    float sb = s1;
+    uint32_t jb = j1;
+    if (t.i2 < (uint32_t)k) {
+        float s2 = score_ref(norms[j2], d2);
+        if (lex_less(s2, j2, sb, jb)) {
+            sb = s2;
+            jb = j2;
+        }
+    }
+    if (ok && k > 2) {
+        float xnorm = __fmul_ru(__fsqrt_ru(fmaxf(xn, 0.0f)), 1.0000005f);
+        float E = __fadd_ru(__fmul_ru(__fmul_ru(ka, xnorm), bounds->cmax), __fmul_ru(kb, bounds->nmax));
+        float thr = __fsub_rd(t.s2, E);
+        ok = isfinite(E) && sb < thr;  // NaN-safe: any NaN fails
+    }
+    if (ok && !(sb < __int_as_float(0x7f800000))) ok = false;  // non-finite best: re-search
+    if (ok) {
+        labels[row] = jb;
+        dist[row] = fmaxf(__fadd_rn(sb, xn), 0.0f);
+        atomicAdd(cert_count, 1u);
+    } else {
+        uint32_t slot = atomicAdd(redo_count, 1u);
+        redo_rows[slot] = (uint32_t)row;
+    }
+}
+
+// Exact re-search (src/cpu.rs:108-167 semantics) of the rows in redo_rows:
+// every centroid scored in the reference rounding, strict < in ascending j
+// (lowest index on ties), best starts at +inf with label 0; dist =
+// max(best + sqnorm(x), 0). One warp per row; the warp's groups take
+// interleaved centroids. Persistent grid: warps stride over the list.
+template <typename T>
+__global__ void k_research(const T* __restrict__ x, const uint32_t* __restrict__ gather, int d,
+                           const float* __restrict__ c, const float* __restrict__ norms, int k, int match,
+                           const uint32_t* __restrict__ redo_rows, const uint32_t* __restrict__ redo_count,
+                           uint32_t* __restrict__ labels, float* __restrict__ dist) {
+    int lane = threadIdx.x & 31;
+    int gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    int nwarps = (gridDim.x * blockDim.x) >> 5;
+    uint32_t count = *redo_count;
+    int gsz = match == kMatchAvx512 ? 16 : 8;
+    int ngroups = 32 / gsz;
+    int g = lane / gsz;
+    for (uint32_t r = gwarp; r < count; r += nwarps) {
+        uint32_t row = redo_rows[r];
+        size_t src = gather ? gather[row] : (size_t)row;
+        const T* xr = x + src * (size_t)d;
+        float best = __int_as_float(0x7f800000);
+        uint32_t lab = 0;
+        bool any = false;  // whether this group scored at least one centroid
+        for (int j0 = 0; j0 < k; j0 += ngroups) {
+            int j = j0 + g;
+            int jc = j < k ? j : k - 1;
+            float dg = group_dot_ref(match, xr, c + (size_t)jc * d, d, lane);
+            if (j < k) {
+                float s = score_ref(norms[j], dg);
+                if (s < best) {
+                    best = s;
+                    lab = (uint32_t)j;
+                }
+                any = true;
+            }
+        }
+        // Merge the groups in (score, index) order; a group that never beat +inf
+        // keeps label 0 like the reference (its candidate loses to any finite one).
+        float rb = best;
+        uint32_t rl = lab;
+        for (int q = 1; q < ngroups; q++) {
+            float ob = __shfl_sync(kFull, best, q * gsz);
+            uint32_t ol = __shfl_sync(kFull, lab, q * gsz);
+            if (lex_less(ob, ol, rb, rl) && ob < __int_as_float(0x7f800000)) {
+                rb = ob;
+                rl = ol;
+            }
+        }
+        (void)any;
+        float xn = warp_sqnorm_ref(xr, d, lane);
+        if (lane == 0) {
+            labels[row] = rl;
+            dist[row] = fmaxf(__fadd_rn(rb, xn), 0.0f);
+        }
+    }
+}
+
+}  // namespace emb

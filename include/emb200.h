@@ -1,0 +1,159 @@
+/*
+ * emb200.h - C ABI of the B200 e-means engine (libemb200.so).
+ *
+ * The engine is a drop-in backend for the nearest-centroid search and the
+ * training loop of the Rust crate `emeans` (andrewluetgers/e-means). Each
+ * entry point names the reference interface it replaces (paths inside the
+ * reference project). Conventions:
+ *   - every call returns 0 on success and a negative EMB200_E* code on error;
+ *     emb200_last_error() then describes it. No call aborts or throws;
+ *   - host pointers are caller-owned and only read or written during the call;
+ *     device memory is owned by the handle and freed by emb200_destroy;
+ *   - one thread at a time per handle (the trait methods take &mut self);
+ *     distinct handles are independent;
+ *   - every computation runs on the GPU; there is no CPU fallback. A missing
+ *     or unsupported GPU is reported by emb200_create.
+ */
+#ifndef EMB200_H
+#define EMB200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct emb200_handle emb200_handle;
+
+/* Error codes. */
+#define EMB200_OK 0
+#define EMB200_EINVAL -1  /* bad argument or shape (the reference asserts or returns Err) */
+#define EMB200_ECUDA -2   /* CUDA runtime or driver error */
+#define EMB200_ENOMEM -3  /* device allocation failed */
+#define EMB200_ESTATE -4  /* call out of order (e.g. assign before set_centroids) */
+#define EMB200_EDEVICE -5 /* no usable sm_100 device */
+
+/* Row element types (src/lib.rs:47-71, trait Scalar: f32, i8, u8). */
+#define EMB200_F32 0
+#define EMB200_I8 1
+#define EMB200_U8 2
+
+/* Search precision of the main contraction. Every mode returns the labels and
+ * distances of the reference CpuAssigner bit for bit: the fast contraction
+ * keeps the top-2 candidates per row with a rigorous error bound, both are
+ * re-scored with the reference's own f32 arithmetic, and rows the bound cannot
+ * certify are searched again exactly. */
+#define EMB200_PREC_FP32 0  /* FP32 SIMT contraction */
+#define EMB200_PREC_BF16 1  /* tcgen05 BF16, three-term split (hi*hi + hi*lo + lo*hi), FP32 accumulate */
+#define EMB200_PREC_BF16X1 2 /* tcgen05 BF16 single term, FP32 accumulate (wider bound, more re-search) */
+
+/* Centroid representation for i8 rows (src/cpu_i8.rs:21-25). */
+#define EMB200_CENTROIDS_F32 0 /* CpuAssigner semantics: rows widened to f32 */
+#define EMB200_CENTROIDS_I8 8  /* CpuI8Assigner(CentroidBits::I8): centroids rounded to i8, exact integer ranking */
+
+/* Which CpuAssigner kernel's f32 rounding the exact re-score reproduces
+ * (src/cpu.rs:13-33: AVX-512 on CPUs that have it, else AVX2+FMA, else portable). */
+#define EMB200_MATCH_AVX512 0
+#define EMB200_MATCH_AVX2 1
+#define EMB200_MATCH_PORTABLE 2
+
+typedef struct {
+    int precision;     /* EMB200_PREC_* (default FP32) */
+    int centroid_bits; /* EMB200_CENTROIDS_* (default F32) */
+    int match_kernel;  /* EMB200_MATCH_* (default AVX512) */
+    int reserved[5];
+} emb200_opts;
+
+/* Config, src/lib.rs:104-124. Optional fields use sentinels:
+ * batch_size 0 = None, alpha0 <= 0 = None, unused_threshold < 0 = None. */
+typedef struct {
+    double nepochs;
+    int batch_law; /* 0 Auto, 1 Throughput, 2 Quality (src/lib.rs:94-101) */
+    uint64_t batch_size;
+    double alpha0;
+    float unused_threshold;
+    float balance;
+    uint64_t seed;
+    int verbose;
+    int closing_f64; /* 0: f32 pass sums as the reference (bit-exact); 1: FP64 pass sums */
+} emb200_config;
+
+/* Recipe, src/lib.rs:143-149 (epoch_rows written to a caller array). */
+typedef struct {
+    uint64_t batch_size;
+    double alpha0;
+    uint64_t n_epochs;
+    uint64_t total_steps;
+    float unused_threshold;
+} emb200_recipe;
+
+/* Counters of the last assign / train call. */
+typedef struct {
+    uint64_t rows;           /* rows searched */
+    uint64_t rows_certified; /* rows whose fast top-2 the error bound certified */
+    uint64_t rows_researched; /* rows searched again with exact arithmetic */
+    uint64_t kernel_launches; /* kernels launched by the call */
+    double ms_total;          /* device time of the call (CUDA events) */
+} emb200_stats;
+
+/* ---- lifecycle ---------------------------------------------------------- */
+
+/* Replaces CudaAssigner::new (src/cuda.rs:69-91). opts may be NULL (defaults). */
+int emb200_create(int ordinal, const emb200_opts* opts, emb200_handle** out);
+int emb200_destroy(emb200_handle* h);
+/* Description of the last error on this handle (never NULL). */
+const char* emb200_last_error(const emb200_handle* h);
+/* Assigner::name, src/lib.rs:83. */
+int emb200_name(emb200_handle* h, char* buf, size_t len);
+/* Set or read options after creation (takes effect at the next call). */
+int emb200_set_opts(emb200_handle* h, const emb200_opts* opts);
+int emb200_get_stats(const emb200_handle* h, emb200_stats* out);
+
+/* ---- Assigner trait (src/lib.rs:75-91) ---------------------------------- */
+
+/* Assigner::set_centroids, src/lib.rs:77 (CpuAssigner src/cpu.rs:84-93,
+ * CpuI8Assigner src/cpu_i8.rs:73-110): k x d row-major f32, host memory. */
+int emb200_set_centroids(emb200_handle* h, const float* centroids, size_t k, size_t d);
+/* Assigner::set_bias, src/lib.rs:81 (src/cpu.rs:95-99, src/cpu_i8.rs:112-117):
+ * adds bias[j] to centroid j's score until the next set_centroids. */
+int emb200_set_bias(emb200_handle* h, const float* bias, size_t k);
+/* AssignRows<T>::assign, src/lib.rs:90 (src/cpu.rs:108-167, src/cpu_i8.rs:130-191):
+ * m rows of d elements (host, row-major) -> labels[m], dist[m] (host). */
+int emb200_assign_f32(emb200_handle* h, const float* x, size_t m, uint32_t* labels, float* dist);
+int emb200_assign_i8(emb200_handle* h, const int8_t* x, size_t m, uint32_t* labels, float* dist);
+int emb200_assign_u8(emb200_handle* h, const uint8_t* x, size_t m, uint32_t* labels, float* dist);
+
+/* Same as emb200_assign_* with device pointers, enqueued on `stream`
+ * (cudaStream_t, or NULL for the handle's stream); no host copies, no sync. */
+int emb200_assign_device(emb200_handle* h, int dtype, const void* x_dev, size_t m, uint32_t* labels_dev,
+                         float* dist_dev, void* stream);
+
+/* ---- resident rows (rows uploaded once, src/cuda.rs:8-9 streamed them) ---- */
+
+/* Upload n x d rows of dtype once; they stay in HBM for assign_resident/train. */
+int emb200_load_rows(emb200_handle* h, int dtype, const void* x, size_t n, size_t d);
+/* assign() (src/lib.rs:512-520) over the resident rows with the current
+ * centroids. labels/dist: host arrays of n, or NULL to keep results on device. */
+int emb200_assign_resident(emb200_handle* h, uint32_t* labels, float* dist);
+
+/* ---- training (src/lib.rs:201-225 and 348-491) --------------------------- */
+
+/* resolve_recipe, src/lib.rs:201-225. epoch_rows: array of max_epochs. */
+int emb200_resolve_recipe(size_t n, size_t d, size_t k, const emb200_config* cfg, emb200_recipe* out,
+                          uint64_t* epoch_rows, size_t max_epochs);
+/* scheduled_alpha, src/lib.rs:194-198. */
+double emb200_scheduled_alpha(double alpha0, size_t step, size_t total);
+
+/* train (src/lib.rs:348-491) on the resident rows, entirely on the device.
+ * Outputs (host, caller-allocated, any may be NULL): centroids k*d, labels n
+ * (last-pass labels, UINT32_MAX where unset), objective n_epochs, n_splits.
+ * The trained centroids also become the handle's current centroids. */
+int emb200_train(emb200_handle* h, const emb200_config* cfg, size_t k, float* centroids, uint32_t* labels,
+                 double* objective, uint64_t* n_splits, emb200_recipe* recipe);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* EMB200_H */

@@ -1,0 +1,197 @@
+"""GPU parity of the fused assign through the C ABI against the oracle.
+
+Every precision mode must return the CpuAssigner's labels and distances bit
+for bit (the fast contraction is certified and re-scored in the reference's
+own f32 rounding), and the I8 mode CpuI8Assigner(I8)'s bit for bit.
+"""
+import numpy as np
+import pytest
+
+from tests.test_oracle import SHAPES_F32, SHAPES_I8, lcg_f32, lcg_i8
+
+pytestmark = pytest.mark.gpu
+
+PRECISIONS = ["fp32", "bf16", "bf16x1"]
+
+
+def same_f32(a, b):
+    return np.array_equal(np.asarray(a, np.float32).view(np.uint32), np.asarray(b, np.float32).view(np.uint32))
+
+
+@pytest.fixture(scope="module")
+def assigners(emb):
+    made = {}
+
+    def get(precision="fp32", centroid_bits=0, match="avx512"):
+        key = (precision, centroid_bits, match)
+        if key not in made:
+            made[key] = emb.B200Assigner(0, precision=precision, centroid_bits=centroid_bits, match=match)
+        return made[key]
+
+    yield get
+    for a in made.values():
+        a.close()
+
+
+@pytest.mark.parametrize("precision", PRECISIONS)
+@pytest.mark.parametrize("match", ["avx512", "avx2", "portable"])
+def test_reference_shapes_bit_exact(orc, assigners, precision, match):
+    # The shape list of src/cpu.rs:290 (every tail path), the reference's LCG data.
+    a = assigners(precision, 0, match)
+    for (n, k, d) in SHAPES_F32:
+        x, c = lcg_f32(n * d, 1).reshape(n, d), lcg_f32(k * d, 2).reshape(k, d)
+        a.set_centroids(c)
+        lab, dist = a.assign(x)
+        rl, rd = orc.cpu_assign(x, c, kernel=match, emulate=True)
+        assert np.array_equal(lab, rl), (n, k, d)
+        assert same_f32(dist, rd), (n, k, d)
+        # and the f64 brute-force tolerance of src/cpu.rs:303-305
+        _, best = orc.bruteforce_f64(x, c)
+        assert np.all(np.abs(dist - best) <= 1e-4 * (1 + best))
+
+
+@pytest.mark.parametrize("precision", PRECISIONS)
+def test_matches_cpu_bar(orc, assigners, precision):
+    # src/cuda.rs:221-249: n=3000, k=1031, d=100, >= 99.9% labels; here: all, bit for bit.
+    n, k, d = 3000, 1031, 100
+    s = lcg_f32((n + k) * d, 1)
+    x, c = s[: n * d].reshape(n, d), s[n * d:].reshape(k, d)
+    a = assigners(precision)
+    a.set_centroids(c)
+    lab, dist = a.assign(x)
+    rl, rd = orc.cpu_assign(x, c, emulate=True)
+    assert np.array_equal(lab, rl)
+    assert same_f32(dist, rd)
+    st = a.stats()
+    assert st["rows"] == n and st["rows_certified"] + st["rows_researched"] == n
+
+
+@pytest.mark.parametrize("precision", PRECISIONS)
+def test_embedding_rows_bit_exact(emb, orc, assigners, precision):
+    x = emb.datasets.embeddings(20_000, 128, seed=3)
+    c = x[np.random.default_rng(4).choice(len(x), 2048, replace=False)] + np.float32(1e-3)
+    a = assigners(precision)
+    a.set_centroids(c)
+    lab, dist = a.assign(x)
+    rl, rd = orc.cpu_assign(x, c, emulate=False if orc.has_kernel("avx512") else True)
+    assert np.array_equal(lab, rl)
+    assert same_f32(dist, rd)
+
+
+@pytest.mark.parametrize("precision", PRECISIONS)
+@pytest.mark.parametrize("dtype", [np.int8, np.uint8])
+def test_integer_rows_f32_semantics(orc, assigners, precision, dtype):
+    # src/cpu.rs:106-127: non-f32 rows widened, identical to f32 input.
+    rng = np.random.default_rng(7)
+    info = np.iinfo(dtype)
+    x = rng.integers(info.min, info.max + 1, (500, 72), dtype=dtype)
+    c = rng.standard_normal((300, 72)).astype(np.float32) * 40
+    a = assigners(precision)
+    a.set_centroids(c)
+    lab, dist = a.assign(x)
+    rl, rd = orc.cpu_assign(x, c, emulate=True)
+    assert np.array_equal(lab, rl) and same_f32(dist, rd)
+
+
+@pytest.mark.parametrize("precision", PRECISIONS)
+def test_bias_is_added_and_reset(orc, assigners, precision):
+    # Assigner::set_bias (src/lib.rs:78-81): dist includes the bias; set_centroids resets it.
+    rng = np.random.default_rng(9)
+    x = rng.standard_normal((777, 33)).astype(np.float32)
+    c = rng.standard_normal((250, 33)).astype(np.float32)
+    bias = rng.uniform(0, 3, 250).astype(np.float32)
+    a = assigners(precision)
+    a.set_centroids(c)
+    a.set_bias(bias)
+    lab, dist = a.assign(x)
+    rl, rd = orc.cpu_assign(x, c, bias=bias, emulate=True)
+    assert np.array_equal(lab, rl) and same_f32(dist, rd)
+    a.set_centroids(c)
+    lab, dist = a.assign(x)
+    rl, rd = orc.cpu_assign(x, c, emulate=True)
+    assert np.array_equal(lab, rl) and same_f32(dist, rd)
+
+
+@pytest.mark.parametrize("precision", PRECISIONS)
+def test_ties_go_to_lowest_index(orc, assigners, precision):
+    rng = np.random.default_rng(11)
+    base = rng.standard_normal((40, 16)).astype(np.float32)
+    c = np.concatenate([base, base, base[::-1]])  # every centroid duplicated
+    x = base[rng.integers(0, 40, 300)] + rng.standard_normal((300, 16)).astype(np.float32) * 0.01
+    x[:40] = base  # exact hits: distance 0 with two tied centroids
+    a = assigners(precision)
+    a.set_centroids(c)
+    lab, dist = a.assign(x)
+    rl, rd = orc.cpu_assign(x, c, emulate=True)
+    assert np.array_equal(lab, rl) and same_f32(dist, rd)
+    assert np.all(lab < 40)
+
+
+def test_edge_cases(orc, assigners):
+    a = assigners("fp32")
+    # k = 1, d = 1
+    a.set_centroids(np.array([[2.0]], np.float32))
+    lab, dist = a.assign(np.array([[0.0], [5.0]], np.float32))
+    assert lab.tolist() == [0, 0] and dist.tolist() == [4.0, 9.0]
+    # m = 0
+    a.set_centroids(np.ones((3, 4), np.float32))
+    lab, dist = a.assign(np.zeros((0, 4), np.float32))
+    assert lab.size == 0
+    # NaN row: no score beats +inf, label 0, dist max(NaN, 0) = 0 (src/cpu.rs:149,161)
+    c = np.random.default_rng(1).standard_normal((70, 4)).astype(np.float32)
+    x = np.random.default_rng(2).standard_normal((5, 4)).astype(np.float32)
+    x[2, 1] = np.nan
+    a.set_centroids(c)
+    lab, dist = a.assign(x)
+    rl, rd = orc.cpu_assign(x, c, emulate=True)
+    assert np.array_equal(lab, rl) and same_f32(dist, rd)
+
+
+def test_errors_are_reported(emb):
+    a = emb.B200Assigner(0)
+    with pytest.raises(emb.EngineError, match="set_centroids"):
+        a.assign(np.zeros((3, 4), np.float32))
+    a.set_centroids(np.ones((3, 4), np.float32))
+    with pytest.raises(emb.EngineError, match="bias"):
+        a.set_bias(np.ones(5, np.float32))
+    with pytest.raises(emb.EngineError):
+        emb.B200Assigner(99)
+    a.close()
+
+
+@pytest.mark.parametrize("shape", SHAPES_I8)
+def test_i8_mode_integer_exact(orc, assigners, shape):
+    # src/cpu_i8.rs:298-324 data; CpuI8Assigner(I8) labels and dists bit for bit.
+    n, k, d = shape
+    x, ci = lcg_i8(n * d, 1).reshape(n, d), lcg_i8(k * d, 2).reshape(k, d)
+    a = assigners("fp32", 8)
+    for c in (ci.astype(np.float32), ci.astype(np.float32) * np.float32(0.37) + np.float32(0.5)):
+        a.set_centroids(c)
+        lab, dist = a.assign(x)
+        rl, rd = orc.i8_assign(x, c, bits=8)
+        assert np.array_equal(lab, rl) and same_f32(dist, rd)
+
+
+def test_i8_mode_with_bias(orc, assigners):
+    rng = np.random.default_rng(5)
+    x = rng.integers(-128, 128, (600, 96), dtype=np.int8)
+    c = rng.standard_normal((333, 96)).astype(np.float32) * 50
+    bias = rng.uniform(0, 5000, 333).astype(np.float32)
+    a = assigners("fp32", 8)
+    a.set_centroids(c)
+    a.set_bias(bias)
+    lab, dist = a.assign(x)
+    rl, rd = orc.i8_assign(x, c, bits=8, bias=bias)
+    assert np.array_equal(lab, rl) and same_f32(dist, rd)
+
+
+@pytest.mark.parametrize("precision", PRECISIONS)
+def test_resident_assign_matches_host_path(emb, assigners, precision):
+    x = emb.datasets.embeddings(50_000, 64, seed=8)
+    c = x[:1500] * np.float32(0.9)
+    a = assigners(precision)
+    a.set_centroids(c)
+    l1, d1 = a.assign(x)
+    a.load_rows(x)
+    l2, d2 = a.assign_resident()
+    assert np.array_equal(l1, l2) and same_f32(d1, d2)
