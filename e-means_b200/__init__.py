@@ -51,7 +51,8 @@ class _Recipe(ctypes.Structure):
 
 class _Stats(ctypes.Structure):
     _fields_ = [("rows", ctypes.c_uint64), ("rows_certified", ctypes.c_uint64), ("rows_researched", ctypes.c_uint64),
-                ("kernel_launches", ctypes.c_uint64), ("ms_total", ctypes.c_double)]
+                ("kernel_launches", ctypes.c_uint64), ("ms_total", ctypes.c_double), ("fast_kernel", ctypes.c_int32),
+                ("fast_aborted", ctypes.c_int32)]
 
 
 def build(force=False):

@@ -75,6 +75,8 @@ struct emb200_handle {
     DevBuf<Bounds> bounds;
     DevBuf<__nv_bfloat16> c_hi, c_lo;  // K-major BF16 split, row stride kpad
     size_t kpad = 0;
+    CUtensorMap map_hi{}, map_lo{};  // TMA descriptors of c_hi / c_lo (128B swizzle, 64 x 128 boxes)
+    bool maps_ok = false;
     DevBuf<int8_t> c8;   // I8 centroids (CpuI8Assigner)
     DevBuf<long long> off8;  // I8 offsets: sum c8^2 (+ bias)
     bool bias_set = false;
@@ -155,6 +157,41 @@ bool use_i8_mode(const emb200_handle* h, int dtype) {
 }
 
 
+// cuTensorMapEncodeTiled from the driver, fetched at run time (no libcuda link).
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encode_tiled_fn() {
+    static EncodeTiledFn fn = nullptr;
+    static bool tried = false;
+    if (!tried) {
+        tried = true;
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = (EncodeTiledFn)p;
+    }
+    return fn;
+}
+
+// 2-D map over a k x kpad BF16 matrix (row stride kpad), boxes of 64 x 128
+// (one 128-byte swizzle atom wide); rows past k read as zeros.
+int encode_bf16_map(emb200_handle* h, CUtensorMap* map, void* base) {
+    EncodeTiledFn fn = encode_tiled_fn();
+    if (!fn) return fail(h, EMB200_ECUDA, "cuTensorMapEncodeTiled unavailable");
+    cuuint64_t dims[2] = {(cuuint64_t)h->kpad, (cuuint64_t)h->k};
+    cuuint64_t strides[1] = {(cuuint64_t)h->kpad * 2};
+    cuuint32_t box[2] = {64, (cuuint32_t)kTcBN};
+    cuuint32_t estr[2] = {1, 1};
+    CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, base, dims, strides, box, estr,
+                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return fail(h, EMB200_ECUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+    return EMB200_OK;
+}
+
 // set_centroids on the device: reference norms, certification bounds, and the
 // forms the selected search needs (BF16 split for tcgen05, i8 for I8 mode).
 int prepare_centroids(emb200_handle* h) {
@@ -168,7 +205,14 @@ int prepare_centroids(emb200_handle* h) {
             return fail(h, EMB200_ENOMEM, "BF16 centroid allocation failed");
         hi = h->c_hi.p;
         lo = h->c_lo.p;
+        h->maps_ok = false;
+        int rc = encode_bf16_map(h, &h->map_hi, hi);
+        if (rc) return rc;
+        rc = encode_bf16_map(h, &h->map_lo, lo);
+        if (rc) return rc;
+        h->maps_ok = true;
     } else {
+        h->maps_ok = false;
         h->kpad = (h->d + 63) / 64 * 64;
     }
     k_prep_centroids<<<(unsigned)((k + 7) / 8), 256, 0, st>>>(h->c.p, k, d, h->norms.p, h->bounds.p, hi, lo,
@@ -210,7 +254,7 @@ int launch_i8_assign(emb200_handle* h, const int8_t* x, const uint32_t* gather, 
     if (h->part_s.ensure((size_t)nsplit * m * 2) || h->part_i.ensure((size_t)nsplit * m))
         return fail(h, EMB200_ENOMEM, "scratch allocation failed for %zu rows", m);
     size_t kp = (h->d + 31) / 32 * 32;
-    int xvec = (d % 16 == 0) ? 1 : 0;
+    int xvec = (d % 16 == 0 && ((uintptr_t)x & 15) == 0) ? 1 : 0;
     dim3 grid(row_tiles, nsplit);
     k_assign_i8<<<grid, 256, 0, st>>>(x, gather, (int)m, d, h->c8.p, (int)kp, h->off8.p, k,
                                       (long long*)h->part_s.p, h->part_i.p, xvec);
@@ -221,18 +265,50 @@ int launch_i8_assign(emb200_handle* h, const int8_t* x, const uint32_t* gather, 
     return EMB200_OK;
 }
 
+int tc_terms(const emb200_handle* h, int dtype) {
+    if (h->opts.precision == EMB200_PREC_BF16X1) return 1;
+    return dtype == EMB200_F32 ? 3 : 2;
+}
+
 bool tc_supported(const emb200_handle* h, int dtype) {
-    (void)h; (void)dtype;
-    return false;
+    if (!h->maps_ok) return false;
+    TcSmem L = tc_smem_layout((int)h->kpad, tc_terms(h, dtype));
+    return L.total + 1024 <= 227 * 1024;
 }
+
 int tc_nsplit(const emb200_handle* h, size_t m) {
-    (void)h; (void)m;
-    return 1;
+    int row_tiles = (int)((m + kTcBM - 1) / kTcBM);
+    int ntiles = (int)((h->k + kTcBN - 1) / kTcBN);
+    if (row_tiles >= h->sm_count) return 1;
+    return std::max(1, std::min(ntiles, (h->sm_count + row_tiles - 1) / row_tiles));
 }
+
 template <typename T>
 int launch_tc_assign(emb200_handle* h, const T* x, const uint32_t* gather, size_t m, int nsplit, cudaStream_t st) {
-    (void)x; (void)gather; (void)m; (void)nsplit; (void)st;
-    return fail(h, EMB200_ESTATE, "tensor-core path not available");
+    const int dtype = std::is_same<T, float>::value ? EMB200_F32 : (std::is_same<T, int8_t>::value ? EMB200_I8 : EMB200_U8);
+    TcParams p;
+    p.m = (int)m;
+    p.d = (int)h->d;
+    p.k = (int)h->k;
+    p.kpad = (int)h->kpad;
+    p.nterms = tc_terms(h, dtype);
+    p.gather = gather;
+    p.norms = h->norms.p;
+    p.part_s = h->part_s.p;
+    p.part_i = h->part_i.p;
+    p.err = (int*)(h->counters.p + 2);
+    p.xvec = (h->d % 4 == 0 && ((uintptr_t)x & 15) == 0) ? 1 : 0;
+    TcSmem L = tc_smem_layout(p.kpad, p.nterms);
+    size_t smem = L.total + 1024;
+    static bool attr_set[3] = {false, false, false};
+    if (!attr_set[dtype]) {
+        CK(cudaFuncSetAttribute(k_assign_tc<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
+        attr_set[dtype] = true;
+    }
+    dim3 grid((unsigned)((m + kTcBM - 1) / kTcBM), (unsigned)nsplit);
+    k_assign_tc<T><<<grid, kTcThreads, smem, st>>>(x, h->map_hi, h->map_lo, p);
+    CKL();
+    return EMB200_OK;
 }
 
 // Full pipeline of one assign over m rows already on the device (x_dev, or
@@ -244,6 +320,7 @@ int assign_rows_dev(emb200_handle* h, const T* x, const uint32_t* gather, size_t
     const int k = (int)h->k, d = (int)h->d;
     if (m == 0) return EMB200_OK;
     if (use_i8_mode(h, dtype)) {
+        h->stats.fast_kernel = 2;
         return launch_i8_assign(h, (const int8_t*)x, gather, m, labels, dist, st);
     }
     int prec = h->opts.precision;
@@ -262,12 +339,13 @@ int assign_rows_dev(emb200_handle* h, const T* x, const uint32_t* gather, size_t
         h->redo_rows.ensure(mm) || h->counters.ensure(4))
         return fail(h, EMB200_ENOMEM, "scratch allocation failed for %zu rows", m);
     CK(cudaMemsetAsync(h->counters.p, 0, 4 * sizeof(uint32_t), st));
+    h->stats.fast_kernel = tc ? 1 : 0;
     if (tc) {
         int rc = launch_tc_assign(h, x, gather, m, nsplit, st);
         if (rc) return rc;
     } else {
         dim3 grid(row_tiles, nsplit);
-        int vec4 = (d % 4 == 0) ? 1 : 0;
+        int vec4 = (d % 4 == 0 && ((uintptr_t)x & 15) == 0) ? 1 : 0;
         k_assign_simt<T><<<grid, kSimtThreads, 0, st>>>(x, gather, (int)m, d, h->c.p, h->norms.p, k, h->part_s.p,
                                                          h->part_i.p, vec4);
         CKL();
@@ -277,7 +355,8 @@ int assign_rows_dev(emb200_handle* h, const T* x, const uint32_t* gather, size_t
     int match = h->opts.match_kernel;
     k_certify<T><<<(unsigned)((m + 7) / 8), 256, 0, st>>>(x, gather, (int)m, d, h->c.p, h->norms.p, k, h->part_s.p,
                                                            h->part_i.p, nsplit, h->bounds.p, ka, kb, match, labels,
-                                                           dist, h->redo_rows.p, h->counters.p, h->counters.p + 1);
+                                                           dist, h->redo_rows.p, h->counters.p, h->counters.p + 1,
+                                                           tc ? (const int*)(h->counters.p + 2) : nullptr);
     CKL();
     k_research<T><<<h->sm_count * 4, 256, 0, st>>>(x, gather, d, h->c.p, h->norms.p, k, match, h->redo_rows.p,
                                                     h->counters.p, labels, dist);
@@ -326,11 +405,12 @@ int assign_host(emb200_handle* h, int dtype, const void* x, size_t m, uint32_t* 
         if (rc) return rc;
         CK(cudaMemcpyAsync(labels + r0, h->st_labels.p, mc * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
         CK(cudaMemcpyAsync(dist + r0, h->st_dist.p, mc * sizeof(float), cudaMemcpyDeviceToHost, st));
-        uint32_t cnt[2] = {0, 0};
+        uint32_t cnt[3] = {0, 0, 0};
         if (!use_i8_mode(h, dtype)) CK(cudaMemcpyAsync(cnt, h->counters.p, sizeof cnt, cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
         redo += cnt[0];
         cert += cnt[1];
+        if (cnt[2]) h->stats.fast_aborted = 1;
     }
     CK(cudaEventRecord(h->ev1, st));
     CK(cudaEventSynchronize(h->ev1));
@@ -499,7 +579,7 @@ int emb200_assign_resident(emb200_handle* h, uint32_t* labels, float* dist) {
     rc = assign_dispatch(h, h->rows_dtype, h->rows.p, nullptr, h->rows_n, h->res_labels.p, h->res_dist.p, st);
     if (rc) return rc;
     CK(cudaEventRecord(h->ev1, st));
-    uint32_t cnt[2] = {0, 0};
+    uint32_t cnt[3] = {0, 0, 0};
     if (!use_i8_mode(h, h->rows_dtype)) CK(cudaMemcpyAsync(cnt, h->counters.p, sizeof cnt, cudaMemcpyDeviceToHost, st));
     if (labels) CK(cudaMemcpyAsync(labels, h->res_labels.p, h->rows_n * 4, cudaMemcpyDeviceToHost, st));
     if (dist) CK(cudaMemcpyAsync(dist, h->res_dist.p, h->rows_n * 4, cudaMemcpyDeviceToHost, st));
@@ -509,6 +589,7 @@ int emb200_assign_resident(emb200_handle* h, uint32_t* labels, float* dist) {
     h->stats.rows = h->rows_n;
     h->stats.rows_certified = use_i8_mode(h, h->rows_dtype) ? h->rows_n : cnt[1];
     h->stats.rows_researched = cnt[0];
+    h->stats.fast_aborted = cnt[2] ? 1 : 0;
     h->stats.ms_total = ms;
     return EMB200_OK;
 }

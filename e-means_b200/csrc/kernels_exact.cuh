@@ -147,7 +147,7 @@ __global__ void k_certify(const T* __restrict__ x, const uint32_t* __restrict__ 
                           const Bounds* __restrict__ bounds, float ka, float kb, int match,
                           uint32_t* __restrict__ labels, float* __restrict__ dist,
                           uint32_t* __restrict__ redo_rows, uint32_t* __restrict__ redo_count,
-                          uint32_t* __restrict__ cert_count) {
+                          uint32_t* __restrict__ cert_count, const int* __restrict__ fast_err) {
     int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     int lane = threadIdx.x & 31;
     if (row >= m) return;
@@ -189,6 +189,7 @@ __global__ void k_certify(const T* __restrict__ x, const uint32_t* __restrict__ 
         ok = isfinite(E) && sb < thr;  // NaN-safe: any NaN fails
     }
     if (ok && !(sb < __int_as_float(0x7f800000))) ok = false;  // non-finite best: re-search
+    if (fast_err && *fast_err) ok = false;  // the fast kernel gave up: trust nothing it wrote
     if (ok) {
         labels[row] = jb;
         dist[row] = fmaxf(__fadd_rn(sb, xn), 0.0f);

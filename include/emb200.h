@@ -95,6 +95,8 @@ typedef struct {
     uint64_t rows_researched; /* rows searched again with exact arithmetic */
     uint64_t kernel_launches; /* kernels launched by the call */
     double ms_total;          /* device time of the call (CUDA events) */
+    int32_t fast_kernel;      /* fast contraction used: 0 FP32 SIMT, 1 tcgen05 BF16, 2 exact int8 */
+    int32_t fast_aborted;     /* 1 if a bounded wait in the fast kernel gave up (rows then re-searched) */
 } emb200_stats;
 
 /* ---- lifecycle ---------------------------------------------------------- */

@@ -195,3 +195,21 @@ def test_resident_assign_matches_host_path(emb, assigners, precision):
     a.load_rows(x)
     l2, d2 = a.assign_resident()
     assert np.array_equal(l1, l2) and same_f32(d1, d2)
+
+
+@pytest.mark.parametrize("precision", ["bf16", "bf16x1"])
+@pytest.mark.parametrize("d", [1, 33, 64, 96, 128])
+def test_tcgen05_path_runs_and_certifies(emb, orc, assigners, precision, d):
+    # The tensor-core kernel (not the SIMT fallback) must serve d <= 128 and
+    # finish without a bounded wait giving up.
+    x = emb.datasets.embeddings(4000, d, latent=min(8, d), seed=d)
+    c = x[np.random.default_rng(d).choice(len(x), 700, replace=False)] * np.float32(0.98)
+    a = assigners(precision)
+    a.set_centroids(c)
+    lab, dist = a.assign(x)
+    st = a.stats()
+    assert st["fast_kernel"] == 1 and st["fast_aborted"] == 0, st
+    rl, rd = orc.cpu_assign(x, c, emulate=True)
+    assert np.array_equal(lab, rl) and same_f32(dist, rd)
+    if precision == "bf16" and d >= 33:  # at d = 1 every centroid ties with others: all rows re-searched
+        assert st["rows_researched"] <= 0.02 * len(x), st
