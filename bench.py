@@ -150,7 +150,8 @@ def run_ours(args):
         "config": {"workload": WORKLOAD, "rows_per_gpu": N_ROWS, "d": DIM, "k": K, "precision": head,
                    "l2": "inputs (512 MB of rows) larger than L2", "parallelism": f"replicas x{world}"},
         "per_precision": {p: {"rows_per_s": results[p]["rows_per_s_total"], "ms_per_step": results[p]["ms_per_step"],
-                              "researched_rows": results[p]["researched"]} for p in results},
+                              "refined_rows": results[p]["refined"], "researched_rows": results[p]["researched"]}
+                          for p in results},
         "gpu_launches": r["launches"],
     }
     if rank == 0:
@@ -178,6 +179,7 @@ def time_resident(a, emb, args, prec, world):
         t = float(tt.item())
     rows = N_ROWS * args.steps * world
     return {"rows_per_s_total": rows / (t / 1e3), "ms_per_step": t / args.steps, "researched": st["rows_researched"],
+            "refined": st["rows_refined"],
             "launches": st["kernel_launches"] * args.steps}
 
 

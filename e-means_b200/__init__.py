@@ -52,7 +52,7 @@ class _Recipe(ctypes.Structure):
 class _Stats(ctypes.Structure):
     _fields_ = [("rows", ctypes.c_uint64), ("rows_certified", ctypes.c_uint64), ("rows_researched", ctypes.c_uint64),
                 ("kernel_launches", ctypes.c_uint64), ("ms_total", ctypes.c_double), ("fast_kernel", ctypes.c_int32),
-                ("fast_aborted", ctypes.c_int32)]
+                ("fast_aborted", ctypes.c_int32), ("rows_refined", ctypes.c_uint64)]
 
 
 def build(force=False):

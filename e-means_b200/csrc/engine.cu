@@ -21,6 +21,8 @@
 #include "kernels_tc.cuh"
 #include "kernels_update.cuh"
 
+constexpr int kRefineCap = 32;  // candidates kept per refined row
+
 using namespace emb;
 
 namespace {
@@ -95,7 +97,9 @@ struct emb200_handle {
     DevBuf<float> part_s;
     DevBuf<uint32_t> part_i;
     DevBuf<uint32_t> redo_rows;
-    DevBuf<uint32_t> counters;  // [0] redo count, [1] certified count
+    DevBuf<float> redo_theta;
+    DevBuf<uint32_t> cand, cand_count, redo2_rows;  // refine pass
+    DevBuf<uint32_t> counters;  // see assign_rows_dev
 
     // training state
     TrainState train;
@@ -198,30 +202,32 @@ int prepare_centroids(emb200_handle* h) {
     cudaStream_t st = h->stream;
     const int k = (int)h->k, d = (int)h->d;
     CK(cudaMemsetAsync(h->bounds.p, 0, sizeof(Bounds), st));
+    // Norms are padded to whole 128-centroid tiles with +inf (never a candidate).
+    const size_t kp = (h->k + kTcBN - 1) / kTcBN * kTcBN;
+    k_fill<<<(unsigned)((kp + 255) / 256), 256, 0, st>>>(h->norms.p, (int)kp, INFINITY);
+    CKL();
+    h->kpad = (h->d + 63) / 64 * 64;
     __nv_bfloat16 *hi = nullptr, *lo = nullptr;
-    if (h->opts.precision != EMB200_PREC_FP32) {
-        h->kpad = (h->d + 63) / 64 * 64;
+    h->maps_ok = false;
+    if (h->kpad <= 256) {
+        // BF16 hi/lo split for the tensor-core search and refine passes.
         if (h->c_hi.ensure((size_t)k * h->kpad) || h->c_lo.ensure((size_t)k * h->kpad))
             return fail(h, EMB200_ENOMEM, "BF16 centroid allocation failed");
         hi = h->c_hi.p;
         lo = h->c_lo.p;
-        h->maps_ok = false;
         int rc = encode_bf16_map(h, &h->map_hi, hi);
         if (rc) return rc;
         rc = encode_bf16_map(h, &h->map_lo, lo);
         if (rc) return rc;
         h->maps_ok = true;
-    } else {
-        h->maps_ok = false;
-        h->kpad = (h->d + 63) / 64 * 64;
     }
     k_prep_centroids<<<(unsigned)((k + 7) / 8), 256, 0, st>>>(h->c.p, k, d, h->norms.p, h->bounds.p, hi, lo,
                                                               (int)h->kpad);
     CKL();
     if (h->opts.centroid_bits == EMB200_CENTROIDS_I8) {
-        size_t kp = (h->d + 31) / 32 * 32;
-        if (h->c8.ensure((size_t)k * kp) || h->off8.ensure(k)) return fail(h, EMB200_ENOMEM, "i8 centroid allocation failed");
-        k_prep_i8<<<(unsigned)((k + 7) / 8), 256, 0, st>>>(h->c.p, k, d, (int)kp, h->c8.p, h->off8.p);
+        size_t kp8 = (h->d + 31) / 32 * 32;
+        if (h->c8.ensure((size_t)k * kp8) || h->off8.ensure(k)) return fail(h, EMB200_ENOMEM, "i8 centroid allocation failed");
+        k_prep_i8<<<(unsigned)((k + 7) / 8), 256, 0, st>>>(h->c.p, k, d, (int)kp8, h->c8.p, h->off8.p);
         CKL();
     }
     h->bias_set = false;
@@ -265,14 +271,16 @@ int launch_i8_assign(emb200_handle* h, const int8_t* x, const uint32_t* gather, 
     return EMB200_OK;
 }
 
-int tc_terms(const emb200_handle* h, int dtype) {
-    if (h->opts.precision == EMB200_PREC_BF16X1) return 1;
+// Product terms of the tensor-core search: three for f32 rows (their BF16 split
+// has a low part), two for integer rows (exact in BF16), one for BF16X1.
+int tc_terms(int precision, int dtype) {
+    if (precision == EMB200_PREC_BF16X1) return 1;
     return dtype == EMB200_F32 ? 3 : 2;
 }
 
-bool tc_supported(const emb200_handle* h, int dtype) {
+bool tc_supported(const emb200_handle* h, int nterms) {
     if (!h->maps_ok) return false;
-    TcSmem L = tc_smem_layout((int)h->kpad, tc_terms(h, dtype));
+    TcSmem L = tc_smem_layout((int)h->kpad, nterms);
     return L.total + 1024 <= 227 * 1024;
 }
 
@@ -283,36 +291,61 @@ int tc_nsplit(const emb200_handle* h, size_t m) {
     return std::max(1, std::min(ntiles, (h->sm_count + row_tiles - 1) / row_tiles));
 }
 
-template <typename T>
-int launch_tc_assign(emb200_handle* h, const T* x, const uint32_t* gather, size_t m, int nsplit, cudaStream_t st) {
-    const int dtype = std::is_same<T, float>::value ? EMB200_F32 : (std::is_same<T, int8_t>::value ? EMB200_I8 : EMB200_U8);
-    TcParams p;
+template <typename T, bool COLLECT>
+int launch_tc(emb200_handle* h, const T* x, const uint32_t* gather, const uint32_t* gather2, size_t m, int nterms,
+              const float* theta, uint32_t* cand, uint32_t* cand_count, int cap, int* err, cudaStream_t st) {
+    TcParams p{};
     p.m = (int)m;
     p.d = (int)h->d;
     p.k = (int)h->k;
     p.kpad = (int)h->kpad;
-    p.nterms = tc_terms(h, dtype);
+    p.nterms = nterms;
     p.gather = gather;
+    p.gather2 = gather2;
     p.norms = h->norms.p;
     p.part_s = h->part_s.p;
     p.part_i = h->part_i.p;
-    p.err = (int*)(h->counters.p + 2);
+    p.err = err;
     p.xvec = (h->d % 4 == 0 && ((uintptr_t)x & 15) == 0) ? 1 : 0;
+    p.theta = theta;
+    p.cand = cand;
+    p.cand_count = cand_count;
+    p.cand_cap = cap;
     TcSmem L = tc_smem_layout(p.kpad, p.nterms);
     size_t smem = L.total + 1024;
-    static bool attr_set[3] = {false, false, false};
-    if (!attr_set[dtype]) {
-        CK(cudaFuncSetAttribute(k_assign_tc<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
-        attr_set[dtype] = true;
+    static bool attr_set = false;  // one flag per <T, COLLECT> instantiation
+    if (!attr_set) {
+        CK(cudaFuncSetAttribute(k_assign_tc<T, COLLECT>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
+        attr_set = true;
     }
+    int nsplit = tc_nsplit(h, m);
     dim3 grid((unsigned)((m + kTcBM - 1) / kTcBM), (unsigned)nsplit);
-    k_assign_tc<T><<<grid, kTcThreads, smem, st>>>(x, h->map_hi, h->map_lo, p);
+    k_assign_tc<T, COLLECT><<<grid, kTcThreads, smem, st>>>(x, h->map_hi, h->map_lo, p);
     CKL();
     return EMB200_OK;
 }
 
-// Full pipeline of one assign over m rows already on the device (x_dev, or
-// gathered through `gather`), results to device labels/dist.
+// Fold the device counters of one pipeline run into the handle's stats.
+int finish_counters(emb200_handle* h, cudaStream_t st, bool refined) {
+    uint32_t c[5];
+    CK(cudaMemcpyAsync(c, h->counters.p, sizeof c, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    h->stats.rows_certified += c[1];
+    h->stats.rows_researched += refined ? c[3] : c[0];
+    if (c[2] || c[4]) h->stats.fast_aborted = 1;
+    return EMB200_OK;
+}
+
+// Full pipeline of one assign over m rows already on the device (x, or
+// gathered through `gather`), results to device labels/dist:
+//   1. fast contraction (tcgen05 BF16 or FP32 SIMT): top-2 per row with an error bound
+//   2. certify: exact re-score of the two candidates; rows whose margin the bound
+//      certifies are final
+//   3. refine (uncertified rows): a three-term BF16 tensor-core pass collects every
+//      centroid whose score could reach the exact best, then exact re-score of those
+//   4. exhaustive exact search for rows the refine pass could not settle
+// Counters (device): [0] uncertified rows, [1] certified rows, [2] fast-kernel abort,
+// [3] exhaustive rows, [4] refine abort.
 template <typename T>
 int assign_rows_dev(emb200_handle* h, const T* x, const uint32_t* gather, size_t m, uint32_t* labels, float* dist,
                     cudaStream_t st) {
@@ -323,25 +356,28 @@ int assign_rows_dev(emb200_handle* h, const T* x, const uint32_t* gather, size_t
         h->stats.fast_kernel = 2;
         return launch_i8_assign(h, (const int8_t*)x, gather, m, labels, dist, st);
     }
-    int prec = h->opts.precision;
-    int row_tiles = (int)((m + kSimtBM - 1) / kSimtBM);
-    int ntiles = (k + kSimtBN - 1) / kSimtBN;
+    const int prec = h->opts.precision;
+    const int row_tiles = (int)((m + kSimtBM - 1) / kSimtBM);
+    const int ntiles = (k + kSimtBN - 1) / kSimtBN;
+    const int fast_terms = tc_terms(prec, dtype);
+    const int refine_terms = tc_terms(EMB200_PREC_BF16, dtype);
+    const bool tc = prec != EMB200_PREC_FP32 && tc_supported(h, fast_terms);
     int nsplit = 1;
-    bool tc = prec != EMB200_PREC_FP32 && tc_supported(h, dtype);
     if (tc) {
         nsplit = tc_nsplit(h, m);
     } else {
         int target = 2 * h->sm_count;
         if (row_tiles < target) nsplit = std::min(ntiles, (target + row_tiles - 1) / row_tiles);
     }
-    size_t mm = m;
-    if (h->part_s.ensure((size_t)nsplit * mm * 2) || h->part_i.ensure((size_t)nsplit * mm * 2) ||
-        h->redo_rows.ensure(mm) || h->counters.ensure(4))
+    if (h->part_s.ensure((size_t)nsplit * m * 2) || h->part_i.ensure((size_t)nsplit * m * 2) ||
+        h->redo_rows.ensure(m) || h->redo_theta.ensure(m) || h->counters.ensure(8))
         return fail(h, EMB200_ENOMEM, "scratch allocation failed for %zu rows", m);
-    CK(cudaMemsetAsync(h->counters.p, 0, 4 * sizeof(uint32_t), st));
+    uint32_t* ctr = h->counters.p;
+    CK(cudaMemsetAsync(ctr, 0, 8 * sizeof(uint32_t), st));
     h->stats.fast_kernel = tc ? 1 : 0;
     if (tc) {
-        int rc = launch_tc_assign(h, x, gather, m, nsplit, st);
+        int rc = launch_tc<T, false>(h, x, gather, nullptr, m, fast_terms, nullptr, nullptr, nullptr, 0,
+                                     (int*)(ctr + 2), st);
         if (rc) return rc;
     } else {
         dim3 grid(row_tiles, nsplit);
@@ -350,18 +386,43 @@ int assign_rows_dev(emb200_handle* h, const T* x, const uint32_t* gather, size_t
                                                          h->part_i.p, vec4);
         CKL();
     }
-    float ka, kb;
+    float ka, kb, ka2, kb2;
     bound_coefficients(tc ? prec : EMB200_PREC_FP32, dtype, h->d, &ka, &kb);
-    int match = h->opts.match_kernel;
+    bound_coefficients(EMB200_PREC_BF16, dtype, h->d, &ka2, &kb2);
+    const int match = h->opts.match_kernel;
     k_certify<T><<<(unsigned)((m + 7) / 8), 256, 0, st>>>(x, gather, (int)m, d, h->c.p, h->norms.p, k, h->part_s.p,
                                                            h->part_i.p, nsplit, h->bounds.p, ka, kb, match, labels,
-                                                           dist, h->redo_rows.p, h->counters.p, h->counters.p + 1,
-                                                           tc ? (const int*)(h->counters.p + 2) : nullptr);
+                                                           dist, h->redo_rows.p, ctr, ctr + 1,
+                                                           tc ? (const int*)(ctr + 2) : nullptr, h->redo_theta.p,
+                                                           ka2, kb2);
     CKL();
-    k_research<T><<<h->sm_count * 4, 256, 0, st>>>(x, gather, d, h->c.p, h->norms.p, k, match, h->redo_rows.p,
-                                                    h->counters.p, labels, dist);
+    uint32_t nredo = 0;
+    CK(cudaMemcpyAsync(&nredo, ctr, sizeof nredo, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    h->stats.rows_refined += nredo;
+    if (nredo == 0) return finish_counters(h, st, false);
+    const uint32_t* exhaustive = h->redo_rows.p;
+    const uint32_t* exhaustive_count = ctr;
+    if (tc_supported(h, refine_terms)) {
+        const int cap = kRefineCap;
+        if (h->cand.ensure((size_t)nredo * cap) || h->cand_count.ensure(nredo) || h->redo2_rows.ensure(nredo))
+            return fail(h, EMB200_ENOMEM, "refine allocation failed for %u rows", nredo);
+        CK(cudaMemsetAsync(h->cand_count.p, 0, nredo * sizeof(uint32_t), st));
+        int rc = launch_tc<T, true>(h, x, gather, h->redo_rows.p, nredo, refine_terms, h->redo_theta.p, h->cand.p,
+                                    h->cand_count.p, cap, (int*)(ctr + 4), st);
+        if (rc) return rc;
+        k_rescore_cands<T><<<(nredo + 7) / 8, 256, 0, st>>>(x, gather, d, h->c.p, h->norms.p, match, h->redo_rows.p,
+                                                           ctr, h->cand.p, h->cand_count.p, cap,
+                                                           (const int*)(ctr + 4), labels, dist, h->redo2_rows.p,
+                                                           ctr + 3);
+        CKL();
+        exhaustive = h->redo2_rows.p;
+        exhaustive_count = ctr + 3;
+    }
+    k_research_cta<T><<<h->sm_count * 2, 256, 0, st>>>(x, gather, d, h->c.p, h->norms.p, k, match, exhaustive,
+                                                        exhaustive_count, labels, dist);
     CKL();
-    return EMB200_OK;
+    return finish_counters(h, st, exhaustive_count == ctr + 3);
 }
 
 int assign_dispatch(emb200_handle* h, int dtype, const void* x, const uint32_t* gather, size_t m, uint32_t* labels,
@@ -397,7 +458,6 @@ int assign_host(emb200_handle* h, int dtype, const void* x, size_t m, uint32_t* 
     const size_t chunk = std::min(m, (size_t)1 << 20);
     if (h->stage.ensure(chunk * h->d * esz) || h->st_labels.ensure(chunk) || h->st_dist.ensure(chunk))
         return fail(h, EMB200_ENOMEM, "staging allocation failed");
-    uint32_t cert = 0, redo = 0;
     for (size_t r0 = 0; r0 < m; r0 += chunk) {
         size_t mc = std::min(chunk, m - r0);
         CK(cudaMemcpyAsync(h->stage.p, (const uint8_t*)x + r0 * h->d * esz, mc * h->d * esz, cudaMemcpyHostToDevice, st));
@@ -405,20 +465,14 @@ int assign_host(emb200_handle* h, int dtype, const void* x, size_t m, uint32_t* 
         if (rc) return rc;
         CK(cudaMemcpyAsync(labels + r0, h->st_labels.p, mc * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
         CK(cudaMemcpyAsync(dist + r0, h->st_dist.p, mc * sizeof(float), cudaMemcpyDeviceToHost, st));
-        uint32_t cnt[3] = {0, 0, 0};
-        if (!use_i8_mode(h, dtype)) CK(cudaMemcpyAsync(cnt, h->counters.p, sizeof cnt, cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
-        redo += cnt[0];
-        cert += cnt[1];
-        if (cnt[2]) h->stats.fast_aborted = 1;
     }
     CK(cudaEventRecord(h->ev1, st));
     CK(cudaEventSynchronize(h->ev1));
     float ms = 0;
     cudaEventElapsedTime(&ms, h->ev0, h->ev1);
     h->stats.rows = m;
-    h->stats.rows_certified = use_i8_mode(h, dtype) ? m : cert;
-    h->stats.rows_researched = redo;
+    if (use_i8_mode(h, dtype)) h->stats.rows_certified = m;
     h->stats.ms_total = ms;
     return EMB200_OK;
 }
@@ -459,6 +513,7 @@ int emb200_destroy(emb200_handle* h) {
     h->rows.release(); h->res_labels.release(); h->res_dist.release();
     h->stage.release(); h->st_labels.release(); h->st_dist.release();
     h->part_s.release(); h->part_i.release(); h->redo_rows.release(); h->counters.release();
+    h->redo_theta.release(); h->cand.release(); h->cand_count.release(); h->redo2_rows.release();
     h->train.release();
     if (h->ev0) cudaEventDestroy(h->ev0);
     if (h->ev1) cudaEventDestroy(h->ev1);
@@ -506,7 +561,7 @@ int emb200_set_centroids(emb200_handle* h, const float* centroids, size_t k, siz
     if (!centroids || k == 0 || d == 0) return fail(h, EMB200_EINVAL, "centroids must be a non-empty k x d array");
     if (k > 0x7FFFFFFF || d > 0x7FFFFFFF) return fail(h, EMB200_EINVAL, "k and d must fit in 31 bits");
     CK(cudaSetDevice(h->device));
-    if (h->c.ensure(k * d) || h->norms.ensure(k) || h->bias.ensure(k))
+    if (h->c.ensure(k * d) || h->norms.ensure((k + kTcBN - 1) / kTcBN * kTcBN) || h->bias.ensure(k))
         return fail(h, EMB200_ENOMEM, "centroid allocation failed");
     h->k = k;
     h->d = d;
@@ -579,17 +634,13 @@ int emb200_assign_resident(emb200_handle* h, uint32_t* labels, float* dist) {
     rc = assign_dispatch(h, h->rows_dtype, h->rows.p, nullptr, h->rows_n, h->res_labels.p, h->res_dist.p, st);
     if (rc) return rc;
     CK(cudaEventRecord(h->ev1, st));
-    uint32_t cnt[3] = {0, 0, 0};
-    if (!use_i8_mode(h, h->rows_dtype)) CK(cudaMemcpyAsync(cnt, h->counters.p, sizeof cnt, cudaMemcpyDeviceToHost, st));
     if (labels) CK(cudaMemcpyAsync(labels, h->res_labels.p, h->rows_n * 4, cudaMemcpyDeviceToHost, st));
     if (dist) CK(cudaMemcpyAsync(dist, h->res_dist.p, h->rows_n * 4, cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
     float ms = 0;
     cudaEventElapsedTime(&ms, h->ev0, h->ev1);
     h->stats.rows = h->rows_n;
-    h->stats.rows_certified = use_i8_mode(h, h->rows_dtype) ? h->rows_n : cnt[1];
-    h->stats.rows_researched = cnt[0];
-    h->stats.fast_aborted = cnt[2] ? 1 : 0;
+    if (use_i8_mode(h, h->rows_dtype)) h->stats.rows_certified = h->rows_n;
     h->stats.ms_total = ms;
     return EMB200_OK;
 }

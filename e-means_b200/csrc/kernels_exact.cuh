@@ -124,6 +124,11 @@ __global__ void k_prep_centroids(const float* __restrict__ c, int k, int d, floa
     }
 }
 
+__global__ void k_fill(float* __restrict__ p, int n, float v) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) p[i] = v;
+}
+
 // set_bias (src/cpu.rs:95-99): norms_j += bias_j, and refresh nmax.
 __global__ void k_add_bias(float* __restrict__ norms, const float* __restrict__ bias, int k, Bounds* bounds) {
     int j = blockIdx.x * blockDim.x + threadIdx.x;
@@ -147,7 +152,8 @@ __global__ void k_certify(const T* __restrict__ x, const uint32_t* __restrict__ 
                           const Bounds* __restrict__ bounds, float ka, float kb, int match,
                           uint32_t* __restrict__ labels, float* __restrict__ dist,
                           uint32_t* __restrict__ redo_rows, uint32_t* __restrict__ redo_count,
-                          uint32_t* __restrict__ cert_count, const int* __restrict__ fast_err) {
+                          uint32_t* __restrict__ cert_count, const int* __restrict__ fast_err,
+                          float* __restrict__ redo_theta, float ka2, float kb2) {
     int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     int lane = threadIdx.x & 31;
     if (row >= m) return;
@@ -195,8 +201,144 @@ __global__ void k_certify(const T* __restrict__ x, const uint32_t* __restrict__ 
         dist[row] = fmaxf(__fadd_rn(sb, xn), 0.0f);
         atomicAdd(cert_count, 1u);
     } else {
+        // Threshold for the refine pass: the reference's best j* has s_j* <= sb,
+        // so its refine-pass score is <= sb + E2. Non-finite: no candidates, so
+        // the row is searched exhaustively.
+        float theta = __int_as_float(0x7fc00000);
+        if (t.i1 < (uint32_t)k && sb < __int_as_float(0x7f800000) && sb > -__int_as_float(0x7f800000)) {
+            float xnorm = __fmul_ru(__fsqrt_ru(fmaxf(xn, 0.0f)), 1.0000005f);
+            float E2 = __fadd_ru(__fmul_ru(__fmul_ru(ka2, xnorm), bounds->cmax), __fmul_ru(kb2, bounds->nmax));
+            float th = __fadd_ru(sb, E2);
+            if (isfinite(th)) theta = th;
+        }
         uint32_t slot = atomicAdd(redo_count, 1u);
         redo_rows[slot] = (uint32_t)row;
+        redo_theta[slot] = theta;
+    }
+}
+
+// Exact re-score of the refine pass's candidates (one warp per refined row):
+// the reference's label is the lowest-index minimum of the exact scores of the
+// candidates, because every centroid whose exact score could reach sb was
+// collected. Rows with no candidates or more than cap go to the exhaustive list.
+template <typename T>
+__global__ void k_rescore_cands(const T* __restrict__ x, const uint32_t* __restrict__ gather, int d,
+                                const float* __restrict__ c, const float* __restrict__ norms, int match,
+                                const uint32_t* __restrict__ redo_rows, const uint32_t* __restrict__ redo_count,
+                                const uint32_t* __restrict__ cand, const uint32_t* __restrict__ cand_count, int cap,
+                                const int* __restrict__ refine_err, uint32_t* __restrict__ labels,
+                                float* __restrict__ dist, uint32_t* __restrict__ redo2_rows,
+                                uint32_t* __restrict__ redo2_count) {
+    int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    int lane = threadIdx.x & 31;
+    if (i >= (int)*redo_count) return;
+    uint32_t row = redo_rows[i];
+    uint32_t cnt = cand_count[i];
+    if (cnt == 0 || cnt > (uint32_t)cap || *refine_err) {
+        if (lane == 0) redo2_rows[atomicAdd(redo2_count, 1u)] = row;
+        return;
+    }
+    size_t src = gather ? gather[row] : (size_t)row;
+    const T* xr = x + src * (size_t)d;
+    const int gsz = match == kMatchAvx512 ? 16 : 8;
+    const int ngroups = 32 / gsz, g = lane / gsz;
+    float best = __int_as_float(0x7f800000);
+    uint32_t lab = 0xffffffffu;
+    for (uint32_t c0 = 0; c0 < cnt; c0 += ngroups) {
+        uint32_t ci = c0 + g < cnt ? c0 + g : cnt - 1;
+        uint32_t j = cand[(size_t)i * cap + ci];
+        float dg = group_dot_ref(match, xr, c + (size_t)j * d, d, lane);
+        float s = score_ref(norms[j], dg);
+        if (lex_less(s, j, best, lab)) {
+            best = s;
+            lab = j;
+        }
+    }
+    for (int q = 1; q < ngroups; q++) {
+        float ob = __shfl_sync(kFull, best, q * gsz);
+        uint32_t ol = __shfl_sync(kFull, lab, q * gsz);
+        if (lex_less(ob, ol, best, lab)) {
+            best = ob;
+            lab = ol;
+        }
+    }
+    float xn = warp_sqnorm_ref(xr, d, lane);
+    if (lane == 0) {
+        if (best < __int_as_float(0x7f800000)) {
+            labels[row] = lab;
+            dist[row] = fmaxf(__fadd_rn(best, xn), 0.0f);
+        } else {
+            redo2_rows[atomicAdd(redo2_count, 1u)] = row;
+        }
+    }
+}
+
+// Exhaustive exact search with one CTA per row (persistent over the list):
+// 8 warps x (32 / G) lane groups score interleaved centroids, two per group in
+// flight, then the groups are merged in (score, index) order.
+template <typename T>
+__global__ void __launch_bounds__(256) k_research_cta(const T* __restrict__ x, const uint32_t* __restrict__ gather,
+                                                      int d, const float* __restrict__ c,
+                                                      const float* __restrict__ norms, int k, int match,
+                                                      const uint32_t* __restrict__ rows,
+                                                      const uint32_t* __restrict__ count,
+                                                      uint32_t* __restrict__ labels, float* __restrict__ dist) {
+    __shared__ float sb[32];
+    __shared__ uint32_t sl[32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int gsz = match == kMatchAvx512 ? 16 : 8;
+    const int gpw = 32 / gsz;                 // groups per warp
+    const int G = 8 * gpw;                    // groups per CTA
+    const int g = warp * gpw + lane / gsz;    // this lane's group
+    const uint32_t n = *count;
+    for (uint32_t r = blockIdx.x; r < n; r += gridDim.x) {
+        uint32_t row = rows[r];
+        size_t src = gather ? gather[row] : (size_t)row;
+        const T* xr = x + src * (size_t)d;
+        float best = __int_as_float(0x7f800000);
+        uint32_t lab = 0;
+        for (int j0 = 0; j0 < k; j0 += 2 * G) {
+            int ja = j0 + g, jb = j0 + G + g;
+            int jac = ja < k ? ja : k - 1, jbc = jb < k ? jb : k - 1;
+            float da = group_dot_ref(match, xr, c + (size_t)jac * d, d, lane);
+            float db = group_dot_ref(match, xr, c + (size_t)jbc * d, d, lane);
+            if (ja < k) {
+                float s = score_ref(norms[ja], da);
+                if (s < best) {
+                    best = s;
+                    lab = (uint32_t)ja;
+                }
+            }
+            if (jb < k) {
+                float s = score_ref(norms[jb], db);
+                if (s < best) {
+                    best = s;
+                    lab = (uint32_t)jb;
+                }
+            }
+        }
+        // A group that never beat +inf reports (inf, 0): it loses to any finite
+        // score, and if every group is at +inf the reference's label 0 results.
+        if ((lane & (gsz - 1)) == 0) {
+            sb[g] = best;
+            sl[g] = best < __int_as_float(0x7f800000) ? lab : 0u;
+        }
+        __syncthreads();
+        if (warp == 0) {
+            float rb = __int_as_float(0x7f800000);
+            uint32_t rl = 0;
+            for (int q = 0; q < G; q++)
+                if (sb[q] < __int_as_float(0x7f800000) && lex_less(sb[q], sl[q], rb, rl)) {
+                    rb = sb[q];
+                    rl = sl[q];
+                }
+            float xn = warp_sqnorm_ref(xr, d, lane);
+            if (lane == 0) {
+                labels[row] = rl;
+                dist[row] = fmaxf(__fadd_rn(rb, xn), 0.0f);
+            }
+        }
+        __syncthreads();
     }
 }
 

@@ -7,9 +7,11 @@
 //   warp 0      TMA producer: centroid tiles (BF16 hi and lo parts, 128B swizzle)
 //               into a 2-stage shared-memory ring
 //   warp 1      allocates TMEM, issues tcgen05.mma (one thread), commits to mbarriers
-//   warps 2..5  epilogue: tcgen05.ld of a 128 x 128 FP32 accumulator, score =
-//               norm - 2 acc, running top-2 per row; two accumulators in TMEM so
-//               the epilogue of tile t overlaps the MMAs of tile t+1
+//   warps 2..9  epilogue: tcgen05.ld of a 128 x 128 FP32 accumulator (two warps per
+//               TMEM lane quarter, one per column half), score = norm - 2 acc with the
+//               tile's norms from shared memory, running top-2 per row with one branch
+//               per 32 columns; two accumulators in TMEM so the epilogue of tile t
+//               overlaps the MMAs of tile t+1
 // The row tile is converted once per CTA (f32 -> BF16 hi + lo) by all threads
 // and stays resident in shared memory for the whole centroid walk.
 //
@@ -27,7 +29,8 @@ namespace emb {
 constexpr int kTcBM = 128;       // rows per CTA (TMEM lanes)
 constexpr int kTcBN = 128;       // centroids per tile (accumulator columns)
 constexpr int kTcStages = 2;     // centroid-tile ring depth
-constexpr int kTcThreads = 192;  // 6 warps
+constexpr int kTcEpiWarps = 8;   // two warps per TMEM lane quarter (column halves)
+constexpr int kTcThreads = 64 + kTcEpiWarps * 32;  // producer, MMA, epilogue warps
 constexpr int kTcTmemCols = 256; // two 128-column accumulators
 
 struct TcParams {
@@ -39,6 +42,11 @@ struct TcParams {
     uint32_t* part_i;
     int* err;            // set to 1 if a wait gave up (results then re-searched exactly)
     int xvec;            // rows are 16-byte aligned f32 with d % 4 == 0: vector loads
+    const uint32_t* gather2;  // optional first-level row map (kernel row -> batch row)
+    const float* theta;       // COLLECT: per kernel row, collect scores <= theta
+    uint32_t* cand;           // COLLECT: [m][cand_cap] centroid indices
+    uint32_t* cand_count;     // COLLECT: [m] candidates found (may exceed cand_cap)
+    int cand_cap;
 };
 
 // ---- PTX wrappers -----------------------------------------------------------
@@ -153,8 +161,10 @@ EMB_DEV uint32_t sw128_offset(int r, int kc, int rows) {
 
 struct TcSmem {
     // Offsets (bytes) inside the dynamic shared memory block (1024-aligned base).
-    uint32_t a_hi, a_lo, b0, stage_bytes, term_bytes, bars, total;
+    uint32_t a_hi, a_lo, b0, stage_bytes, term_bytes, norms, merge, bars, total;
 };
+
+constexpr int kTcNormSlots = 4;  // norms ring: slot t % 4 is refilled only after tile t's epilogue
 
 __host__ __device__ inline TcSmem tc_smem_layout(int kpad, int nterms) {
     TcSmem s;
@@ -167,7 +177,9 @@ __host__ __device__ inline TcSmem tc_smem_layout(int kpad, int nterms) {
     s.b0 = a_total;
     s.term_bytes = b_term;
     s.stage_bytes = b_term * bterms;
-    s.bars = s.b0 + kTcStages * s.stage_bytes;
+    s.norms = s.b0 + kTcStages * s.stage_bytes;            // [4][128] f32
+    s.merge = s.norms + kTcNormSlots * kTcBN * 4;          // [128] x (s1, i1, s2, i2)
+    s.bars = s.merge + kTcBM * 16;
     s.total = s.bars + 256;
     return s;
 }
@@ -182,7 +194,8 @@ EMB_DEV void tc_load_rows(uint8_t* smem, const TcSmem& L, const T* __restrict__ 
         int g = row0 + r;
         float v[8];
         if (g < p.m) {
-            size_t src = p.gather ? p.gather[g] : (size_t)g;
+            size_t src = p.gather2 ? (size_t)p.gather2[g] : (size_t)g;
+            if (p.gather) src = p.gather[src];
             const T* xr = x + src * (size_t)p.d;
             int k0 = kc * 8;
             if (sizeof(T) == 4 && p.xvec && k0 + 8 <= p.d) {
@@ -212,26 +225,67 @@ EMB_DEV void tc_load_rows(uint8_t* smem, const TcSmem& L, const T* __restrict__ 
     }
 }
 
+EMB_DEV void bulk_load(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                 ::"r"(smem_u32(dst)), "l"((uint64_t)src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+
+EMB_DEV float min3f(float a, float b, float c) {
+    float r;
+    asm("min.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+    return r;
+}
+
+// Scores of 32 accumulator columns: s = norm - 2 acc (one rounding); returns their minimum.
+EMB_DEV float tc_scores32(const uint32_t (&v)[32], const float* __restrict__ nrm, float (&s)[32]) {
+#pragma unroll
+    for (int j = 0; j < 32; j += 4) {
+        float4 n4 = *reinterpret_cast<const float4*>(nrm + j);
+        s[j] = __fmaf_rn(-2.0f, __uint_as_float(v[j]), n4.x);
+        s[j + 1] = __fmaf_rn(-2.0f, __uint_as_float(v[j + 1]), n4.y);
+        s[j + 2] = __fmaf_rn(-2.0f, __uint_as_float(v[j + 2]), n4.z);
+        s[j + 3] = __fmaf_rn(-2.0f, __uint_as_float(v[j + 3]), n4.w);
+    }
+    float m[11];
+#pragma unroll
+    for (int i = 0; i < 10; i++) m[i] = min3f(s[3 * i], s[3 * i + 1], s[3 * i + 2]);
+    m[10] = fminf(s[30], s[31]);
+    float a = min3f(m[0], m[1], m[2]), b = min3f(m[3], m[4], m[5]), c = min3f(m[6], m[7], m[8]);
+    return min3f(min3f(a, b, c), m[9], m[10]);
+}
+
+// Keep the compiler from reading registers of a tcgen05.ld before its wait.
+EMB_DEV void tc_regs_ready(uint32_t (&v)[32]) {
+#pragma unroll
+    for (int j = 0; j < 32; j++) asm volatile("" : "+r"(v[j]));
+}
+
 // Grid: (ceil(m / 128), nsplit); CTA (bx, by) walks centroid tiles by, by + nsplit, ...
-template <typename T>
+// COLLECT = false: per-row top-2 of approximate scores to part_s/part_i.
+// COLLECT = true : every centroid with approximate score <= theta[row] is appended
+//                  to cand[row][*] (cand_count[row] counts all, capped storage).
+template <typename T, bool COLLECT>
 __global__ void __launch_bounds__(kTcThreads, 1)
 k_assign_tc(const T* __restrict__ x, const __grid_constant__ CUtensorMap map_hi,
             const __grid_constant__ CUtensorMap map_lo, const TcParams p) {
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
     const TcSmem L = tc_smem_layout(p.kpad, p.nterms);
-    uint64_t* full = (uint64_t*)(smem + L.bars);         // [kTcStages]
-    uint64_t* empty = full + kTcStages;                  // [kTcStages]
-    uint64_t* acc_full = empty + kTcStages;              // [2]
-    uint64_t* acc_empty = acc_full + 2;                  // [2]
-    uint32_t* tmem_slot = (uint32_t*)(acc_empty + 2);
+    uint64_t* full = (uint64_t*)(smem + L.bars);          // [kTcStages]
+    uint64_t* empty = full + kTcStages;                   // [kTcStages]
+    uint64_t* acc_full = empty + kTcStages;               // [2]
+    uint64_t* acc_empty = acc_full + 2;                   // [2]
+    uint64_t* norms_full = acc_empty + 2;                 // [kTcNormSlots]
+    uint32_t* tmem_slot = (uint32_t*)(norms_full + kTcNormSlots);
     volatile int* abort_flag = (volatile int*)(tmem_slot + 1);
+    float* norms_s = (float*)(smem + L.norms);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int row0 = blockIdx.x * kTcBM;
     const int nsplit = gridDim.y;
     const int ntiles_all = (p.k + kTcBN - 1) / kTcBN;
-    const int my_tiles = blockIdx.y < ntiles_all ? (ntiles_all - blockIdx.y + nsplit - 1) / nsplit : 0;
+    const int my_tiles = (int)blockIdx.y < ntiles_all ? (ntiles_all - (int)blockIdx.y + nsplit - 1) / nsplit : 0;
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < kTcStages; s++) {
@@ -240,8 +294,9 @@ k_assign_tc(const T* __restrict__ x, const __grid_constant__ CUtensorMap map_hi,
         }
         for (int b = 0; b < 2; b++) {
             mbar_init(&acc_full[b], 1);
-            mbar_init(&acc_empty[b], 4);  // one arrival per epilogue warp
+            mbar_init(&acc_empty[b], kTcEpiWarps);  // one arrival per epilogue warp
         }
+        for (int i = 0; i < kTcNormSlots; i++) mbar_init(&norms_full[i], 1);
         *abort_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
@@ -255,7 +310,7 @@ k_assign_tc(const T* __restrict__ x, const __grid_constant__ CUtensorMap map_hi,
 
     if (warp == 0) {
         if (lane == 0) {
-            // ---- TMA producer
+            // ---- TMA producer: centroid tiles into the stage ring, their norms into the norms ring
             int issued = 0;
             for (int t = 0; t < my_tiles; t++) {
                 int s = t % kTcStages;
@@ -269,16 +324,20 @@ k_assign_tc(const T* __restrict__ x, const __grid_constant__ CUtensorMap map_hi,
                     if (p.nterms > 1)
                         tma_load_2d(stage + L.term_bytes + a * (kTcBN * 128), &map_lo, &full[s], a * 64, tile * kTcBN);
                 }
+                int ns = t % kTcNormSlots;
+                mbar_expect_tx(&norms_full[ns], kTcBN * 4);
+                bulk_load(norms_s + ns * kTcBN, p.norms + (size_t)tile * kTcBN, kTcBN * 4, &norms_full[ns]);
                 issued = t + 1;
             }
-            // After an abort, let the copies still in flight (the last stages
-            // issued) land before the CTA exits; bounded like every wait.
+            // After an abort, let the copies still in flight land before the CTA
+            // exits; bounded like every wait.
             if (*abort_flag) {
                 for (int t = issued > kTcStages ? issued - kTcStages : 0; t < issued; t++) {
-                    int s = t % kTcStages;
-                    uint32_t ph = (uint32_t)(t / kTcStages) & 1u;
+                    uint32_t ph = (uint32_t)(t / kTcStages) & 1u, nph = (uint32_t)(t / kTcNormSlots) & 1u;
                     const uint64_t t0 = global_ns();
-                    while (!mbar_try(&full[s], ph) && global_ns() - t0 < kWaitLimitNs) {
+                    while (!mbar_try(&full[t % kTcStages], ph) && global_ns() - t0 < kWaitLimitNs) {
+                    }
+                    while (!mbar_try(&norms_full[t % kTcNormSlots], nph) && global_ns() - t0 < kWaitLimitNs) {
                     }
                 }
             }
@@ -316,36 +375,51 @@ k_assign_tc(const T* __restrict__ x, const __grid_constant__ CUtensorMap map_hi,
             }
         }
     } else {
-        // ---- epilogue: warps 2..5, thread = row (TMEM lane)
+        // ---- epilogue: warps 2..9. Thread = row (TMEM lane); warps 2..5 take
+        // columns 0..63 of each tile, warps 6..9 columns 64..127.
         const int q = warp & 3;  // TMEM lane quarter this warp may access
+        const int h = (warp - 2) >> 2;
         const int r = q * 32 + lane;
+        const int row = row0 + r;
         Top2 top;
         top.init();
+        float theta = 0.0f;
+        if (COLLECT) theta = row < p.m ? p.theta[row] : __int_as_float(0x7fc00000);
         for (int t = 0; t < my_tiles; t++) {
             int b = t & 1;
             uint32_t bph = (uint32_t)(t >> 1) & 1u;
             if (!mbar_wait(&acc_full[b], bph, abort_flag)) break;
+            if (!mbar_wait(&norms_full[t % kTcNormSlots], (uint32_t)(t / kTcNormSlots) & 1u, abort_flag)) break;
             tc_fence_after();
-            const int col0 = (blockIdx.y + t * nsplit) * kTcBN;
-            const uint32_t taddr = tmem_base + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * kTcBN);
-#pragma unroll 1
-            for (int ch = 0; ch < kTcBN / 32; ch++) {
-                uint32_t v[32];
-                EMB_TMEM_LD32(taddr + ch * 32, v);
-                tmem_wait_ld();
-                const int cbase = col0 + ch * 32;
-                if (cbase + 32 <= p.k) {
+            const int colh = (blockIdx.y + t * nsplit) * kTcBN + h * 64;
+            const float* nrm = norms_s + (t % kTcNormSlots) * kTcBN + h * 64;
+            const uint32_t taddr = tmem_base + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * kTcBN + h * 64);
+            uint32_t va[32], vb[32];
+            float s[32];
+            EMB_TMEM_LD32(taddr, va);
+            tmem_wait_ld();
+            tc_regs_ready(va);
+            EMB_TMEM_LD32(taddr + 32, vb);  // in flight while the first chunk is scored
 #pragma unroll
-                    for (int j = 0; j < 32; j++) {
-                        float s = __fmaf_rn(-2.0f, __uint_as_float(v[j]), __ldg(&p.norms[cbase + j]));
-                        if (s < top.s2) top.push(s, (uint32_t)(cbase + j));
+            for (int ch = 0; ch < 2; ch++) {
+                if (ch == 1) {
+                    tmem_wait_ld();
+                    tc_regs_ready(vb);
+                }
+                float mn = tc_scores32(ch == 0 ? va : vb, nrm + ch * 32, s);
+                const int cb = colh + ch * 32;
+                if (!COLLECT) {
+                    if (mn < top.s2) {
+#pragma unroll
+                        for (int j = 0; j < 32; j++)
+                            if (s[j] < top.s2) top.push(s[j], (uint32_t)(cb + j));
                     }
-                } else {
+                } else if (mn <= theta) {
 #pragma unroll
                     for (int j = 0; j < 32; j++) {
-                        if (cbase + j < p.k) {
-                            float s = __fmaf_rn(-2.0f, __uint_as_float(v[j]), __ldg(&p.norms[cbase + j]));
-                            if (s < top.s2) top.push(s, (uint32_t)(cbase + j));
+                        if (s[j] <= theta && cb + j < p.k) {
+                            uint32_t slot = atomicAdd(&p.cand_count[row], 1u);
+                            if (slot < (uint32_t)p.cand_cap) p.cand[(size_t)row * p.cand_cap + slot] = (uint32_t)(cb + j);
                         }
                     }
                 }
@@ -354,13 +428,29 @@ k_assign_tc(const T* __restrict__ x, const __grid_constant__ CUtensorMap map_hi,
             __syncwarp();
             if (lane == 0) mbar_arrive(&acc_empty[b]);
         }
-        const int row = row0 + r;
-        if (row < p.m) {
-            size_t o = ((size_t)blockIdx.y * p.m + row) * 2;
-            p.part_s[o] = top.s1;
-            p.part_i[o] = top.i1;
-            p.part_s[o + 1] = top.s2;
-            p.part_i[o + 1] = top.i2;
+        if (!COLLECT) {
+            // Merge the two column halves of each row through shared memory.
+            uint32_t* mg = (uint32_t*)(smem + L.merge) + r * 4;
+            if (h == 1) {
+                mg[0] = __float_as_uint(top.s1);
+                mg[1] = top.i1;
+                mg[2] = __float_as_uint(top.s2);
+                mg[3] = top.i2;
+            }
+            asm volatile("bar.sync 1, %0;" ::"n"(kTcEpiWarps * 32) : "memory");
+            if (h == 0 && row < p.m) {
+                Top2 o;
+                o.s1 = __uint_as_float(mg[0]);
+                o.i1 = mg[1];
+                o.s2 = __uint_as_float(mg[2]);
+                o.i2 = mg[3];
+                top.merge(o);
+                size_t oo = ((size_t)blockIdx.y * p.m + row) * 2;
+                p.part_s[oo] = top.s1;
+                p.part_i[oo] = top.i1;
+                p.part_s[oo + 1] = top.s2;
+                p.part_i[oo + 1] = top.i2;
+            }
         }
     }
     tc_fence_before();

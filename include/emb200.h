@@ -92,11 +92,12 @@ typedef struct {
 typedef struct {
     uint64_t rows;           /* rows searched */
     uint64_t rows_certified; /* rows whose fast top-2 the error bound certified */
-    uint64_t rows_researched; /* rows searched again with exact arithmetic */
+    uint64_t rows_researched; /* rows searched exhaustively with exact arithmetic */
     uint64_t kernel_launches; /* kernels launched by the call */
     double ms_total;          /* device time of the call (CUDA events) */
     int32_t fast_kernel;      /* fast contraction used: 0 FP32 SIMT, 1 tcgen05 BF16, 2 exact int8 */
     int32_t fast_aborted;     /* 1 if a bounded wait in the fast kernel gave up (rows then re-searched) */
+    uint64_t rows_refined;    /* uncertified rows sent through the candidate-collecting refine pass */
 } emb200_stats;
 
 /* ---- lifecycle ---------------------------------------------------------- */
