@@ -137,7 +137,7 @@ size_t elt_size(int dtype) { return dtype == EMB200_F32 ? 4 : 1; }
 // Error-bound coefficients of the certification, E = ka |x| cmax + kb nmax
 // (see k_certify). u = 2^-24 (f32 rounding), ub = 2^-9 (bf16 rounding); the
 // tensor-core accumulation is allowed one f32 truncation (2u) per product term.
-void bound_coefficients(int precision, int dtype, size_t d, float* ka, float* kb) {
+void bound_coefficients(int precision, int dtype, size_t d, bool packed, float* ka, float* kb) {
     const double u = std::ldexp(1.0, -24), ub = std::ldexp(1.0, -9);
     auto gamma = [](double n, double unit) { return n * unit / (1.0 - n * unit); };
     double g_ref = gamma((double)d + 2, u);  // reference dot vs exact
@@ -152,8 +152,14 @@ void bound_coefficients(int precision, int dtype, size_t d, float* ka, float* kb
         double rep = dtype == EMB200_F32 ? 2.0 * ub + ub * ub : ub;
         a = 2.0 * (rep + 1.02 * gamma((double)d + 2, 2 * u) + g_ref) + 4.02 * u;
     }
+    double b = 2.0 * u;
+    if (packed) {  // tensor-core top-2 keys carry the column in 5 mantissa bits: |key - s| <= 2^-18 |s|
+        const double t = std::ldexp(1.0, -18);
+        a += 2.01 * t;
+        b += t;
+    }
     *ka = (float)(1.25 * a);
-    *kb = (float)(1.25 * 2.0 * u);
+    *kb = (float)(1.25 * b);
 }
 
 bool use_i8_mode(const emb200_handle* h, int dtype) {
@@ -180,7 +186,7 @@ EncodeTiledFn encode_tiled_fn() {
     return fn;
 }
 
-// 2-D map over a k x kpad BF16 matrix (row stride kpad), boxes of 64 x 128
+// 2-D map over a k x kpad BF16 matrix (row stride kpad), boxes of 64 x 256
 // (one 128-byte swizzle atom wide); rows past k read as zeros.
 int encode_bf16_map(emb200_handle* h, CUtensorMap* map, void* base) {
     EncodeTiledFn fn = encode_tiled_fn();
@@ -202,9 +208,10 @@ int prepare_centroids(emb200_handle* h) {
     cudaStream_t st = h->stream;
     const int k = (int)h->k, d = (int)h->d;
     CK(cudaMemsetAsync(h->bounds.p, 0, sizeof(Bounds), st));
-    // Norms are padded to whole 128-centroid tiles with +inf (never a candidate).
+    // Norms are padded to whole tiles with 3e38 (never a candidate, and finite
+    // so the packed top-2 keys of the padding stay numbers).
     const size_t kp = (h->k + kTcBN - 1) / kTcBN * kTcBN;
-    k_fill<<<(unsigned)((kp + 255) / 256), 256, 0, st>>>(h->norms.p, (int)kp, INFINITY);
+    k_fill<<<(unsigned)((kp + 255) / 256), 256, 0, st>>>(h->norms.p, (int)kp, 3.0e38f);
     CKL();
     h->kpad = (h->d + 63) / 64 * 64;
     __nv_bfloat16 *hi = nullptr, *lo = nullptr;
@@ -281,7 +288,7 @@ int tc_terms(int precision, int dtype) {
 bool tc_supported(const emb200_handle* h, int nterms) {
     if (!h->maps_ok) return false;
     TcSmem L = tc_smem_layout((int)h->kpad, nterms);
-    return L.total + 1024 <= 227 * 1024;
+    return L.stages >= 2 && L.total + 1024 <= (uint32_t)kTcSmemLimit;
 }
 
 int tc_nsplit(const emb200_handle* h, size_t m) {
@@ -312,7 +319,8 @@ int launch_tc(emb200_handle* h, const T* x, const uint32_t* gather, const uint32
     p.cand_count = cand_count;
     p.cand_cap = cap;
     TcSmem L = tc_smem_layout(p.kpad, p.nterms);
-    size_t smem = L.total + 1024;
+    // At least 120 KB so that two CTAs never share an SM: each holds all 512 TMEM columns.
+    size_t smem = std::max<size_t>(L.total + 1024, 120 * 1024);
     static bool attr_set = false;  // one flag per <T, COLLECT> instantiation
     if (!attr_set) {
         CK(cudaFuncSetAttribute(k_assign_tc<T, COLLECT>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
@@ -387,8 +395,8 @@ int assign_rows_dev(emb200_handle* h, const T* x, const uint32_t* gather, size_t
         CKL();
     }
     float ka, kb, ka2, kb2;
-    bound_coefficients(tc ? prec : EMB200_PREC_FP32, dtype, h->d, &ka, &kb);
-    bound_coefficients(EMB200_PREC_BF16, dtype, h->d, &ka2, &kb2);
+    bound_coefficients(tc ? prec : EMB200_PREC_FP32, dtype, h->d, tc, &ka, &kb);
+    bound_coefficients(EMB200_PREC_BF16, dtype, h->d, false, &ka2, &kb2);
     const int match = h->opts.match_kernel;
     k_certify<T><<<(unsigned)((m + 7) / 8), 256, 0, st>>>(x, gather, (int)m, d, h->c.p, h->norms.p, k, h->part_s.p,
                                                            h->part_i.p, nsplit, h->bounds.p, ka, kb, match, labels,

@@ -3,15 +3,18 @@
 // m x k score matrix reaches HBM.
 //
 // One CTA owns 128 rows (one TMEM lane per row) and walks its share of the
-// centroid tiles (128 centroids each):
-//   warp 0      TMA producer: centroid tiles (BF16 hi and lo parts, 128B swizzle)
-//               into a 2-stage shared-memory ring
-//   warp 1      allocates TMEM, issues tcgen05.mma (one thread), commits to mbarriers
-//   warps 2..9  epilogue: tcgen05.ld of a 128 x 128 FP32 accumulator (two warps per
-//               TMEM lane quarter, one per column half), score = norm - 2 acc with the
-//               tile's norms from shared memory, running top-2 per row with one branch
-//               per 32 columns; two accumulators in TMEM so the epilogue of tile t
-//               overlaps the MMAs of tile t+1
+// centroid tiles (256 centroids each, one 128 x 256 FP32 accumulator in TMEM):
+//   warp 0       TMA producer: each stage holds one 64-wide K slice (a 128-byte
+//                swizzle atom) of a tile's BF16 hi and lo parts; stages ring
+//                through as much shared memory as is left (2..4 stages)
+//   warp 1       allocates TMEM, issues tcgen05.mma M=128 N=256 K=16 (one thread),
+//                commits to mbarriers
+//   warps 2..17  epilogue: four warps per TMEM lane quarter, each owning 64
+//                columns of the tile: tcgen05.ld, score = norm - 2 acc (packed
+//                f32x2 FMA, norms staged in shared memory by a bulk copy),
+//                branch-free top-2 of each 32 columns merged into a running top-2
+//                per row. Two accumulators (512 TMEM columns) let the epilogue of
+//                tile t overlap the MMAs of tile t+1.
 // The row tile is converted once per CTA (f32 -> BF16 hi + lo) by all threads
 // and stays resident in shared memory for the whole centroid walk.
 //
@@ -26,18 +29,24 @@
 
 namespace emb {
 
-constexpr int kTcBM = 128;       // rows per CTA (TMEM lanes)
-constexpr int kTcBN = 128;       // centroids per tile (accumulator columns)
-constexpr int kTcStages = 2;     // centroid-tile ring depth
-constexpr int kTcEpiWarps = 8;   // two warps per TMEM lane quarter (column halves)
+constexpr int kTcBM = 128;        // rows per CTA (TMEM lanes)
+constexpr int kTcBN = 256;        // centroids per tile (accumulator columns, MMA N)
+constexpr int kTcMaxStages = 4;   // stage ring depth limit (one K atom of a tile per stage)
+constexpr int kTcEpiWarps = 16;   // four warps per TMEM lane quarter
 constexpr int kTcThreads = 64 + kTcEpiWarps * 32;  // producer, MMA, epilogue warps
-constexpr int kTcTmemCols = 256; // two 128-column accumulators
+constexpr int kTcTmemCols = 512;  // two 256-column accumulators
+// Norms ring. The producer runs at most S <= 4 stages ahead of the MMA, the MMA
+// at most two tiles ahead of the epilogue's accumulator release, and a warp
+// finishes reading tile t's norms before it releases tile t+1: slot t % 8 is
+// therefore refilled (for tile t+8) only after every warp is done with tile t.
+constexpr int kTcNormSlots = 8;
+constexpr int kTcSmemLimit = 227 * 1024;
 
 struct TcParams {
     int m, d, k, kpad;   // kpad: d rounded up to 64 (one 128-byte swizzle atom per 64 BF16)
     int nterms;          // 1: hi*hi; 2: hi*hi + hi*lo (integer rows); 3: + lo*hi
     const uint32_t* gather;
-    const float* norms;
+    const float* norms;  // padded to whole tiles with a huge finite value
     float* part_s;
     uint32_t* part_i;
     int* err;            // set to 1 if a wait gave up (results then re-searched exactly)
@@ -151,37 +160,40 @@ EMB_DEV void mma_commit(uint64_t* bar) {
 
 EMB_DEV void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
+struct TcSmem {
+    // Offsets (bytes) inside the dynamic shared memory block (1024-aligned base).
+    uint32_t a_hi, a_lo, b0, stage_bytes, term_bytes, norms, merge, bars, total;
+    int stages;
+};
+
+__host__ __device__ inline TcSmem tc_smem_layout(int kpad, int nterms) {
+    TcSmem s;
+    const uint32_t a_bytes = (uint32_t)kTcBM * kpad * 2;
+    const uint32_t b_term = (uint32_t)kTcBN * 128;  // one K atom (64 BF16) of 256 centroids
+    const int bterms = nterms == 1 ? 1 : 2;
+    s.a_hi = 0;
+    s.a_lo = a_bytes;
+    const uint32_t a_total = nterms == 3 ? 2 * a_bytes : a_bytes;
+    s.b0 = a_total;
+    s.term_bytes = b_term;
+    s.stage_bytes = b_term * bterms;
+    const uint32_t fixed = kTcNormSlots * kTcBN * 4 + 3 * kTcBM * 16 + 256 + 1024;  // norms, merge, barriers, align
+    int st = 0;
+    while (st < kTcMaxStages && a_total + (st + 1) * s.stage_bytes + fixed <= (uint32_t)kTcSmemLimit) st++;
+    s.stages = st;
+    s.norms = s.b0 + st * s.stage_bytes;                 // [8][256] f32
+    s.merge = s.norms + kTcNormSlots * kTcBN * 4;        // [3][128] x (s1, i1, s2, i2)
+    s.bars = s.merge + 3 * kTcBM * 16;
+    s.total = s.bars + 256;
+    return s;
+}
+
 // Byte offset of 16-byte chunk `kc` (8 BF16 along K) of row r in a K-major,
 // 128B-swizzled tile of `rows` rows: atoms of 64 BF16 (128 B per row), 16-byte
 // chunks XOR-permuted by the row index mod 8 (the layout TMA SWIZZLE_128B writes).
 EMB_DEV uint32_t sw128_offset(int r, int kc, int rows) {
     int atom = kc >> 3, c = kc & 7;
     return (uint32_t)(atom * rows * 128 + r * 128 + ((c ^ (r & 7)) << 4));
-}
-
-struct TcSmem {
-    // Offsets (bytes) inside the dynamic shared memory block (1024-aligned base).
-    uint32_t a_hi, a_lo, b0, stage_bytes, term_bytes, norms, merge, bars, total;
-};
-
-constexpr int kTcNormSlots = 4;  // norms ring: slot t % 4 is refilled only after tile t's epilogue
-
-__host__ __device__ inline TcSmem tc_smem_layout(int kpad, int nterms) {
-    TcSmem s;
-    uint32_t a_bytes = (uint32_t)kTcBM * kpad * 2;
-    uint32_t b_term = (uint32_t)kTcBN * kpad * 2;
-    int bterms = nterms == 1 ? 1 : 2;
-    s.a_hi = 0;
-    s.a_lo = a_bytes;
-    uint32_t a_total = nterms == 3 ? 2 * a_bytes : a_bytes;
-    s.b0 = a_total;
-    s.term_bytes = b_term;
-    s.stage_bytes = b_term * bterms;
-    s.norms = s.b0 + kTcStages * s.stage_bytes;            // [4][128] f32
-    s.merge = s.norms + kTcNormSlots * kTcBN * 4;          // [128] x (s1, i1, s2, i2)
-    s.bars = s.merge + kTcBM * 16;
-    s.total = s.bars + 256;
-    return s;
 }
 
 template <typename T>
@@ -237,22 +249,71 @@ EMB_DEV float min3f(float a, float b, float c) {
     return r;
 }
 
-// Scores of 32 accumulator columns: s = norm - 2 acc (one rounding); returns their minimum.
-EMB_DEV float tc_scores32(const uint32_t (&v)[32], const float* __restrict__ nrm, float (&s)[32]) {
+// s = norm - 2 acc for two columns at once (fma.rn.f32x2: two IEEE fmas).
+EMB_DEV void fma2_scores(float a0, float a1, float n0, float n1, float& s0, float& s1) {
+    asm("{\n .reg .b64 ra, rb, rc, rd;\n mov.b64 ra, {%2, %3};\n mov.b64 rb, {%4, %5};\n mov.b64 rc, {%6, %7};\n"
+        " fma.rn.f32x2 rd, ra, rb, rc;\n mov.b64 {%0, %1}, rd;\n}\n"
+        : "=f"(s0), "=f"(s1)
+        : "f"(a0), "f"(a1), "f"(-2.0f), "f"(-2.0f), "f"(n0), "f"(n1));
+}
+
+// Scores of 32 accumulator columns: s = norm - 2 acc (one rounding).
+EMB_DEV void tc_scores32(const uint32_t (&v)[32], const float* __restrict__ nrm, float (&s)[32]) {
 #pragma unroll
     for (int j = 0; j < 32; j += 4) {
         float4 n4 = *reinterpret_cast<const float4*>(nrm + j);
-        s[j] = __fmaf_rn(-2.0f, __uint_as_float(v[j]), n4.x);
-        s[j + 1] = __fmaf_rn(-2.0f, __uint_as_float(v[j + 1]), n4.y);
-        s[j + 2] = __fmaf_rn(-2.0f, __uint_as_float(v[j + 2]), n4.z);
-        s[j + 3] = __fmaf_rn(-2.0f, __uint_as_float(v[j + 3]), n4.w);
+        fma2_scores(__uint_as_float(v[j]), __uint_as_float(v[j + 1]), n4.x, n4.y, s[j], s[j + 1]);
+        fma2_scores(__uint_as_float(v[j + 2]), __uint_as_float(v[j + 3]), n4.z, n4.w, s[j + 2], s[j + 3]);
     }
+}
+
+// Smallest of 32 scores (NaN-ignoring).
+EMB_DEV float tc_min32(const float (&s)[32]) {
     float m[11];
 #pragma unroll
     for (int i = 0; i < 10; i++) m[i] = min3f(s[3 * i], s[3 * i + 1], s[3 * i + 2]);
     m[10] = fminf(s[30], s[31]);
     float a = min3f(m[0], m[1], m[2]), b = min3f(m[3], m[4], m[5]), c = min3f(m[6], m[7], m[8]);
     return min3f(min3f(a, b, c), m[9], m[10]);
+}
+
+// Two smallest of 32 scores, branch-free. Each score's 5 low mantissa bits are
+// replaced by its column j (a relative change below 2^-18, which the error bound
+// covers), so min/max carry the column along; NaN keys are ignored by min/max.
+// Returns keys k1 <= k2.
+EMB_DEV void tc_top2_32(const float (&s)[32], float& k1, float& k2) {
+    float lo[16], hi[16];
+#pragma unroll
+    for (int p = 0; p < 16; p++) {
+        float a = __uint_as_float((__float_as_uint(s[2 * p]) & ~31u) | (uint32_t)(2 * p));
+        float b = __uint_as_float((__float_as_uint(s[2 * p + 1]) & ~31u) | (uint32_t)(2 * p + 1));
+        lo[p] = fminf(a, b);
+        hi[p] = fmaxf(a, b);
+    }
+#pragma unroll
+    for (int w = 8; w >= 1; w >>= 1) {
+#pragma unroll
+        for (int p = 0; p < w; p++) {
+            float a1 = lo[p], a2 = hi[p], b1 = lo[p + w], b2 = hi[p + w];
+            lo[p] = fminf(a1, b1);
+            hi[p] = min3f(fmaxf(a1, b1), a2, b2);
+        }
+    }
+    k1 = lo[0];
+    k2 = hi[0];
+}
+
+// Merge a chunk's top-2 (keys k1 <= k2 at columns cb + key&31) into a running top-2.
+EMB_DEV void top2_merge_keys(Top2& t, float k1, float k2, int cb) {
+    const uint32_t j1 = (uint32_t)cb + (__float_as_uint(k1) & 31u), j2 = (uint32_t)cb + (__float_as_uint(k2) & 31u);
+    const bool cw = k1 < t.s1;  // chunk wins first place
+    const float w2 = cw ? k2 : t.s2, l1 = cw ? t.s1 : k1;
+    const uint32_t w2i = cw ? j2 : t.i2, l1i = cw ? t.i1 : j1;
+    t.s1 = cw ? k1 : t.s1;
+    t.i1 = cw ? j1 : t.i1;
+    const bool bw = w2 < l1;
+    t.s2 = bw ? w2 : l1;
+    t.i2 = bw ? w2i : l1i;
 }
 
 // Keep the compiler from reading registers of a tcgen05.ld before its wait.
@@ -272,9 +333,10 @@ k_assign_tc(const T* __restrict__ x, const __grid_constant__ CUtensorMap map_hi,
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
     const TcSmem L = tc_smem_layout(p.kpad, p.nterms);
-    uint64_t* full = (uint64_t*)(smem + L.bars);          // [kTcStages]
-    uint64_t* empty = full + kTcStages;                   // [kTcStages]
-    uint64_t* acc_full = empty + kTcStages;               // [2]
+    const int S = L.stages;
+    uint64_t* full = (uint64_t*)(smem + L.bars);          // [kTcMaxStages]
+    uint64_t* empty = full + kTcMaxStages;                // [kTcMaxStages]
+    uint64_t* acc_full = empty + kTcMaxStages;            // [2]
     uint64_t* acc_empty = acc_full + 2;                   // [2]
     uint64_t* norms_full = acc_empty + 2;                 // [kTcNormSlots]
     uint32_t* tmem_slot = (uint32_t*)(norms_full + kTcNormSlots);
@@ -286,9 +348,10 @@ k_assign_tc(const T* __restrict__ x, const __grid_constant__ CUtensorMap map_hi,
     const int nsplit = gridDim.y;
     const int ntiles_all = (p.k + kTcBN - 1) / kTcBN;
     const int my_tiles = (int)blockIdx.y < ntiles_all ? (ntiles_all - (int)blockIdx.y + nsplit - 1) / nsplit : 0;
+    const int natoms = p.kpad / 64;
 
     if (threadIdx.x == 0) {
-        for (int s = 0; s < kTcStages; s++) {
+        for (int s = 0; s < kTcMaxStages; s++) {
             mbar_init(&full[s], 1);
             mbar_init(&empty[s], 1);
         }
@@ -310,33 +373,38 @@ k_assign_tc(const T* __restrict__ x, const __grid_constant__ CUtensorMap map_hi,
 
     if (warp == 0) {
         if (lane == 0) {
-            // ---- TMA producer: centroid tiles into the stage ring, their norms into the norms ring
+            // ---- TMA producer: unit u = (tile t, K atom a); norms once per tile
+            const int nunits = my_tiles * natoms;
             int issued = 0;
-            for (int t = 0; t < my_tiles; t++) {
-                int s = t % kTcStages;
-                uint32_t ph = (uint32_t)(t / kTcStages) & 1u;
+            for (int u = 0; u < nunits; u++) {
+                const int t = u / natoms, a = u - t * natoms;
+                const int s = u % S;
+                const uint32_t ph = (uint32_t)(u / S) & 1u;
                 if (!mbar_wait(&empty[s], ph ^ 1u, abort_flag)) break;
-                int tile = blockIdx.y + t * nsplit;
+                const int tile = blockIdx.y + t * nsplit;
                 uint8_t* stage = smem + L.b0 + s * L.stage_bytes;
                 mbar_expect_tx(&full[s], L.stage_bytes);
-                for (int a = 0; a < p.kpad / 64; a++) {
-                    tma_load_2d(stage + a * (kTcBN * 128), &map_hi, &full[s], a * 64, tile * kTcBN);
-                    if (p.nterms > 1)
-                        tma_load_2d(stage + L.term_bytes + a * (kTcBN * 128), &map_lo, &full[s], a * 64, tile * kTcBN);
+                tma_load_2d(stage, &map_hi, &full[s], a * 64, tile * kTcBN);
+                if (p.nterms > 1) tma_load_2d(stage + L.term_bytes, &map_lo, &full[s], a * 64, tile * kTcBN);
+                if (a == 0) {
+                    const int ns = t % kTcNormSlots;
+                    mbar_expect_tx(&norms_full[ns], kTcBN * 4);
+                    bulk_load(norms_s + ns * kTcBN, p.norms + (size_t)tile * kTcBN, kTcBN * 4, &norms_full[ns]);
                 }
-                int ns = t % kTcNormSlots;
-                mbar_expect_tx(&norms_full[ns], kTcBN * 4);
-                bulk_load(norms_s + ns * kTcBN, p.norms + (size_t)tile * kTcBN, kTcBN * 4, &norms_full[ns]);
-                issued = t + 1;
+                issued = u + 1;
             }
             // After an abort, let the copies still in flight land before the CTA
             // exits; bounded like every wait.
             if (*abort_flag) {
-                for (int t = issued > kTcStages ? issued - kTcStages : 0; t < issued; t++) {
-                    uint32_t ph = (uint32_t)(t / kTcStages) & 1u, nph = (uint32_t)(t / kTcNormSlots) & 1u;
-                    const uint64_t t0 = global_ns();
-                    while (!mbar_try(&full[t % kTcStages], ph) && global_ns() - t0 < kWaitLimitNs) {
+                const uint64_t t0 = global_ns();
+                for (int u = issued > S ? issued - S : 0; u < issued; u++) {
+                    const uint32_t ph = (uint32_t)(u / S) & 1u;
+                    while (!mbar_try(&full[u % S], ph) && global_ns() - t0 < kWaitLimitNs) {
                     }
+                }
+                const int tl = issued > 0 ? (issued - 1) / natoms : -1;
+                for (int t = tl >= kTcNormSlots ? tl - kTcNormSlots + 1 : 0; t <= tl; t++) {
+                    const uint32_t nph = (uint32_t)(t / kTcNormSlots) & 1u;
                     while (!mbar_try(&norms_full[t % kTcNormSlots], nph) && global_ns() - t0 < kWaitLimitNs) {
                     }
                 }
@@ -344,41 +412,54 @@ k_assign_tc(const T* __restrict__ x, const __grid_constant__ CUtensorMap map_hi,
         }
     } else if (warp == 1) {
         if (lane == 0) {
-            // ---- MMA issuer
+            // ---- MMA issuer: per unit, nterms x 4 MMAs of M=128 N=256 K=16
             const uint32_t idesc = idesc_bf16(kTcBM, kTcBN);
-            const uint32_t a_hi = smem_u32(smem + L.a_hi), a_lo = smem_u32(smem + L.a_lo);
-            const int ksteps = p.kpad / 16;
-            for (int t = 0; t < my_tiles; t++) {
-                int s = t % kTcStages;
-                uint32_t ph = (uint32_t)(t / kTcStages) & 1u;
-                int b = t & 1;
-                uint32_t bph = (uint32_t)(t >> 1) & 1u;
+            const uint64_t a_hi0 = sw128_desc(smem_u32(smem + L.a_hi));
+            const uint64_t a_lo0 = sw128_desc(smem_u32(smem + L.a_lo));
+            const uint32_t a_atom = (kTcBM * 128) >> 4;  // descriptor units (16 B) per A atom
+            bool ok = true;
+            int u = 0;
+            for (int t = 0; t < my_tiles && ok; t++) {
+                const int b = t & 1;
+                const uint32_t bph = (uint32_t)(t >> 1) & 1u;
                 if (!mbar_wait(&acc_empty[b], bph ^ 1u, abort_flag)) break;
-                if (!mbar_wait(&full[s], ph, abort_flag)) break;
                 tc_fence_after();
                 const uint32_t d_tmem = tmem_base + (uint32_t)(b * kTcBN);
-                const uint32_t b_hi = smem_u32(smem + L.b0 + s * L.stage_bytes);
-                const uint32_t b_lo = b_hi + L.term_bytes;
-                uint32_t acc = 0;
-                for (int term = 0; term < p.nterms; term++) {
-                    uint32_t abase = term == 2 ? a_lo : a_hi;
-                    uint32_t bbase = term == 1 ? b_lo : b_hi;
-                    for (int kk = 0; kk < ksteps; kk++) {
-                        uint32_t koff = (uint32_t)((kk >> 2) * (kTcBM * 128) + (kk & 3) * 32);
-                        uint32_t kofb = (uint32_t)((kk >> 2) * (kTcBN * 128) + (kk & 3) * 32);
-                        mma_bf16(d_tmem, sw128_desc(abase + koff), sw128_desc(bbase + kofb), idesc, acc);
+                for (int a = 0; a < natoms; a++, u++) {
+                    const int s = u % S;
+                    const uint32_t ph = (uint32_t)(u / S) & 1u;
+                    if (!mbar_wait(&full[s], ph, abort_flag)) {
+                        ok = false;
+                        break;
+                    }
+                    tc_fence_after();
+                    const uint64_t bh = sw128_desc(smem_u32(smem + L.b0 + s * L.stage_bytes));
+                    const uint64_t bl = bh + (L.term_bytes >> 4);
+                    const uint64_t ah = a_hi0 + (uint64_t)(a * a_atom), al = a_lo0 + (uint64_t)(a * a_atom);
+                    uint32_t acc = a > 0 ? 1u : 0u;
+#pragma unroll
+                    for (int kk = 0; kk < 4; kk++) {  // 16 BF16 = 32 B = 2 descriptor units per K step
+                        mma_bf16(d_tmem, ah + 2 * kk, bh + 2 * kk, idesc, acc);
                         acc = 1;
                     }
+                    if (p.nterms > 1) {
+#pragma unroll
+                        for (int kk = 0; kk < 4; kk++) mma_bf16(d_tmem, ah + 2 * kk, bl + 2 * kk, idesc, 1u);
+                    }
+                    if (p.nterms > 2) {
+#pragma unroll
+                        for (int kk = 0; kk < 4; kk++) mma_bf16(d_tmem, al + 2 * kk, bh + 2 * kk, idesc, 1u);
+                    }
+                    mma_commit(&empty[s]);
                 }
-                mma_commit(&empty[s]);
-                mma_commit(&acc_full[b]);
+                if (ok) mma_commit(&acc_full[b]);
             }
         }
     } else {
-        // ---- epilogue: warps 2..9. Thread = row (TMEM lane); warps 2..5 take
-        // columns 0..63 of each tile, warps 6..9 columns 64..127.
+        // ---- epilogue: warps 2..17. Thread = row (TMEM lane); warp w takes the
+        // 64-column quarter (w - 2) / 4 of every tile, as two 32-column chunks.
         const int q = warp & 3;  // TMEM lane quarter this warp may access
-        const int h = (warp - 2) >> 2;
+        const int cq = (warp - 2) >> 2;
         const int r = q * 32 + lane;
         const int row = row0 + r;
         Top2 top;
@@ -386,35 +467,34 @@ k_assign_tc(const T* __restrict__ x, const __grid_constant__ CUtensorMap map_hi,
         float theta = 0.0f;
         if (COLLECT) theta = row < p.m ? p.theta[row] : __int_as_float(0x7fc00000);
         for (int t = 0; t < my_tiles; t++) {
-            int b = t & 1;
-            uint32_t bph = (uint32_t)(t >> 1) & 1u;
+            const int b = t & 1;
+            const uint32_t bph = (uint32_t)(t >> 1) & 1u;
             if (!mbar_wait(&acc_full[b], bph, abort_flag)) break;
             if (!mbar_wait(&norms_full[t % kTcNormSlots], (uint32_t)(t / kTcNormSlots) & 1u, abort_flag)) break;
             tc_fence_after();
-            const int colh = (blockIdx.y + t * nsplit) * kTcBN + h * 64;
-            const float* nrm = norms_s + (t % kTcNormSlots) * kTcBN + h * 64;
-            const uint32_t taddr = tmem_base + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * kTcBN + h * 64);
-            uint32_t va[32], vb[32];
-            float s[32];
-            EMB_TMEM_LD32(taddr, va);
-            tmem_wait_ld();
-            tc_regs_ready(va);
-            EMB_TMEM_LD32(taddr + 32, vb);  // in flight while the first chunk is scored
+            const int cq0 = (blockIdx.y + t * nsplit) * kTcBN + cq * 64;
+            const float* nrm = norms_s + (t % kTcNormSlots) * kTcBN + cq * 64;
+            const uint32_t taddr = tmem_base + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * kTcBN + cq * 64);
 #pragma unroll
             for (int ch = 0; ch < 2; ch++) {
+                uint32_t v[32];
+                float s[32];
+                EMB_TMEM_LD32(taddr + ch * 32, v);
+                tmem_wait_ld();
+                tc_regs_ready(v);
                 if (ch == 1) {
-                    tmem_wait_ld();
-                    tc_regs_ready(vb);
+                    // Both chunks of this warp are in registers: release the accumulator.
+                    tc_fence_before();
+                    __syncwarp();
+                    if (lane == 0) mbar_arrive(&acc_empty[b]);
                 }
-                float mn = tc_scores32(ch == 0 ? va : vb, nrm + ch * 32, s);
-                const int cb = colh + ch * 32;
+                tc_scores32(v, nrm + ch * 32, s);
+                const int cb = cq0 + ch * 32;
                 if (!COLLECT) {
-                    if (mn < top.s2) {
-#pragma unroll
-                        for (int j = 0; j < 32; j++)
-                            if (s[j] < top.s2) top.push(s[j], (uint32_t)(cb + j));
-                    }
-                } else if (mn <= theta) {
+                    float k1, k2;
+                    tc_top2_32(s, k1, k2);
+                    top2_merge_keys(top, k1, k2, cb);
+                } else if (tc_min32(s) <= theta) {
 #pragma unroll
                     for (int j = 0; j < 32; j++) {
                         if (s[j] <= theta && cb + j < p.k) {
@@ -424,27 +504,29 @@ k_assign_tc(const T* __restrict__ x, const __grid_constant__ CUtensorMap map_hi,
                     }
                 }
             }
-            tc_fence_before();
-            __syncwarp();
-            if (lane == 0) mbar_arrive(&acc_empty[b]);
         }
         if (!COLLECT) {
-            // Merge the two column halves of each row through shared memory.
-            uint32_t* mg = (uint32_t*)(smem + L.merge) + r * 4;
-            if (h == 1) {
-                mg[0] = __float_as_uint(top.s1);
-                mg[1] = top.i1;
-                mg[2] = __float_as_uint(top.s2);
-                mg[3] = top.i2;
+            // Merge the four column quarters of each row through shared memory.
+            uint32_t* mg = (uint32_t*)(smem + L.merge);
+            if (cq > 0) {
+                uint32_t* e = mg + ((cq - 1) * kTcBM + r) * 4;
+                e[0] = __float_as_uint(top.s1);
+                e[1] = top.i1;
+                e[2] = __float_as_uint(top.s2);
+                e[3] = top.i2;
             }
             asm volatile("bar.sync 1, %0;" ::"n"(kTcEpiWarps * 32) : "memory");
-            if (h == 0 && row < p.m) {
-                Top2 o;
-                o.s1 = __uint_as_float(mg[0]);
-                o.i1 = mg[1];
-                o.s2 = __uint_as_float(mg[2]);
-                o.i2 = mg[3];
-                top.merge(o);
+            if (cq == 0 && row < p.m) {
+#pragma unroll
+                for (int o = 0; o < 3; o++) {
+                    const uint32_t* e = mg + (o * kTcBM + r) * 4;
+                    Top2 ot;
+                    ot.s1 = __uint_as_float(e[0]);
+                    ot.i1 = e[1];
+                    ot.s2 = __uint_as_float(e[2]);
+                    ot.i2 = e[3];
+                    top.merge(ot);
+                }
                 size_t oo = ((size_t)blockIdx.y * p.m + row) * 2;
                 p.part_s[oo] = top.s1;
                 p.part_i[oo] = top.i1;
