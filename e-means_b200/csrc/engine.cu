@@ -50,12 +50,16 @@ struct DevBuf {
 
 // Device state of a training run (filled by emb200_train).
 struct TrainState {
-    DevBuf<float> usage, sums;
-    DevBuf<uint32_t> counts, labels_all, order, batch_labels;
-    DevBuf<float> batch_dist;
+    DevBuf<float> usage, sums, pass_sums, batch_dist;
+    DevBuf<double> pass_sums64, keys, scalars, obj, gstream;
+    DevBuf<uint32_t> counts, offsets, slot, list, scratch, batch_labels, labels_all, order, didx, unused;
+    DevBuf<unsigned long long> pass_counts;
     void release() {
-        usage.release(); sums.release(); counts.release(); labels_all.release(); order.release();
-        batch_labels.release(); batch_dist.release();
+        usage.release(); sums.release(); pass_sums.release(); batch_dist.release();
+        pass_sums64.release(); keys.release(); scalars.release(); obj.release(); gstream.release();
+        counts.release(); offsets.release(); slot.release(); list.release(); scratch.release();
+        batch_labels.release(); labels_all.release(); order.release(); didx.release(); unused.release();
+        pass_counts.release();
     }
 };
 

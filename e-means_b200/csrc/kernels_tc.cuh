@@ -79,6 +79,17 @@ EMB_DEV bool mbar_try(uint64_t* bar, uint32_t parity) {
         : "memory");
     return ok != 0;
 }
+// Same, letting the warp sleep up to `hint_ns` inside the instruction (it
+// returns as soon as the phase completes): waiting warps stop taking issue slots.
+EMB_DEV bool mbar_try_sleep(uint64_t* bar, uint32_t parity, uint32_t hint_ns) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity), "r"(hint_ns)
+        : "memory");
+    return ok != 0;
+}
 EMB_DEV uint64_t global_ns() {
     uint64_t t;
     asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
@@ -88,11 +99,11 @@ constexpr uint64_t kWaitLimitNs = 4000000000ull;  // a healthy wait takes micros
 
 // Bounded wait: returns false (and raises the abort flag) if the phase does not
 // complete within kWaitLimitNs, or if another role already aborted.
-EMB_DEV bool mbar_wait(uint64_t* bar, uint32_t parity, volatile int* abort_flag) {
+EMB_DEV bool mbar_wait(uint64_t* bar, uint32_t parity, volatile int* abort_flag, uint32_t hint_ns = 0) {
     if (mbar_try(bar, parity)) return true;
     const uint64_t t0 = global_ns();
     for (uint32_t i = 1;; i++) {
-        if (mbar_try(bar, parity)) return true;
+        if (hint_ns ? mbar_try_sleep(bar, parity, hint_ns) : mbar_try(bar, parity)) return true;
         if ((i & 63) == 0) {
             if (*abort_flag) return false;
             if (global_ns() - t0 > kWaitLimitNs) {
@@ -469,7 +480,7 @@ k_assign_tc(const T* __restrict__ x, const __grid_constant__ CUtensorMap map_hi,
         for (int t = 0; t < my_tiles; t++) {
             const int b = t & 1;
             const uint32_t bph = (uint32_t)(t >> 1) & 1u;
-            if (!mbar_wait(&acc_full[b], bph, abort_flag)) break;
+            if (!mbar_wait(&acc_full[b], bph, abort_flag, 20000)) break;
             if (!mbar_wait(&norms_full[t % kTcNormSlots], (uint32_t)(t / kTcNormSlots) & 1u, abort_flag)) break;
             tc_fence_after();
             const int cq0 = (blockIdx.y + t * nsplit) * kTcBN + cq * 64;

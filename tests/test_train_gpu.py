@@ -1,0 +1,132 @@
+"""GPU parity of the device-resident training loop (src/lib.rs:348-491) with the
+oracle's restatement of the reference's CPU train().
+
+The batch search is bit-exact and the update kernels follow the reference's f32
+operation order, so the trained centroids, last-pass labels and revival counts
+must equal the oracle's bit for bit; the per-epoch objective (an f64 sum whose
+order differs) must agree to 1e-12 relative.
+"""
+import numpy as np
+import pytest
+
+from tests.test_oracle import closing_mean_data
+
+pytestmark = pytest.mark.gpu
+
+
+def same_f32(a, b):
+    return np.array_equal(np.asarray(a, np.float32).view(np.uint32), np.asarray(b, np.float32).view(np.uint32))
+
+
+def run_both(emb, orc, x, k, precision="fp32", centroid_bits=0, assigner="cpu", **cfg):
+    a = emb.B200Assigner(0, precision=precision, centroid_bits=centroid_bits)
+    out = emb.train(x, x.shape[1], k, emb.Config(**cfg), assigner=a)
+    st = a.stats()
+    a.close()
+    ref = orc.train(x, k, orc.make_config(**cfg), assigner=assigner, kernel="avx512", emulate=not orc.has_kernel("avx512"))
+    return out, ref, st
+
+
+def check_same(out, ref):
+    assert out.recipe.batch_size == ref["recipe"]["batch_size"]
+    assert out.recipe.epoch_rows == ref["recipe"]["epoch_rows"]
+    assert out.n_splits == ref["n_splits"]
+    assert np.array_equal(out.labels, ref["labels"])
+    assert same_f32(out.centroids, ref["centroids"])
+    np.testing.assert_allclose(out.objective, ref["objective"], rtol=1e-12)
+
+
+@pytest.mark.parametrize("precision", ["fp32", "bf16"])
+def test_closing_mean_data_bit_exact(emb, orc, precision):
+    # The 20-blob 6-D data of src/lib.rs:575-614 (quality law, revival every 5 steps).
+    x = closing_mean_data(orc)
+    out, ref, _ = run_both(emb, orc, x, 32, precision)
+    check_same(out, ref)
+    # and the reference test's own invariants
+    k, d = 32, 6
+    sums = np.zeros((k, d))
+    counts = np.bincount(out.labels, minlength=k)
+    np.add.at(sums, out.labels, x.astype(np.float64))
+    for j in np.nonzero(counts)[0]:
+        assert np.all(np.abs(out.centroids[j] - sums[j] / counts[j]) < 1e-3)
+    assert np.all(np.diff(out.objective) < 0)
+
+
+@pytest.mark.parametrize("precision", ["fp32", "bf16", "bf16x1"])
+def test_blob_mixture_bit_exact(emb, orc, precision):
+    x = emb.datasets.blobs(30_000, 96, n_blobs=512, seed=2)
+    out, ref, st = run_both(emb, orc, x, 256, precision, nepochs=3.0)
+    check_same(out, ref)
+    assert st["fast_aborted"] == 0
+
+
+def test_embeddings_bit_exact(emb, orc):
+    x = emb.datasets.embeddings(40_000, 128, seed=5)
+    out, ref, _ = run_both(emb, orc, x, 512, "bf16", nepochs=2.0)
+    check_same(out, ref)
+
+
+def test_fractional_and_short_epochs(emb, orc):
+    x = emb.datasets.blobs(6_000, 12, n_blobs=64, seed=3)
+    out, ref, _ = run_both(emb, orc, x, 40, "fp32", nepochs=2.5)
+    check_same(out, ref)
+    assert out.recipe.epoch_rows == [6000, 3000, 6000]
+    out, ref, _ = run_both(emb, orc, x, 40, "fp32", nepochs=0.5)
+    check_same(out, ref)
+    assert (out.labels == 0xFFFFFFFF).sum() == 3000  # rows outside the only (partial) pass
+
+
+def test_balance_penalty_bit_exact(emb, orc):
+    x = emb.datasets.blobs(20_000, 32, n_blobs=300, seed=4)
+    out, ref, _ = run_both(emb, orc, x, 128, "bf16", nepochs=3.0, balance=0.3)
+    check_same(out, ref)
+
+
+def test_int8_rows_both_semantics(emb, orc):
+    xf = emb.datasets.embeddings(30_000, 64, latent=16, seed=6)
+    codes, _, _ = emb.datasets.faiss_int8(xf)
+    # CpuI8Assigner(I8): integer search (src/cpu_i8.rs), f32 sums and EMA.
+    out, ref, _ = run_both(emb, orc, codes, 200, "fp32", centroid_bits=8, assigner="i8", nepochs=3.0)
+    check_same(out, ref)
+    # CpuAssigner on i8 rows: rows widened to f32.
+    out, ref, _ = run_both(emb, orc, codes, 200, "bf16", nepochs=3.0)
+    check_same(out, ref)
+
+
+def test_uint8_rows(emb, orc):
+    rng = np.random.default_rng(8)
+    x = (rng.integers(0, 40, (12_000, 24)) + rng.integers(0, 200, (1, 24))).astype(np.uint8)
+    out, ref, _ = run_both(emb, orc, x, 64, "bf16", nepochs=2.0)
+    check_same(out, ref)
+
+
+def test_closing_mean_f64_option(emb):
+    x = emb.datasets.blobs(20_000, 16, n_blobs=100, seed=9)
+    a = emb.B200Assigner(0, precision="bf16")
+    out = emb.train(x, 16, 64, emb.Config(nepochs=2.0, closing_f64=True), assigner=a)
+    a.close()
+    counts = np.bincount(out.labels, minlength=64)
+    sums = np.zeros((64, 16))
+    np.add.at(sums, out.labels, x.astype(np.float64))
+    for j in np.nonzero(counts)[0]:
+        assert np.array_equal(out.centroids[j], (sums[j] / counts[j]).astype(np.float32))
+
+
+def test_training_argument_errors(emb):
+    a = emb.B200Assigner(0)
+    a.load_rows(np.zeros((10, 3), np.float32))
+    with pytest.raises(emb.EngineError, match="at least k"):
+        a.train_resident(11)
+    with pytest.raises(emb.EngineError, match="nepochs"):
+        a.train_resident(2, emb.Config(nepochs=0.0))
+    a.close()
+
+
+def test_assign_after_training_uses_trained_centroids(emb, orc):
+    x = emb.datasets.blobs(10_000, 20, n_blobs=50, seed=10)
+    a = emb.B200Assigner(0, precision="bf16")
+    out = emb.train(x, 20, 48, emb.Config(nepochs=2.0), assigner=a)
+    lab, dist = a.assign_resident()
+    rl, rd = orc.cpu_assign(x, out.centroids, emulate=True)
+    assert np.array_equal(lab, rl) and same_f32(dist, rd)
+    a.close()
