@@ -1,16 +1,24 @@
 """Benchmark of the B200 e-means engine on its headline workload.
 
-Metric: rows/s assigned at 1,000,000 x 128-D f32 embedding-like rows against
-k = 16384 centroids (the exact nearest-centroid pass of src/lib.rs:512-520).
-A step is one full assign pass over the 1M resident rows. The centroids are
-the output of the engine's own e-means training on the same rows (untimed).
+Workload: the exact nearest-centroid pass (assign(), src/lib.rs:512-520) over
+1,000,000 x 128-D f32 embedding-like rows (32-d N(0,1) latent through a random
+Gaussian map, N(0, 0.1^2) noise, L2-normalised; seeded synthetic data) against
+k = 16384 centroids trained by the engine's own e-means on the same rows
+(2 epochs, untimed). A step is one full pass over the 1M rows.
 
-  value : rows/s with the rows resident in HBM (device-timed, CUDA events)
-  e2e   : rows/s through the public C ABI with host buffers (pinned host rows
-          copied in, labels and distances copied out, inside the timed region)
+  value   rows/s with the rows resident in HBM (device-timed with CUDA events on
+          the engine's stream; the 512 MB of rows exceed the 126 MB L2)
+  e2e     rows/s through the public C ABI call (emb200_assign_f32) with pinned
+          host rows: the host->device copy of the rows and the device->host copy
+          of labels and distances are inside the timed region
+  roofline  the fast contraction kernel (tcgen05): algorithmic flops 2 d k per
+          row / its CUDA-event time, against the measured BF16 tensor peak
 
-`--impl reference` times the reference's CPU implementation (its CpuAssigner
-restated in C++, oracle/) on a bounded sample of the same workload.
+Every number comes from the bit-exact pipeline: labels and distances equal the
+reference CpuAssigner's (AVX-512 rounding) for every row.
+
+`--impl reference` times the reference's CPU search (its CpuAssigner, restated
+in C++ in oracle/) on the host cores over a bounded sample of the same rows.
 """
 import argparse
 import json
@@ -26,19 +34,22 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 N_ROWS, DIM, K = 1_000_000, 128, 16384
-WORKLOAD = "embeddings 1,000,000 x 128 f32 (32-d latent, L2-normalised), k=16384, exact assign pass"
+WORKLOAD = "assign 1,000,000 x 128 f32 embedding rows (32-d latent, L2-normalised) to k=16384 trained centroids"
 METRIC = "rows/s assigned (1M x 128-D, k=16384)"
+DTYPES = {"fp32": "f32", "bf16": "bf16x3 (hi/lo split) -> f32 accumulate", "bf16x1": "bf16 -> f32 accumulate"}
+CPU_SAMPLE_ROWS = 262_144
 
 
 def dist_env():
-    rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    return rank, world, local
+    return (int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")),
+            int(os.environ.get("LOCAL_RANK", "0")))
 
 
 class ClockSampler:
-    """Samples nvidia-smi clocks and throttle reasons during the timed region."""
+    """Samples nvidia-smi SM clocks and throttle reasons during the timed region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
     def __init__(self, index):
         self.index = index
@@ -47,11 +58,9 @@ class ClockSampler:
         self._t = None
 
     def _run(self):
-        q = ("clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
         while not self._stop.is_set():
             try:
-                out = subprocess.run(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
+                out = subprocess.run(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
                                       "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
                 vals = [v.strip() for v in out.stdout.strip().split(",")]
                 if len(vals) == 6:
@@ -72,12 +81,19 @@ class ClockSampler:
     def summary(self):
         if not self.samples:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
-        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+
+        def num(v):
+            try:
+                return float(v)
+            except ValueError:
+                return None
+
+        sm = [num(s[0]) for s in self.samples if num(s[0]) is not None]
+        mx = [num(s[1]) for s in self.samples if num(s[1]) is not None]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for s in self.samples for i in range(4) if s[2 + i].lower() == "active"})
+        reasons = sorted({names[i] for s in self.samples for i in range(4) if s[2 + i].strip().lower() == "active"})
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons}
+                "reasons": reasons, "samples": len(self.samples)}
 
 
 def measured_peaks():
@@ -86,37 +102,117 @@ def measured_peaks():
         with open(p) as f:
             j = json.load(f)
         return {"hbm_gbs": j["hbm_gbs"], "bf16_tflops": j["bf16_tflops"],
-                "bf16_tflops_sustained": j.get("bf16_tflops_sustained"), "source": "measured"}
-    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0, "source": "fallback"}
+                "bf16_tflops_sustained": j.get("bf16_tflops_sustained", j["bf16_tflops"]), "source": "of measured"}
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0, "source": "of fallback"}
 
 
-def make_workload(seed=0):
+def profiled_traffic_per_row():
+    """DRAM bytes per row of the fast kernel from the committed ncu summary (or None)."""
+    p = os.path.join(ROOT, "profiles", "tc_assign_embeddings_1Mx128_k16384.md")
+    if not os.path.exists(p):
+        return None
+    for line in open(p):
+        if line.startswith("traffic_bytes_per_row:"):
+            return float(line.split(":")[1])
+    return None
+
+
+def make_rows(seed=0):
     from __graft_entry__ import load_package
 
     emb = load_package()
-    x = emb.datasets.embeddings(N_ROWS, DIM, seed=seed)
-    return emb, x
+    return emb, emb.datasets.embeddings(N_ROWS, DIM, seed=seed)
 
 
-def trained_centroids(emb, x, cache=True):
-    """k=16384 centroids from the engine's own e-means (2 epochs) on the rows."""
-    path = os.path.join(ROOT, "gpurun_out", "bench_centroids_c2.npy")
-    if cache and os.path.exists(path):
-        return np.load(path)
-    a = emb.B200Assigner(0, precision="bf16")
-    try:
-        a.load_rows(x)
-        out = a.train_resident(K, emb.Config(nepochs=2.0))
-        c = out.centroids
-    except emb.EngineError:
-        # Training not available: seed centroids from a fixed sample of rows.
-        c = x[np.random.default_rng(1).choice(len(x), K, replace=False)].copy()
-    finally:
-        a.close()
-    if cache:
-        os.makedirs(os.path.dirname(path), exist_ok=True)
-        np.save(path, c)
-    return c
+def set_rows(n):
+    """Smaller passes of the same workload (profiling captures); the default is 1M."""
+    global N_ROWS
+    N_ROWS = n
+
+
+def trained_centroids(emb, x, ordinal):
+    """k = 16384 centroids from the engine's own e-means (2 epochs) on the rows."""
+    a = emb.B200Assigner(ordinal, precision="bf16")
+    a.load_rows(x)
+    out = a.train_resident(K, emb.Config(nepochs=2.0))
+    a.close()
+    return out.centroids
+
+
+def allreduce_max(v, world):
+    if world == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world):
+    import torch
+
+    torch.cuda.synchronize()
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+        torch.cuda.synchronize()
+
+
+def time_resident(a, steps, warmup, world):
+    for _ in range(warmup):
+        a.assign_resident(want_host=False)
+    barrier(world)
+    ms, fast_ms, launches, fast_launches, refined, researched = [], 0.0, 0, 0, 0, 0
+    for _ in range(steps):
+        a.assign_resident(want_host=False)
+        st = a.stats()
+        ms.append(st["ms_total"])
+        fast_ms += st["fast_ms"]
+        fast_launches += st["fast_launches"]
+        launches += st["kernel_launches"]
+        refined += st["rows_refined"]
+        researched += st["rows_researched"]
+    barrier(world)
+    t = allreduce_max(float(np.sum(ms)), world)
+    return {"ms_total": t, "ms_per_step": t / steps, "fast_ms_per_launch": fast_ms / max(fast_launches, 1),
+            "launches": launches, "refined_per_step": refined / steps, "researched_per_step": researched / steps}
+
+
+def time_e2e(emb, a, x, steps, warmup, world):
+    """The C-ABI host call on pinned buffers: copies in, search, copies out."""
+    import torch
+
+    xp = torch.from_numpy(x).pin_memory()
+    lab = torch.empty(N_ROWS, dtype=torch.int32).pin_memory()
+    dst = torch.empty(N_ROWS, dtype=torch.float32).pin_memory()
+    for _ in range(warmup):
+        a.assign_host_ptr(xp.data_ptr(), emb.EMB200_F32, N_ROWS, lab.data_ptr(), dst.data_ptr())
+    barrier(world)
+    ms = []
+    for _ in range(steps):
+        a.assign_host_ptr(xp.data_ptr(), emb.EMB200_F32, N_ROWS, lab.data_ptr(), dst.data_ptr())
+        ms.append(a.stats()["ms_total"])
+    barrier(world)
+    t = allreduce_max(float(np.sum(ms)), world)
+    return t / steps
+
+
+def cpu_baseline(x, cent, rows=None):
+    rows = min(rows or CPU_SAMPLE_ROWS, len(x))
+    from oracle import oracle as orc
+
+    kern = "avx512" if orc.has_kernel("avx512") else ("avx2" if orc.has_kernel("avx2") else "portable")
+    cores = os.cpu_count() or 1
+    orc.cpu_assign(x[:256], cent, kernel=kern, nthreads=cores)  # warm the library and threads
+    t0 = time.perf_counter()
+    orc.cpu_assign(x[:rows], cent, kernel=kern, nthreads=cores)
+    dt = time.perf_counter() - t0
+    return {"value": rows / dt, "unit": "rows/s", "cores": cores, "kind": "port",
+            "sample": f"first {rows} of the 1M rows, k=16384: the reference CpuAssigner ({kern} kernel, 256 KB "
+                      f"blocking, 4x4 micro-kernel) restated in C++, OpenMP over {cores} host threads, {dt:.2f} s"}
 
 
 def run_ours(args):
@@ -128,59 +224,65 @@ def run_ours(args):
         import torch.distributed as dist
         from datetime import timedelta
 
-        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
-    emb, x = make_workload(seed=0)
-    cent = trained_centroids(emb, x, cache=(world == 1))
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+    emb, x = make_rows(seed=0)
+    cent = trained_centroids(emb, x, local)
     peaks = measured_peaks()
     results = {}
-    for prec in args.precisions:
-        a = emb.B200Assigner(local, precision=prec)
-        a.set_centroids(cent)
-        a.load_rows(x)
-        results[prec] = time_resident(a, emb, args, prec, world)
-        a.close()
+    sampler = ClockSampler(local)
+    with sampler:
+        for prec in args.precisions:
+            a = emb.B200Assigner(local, precision=prec)
+            a.set_centroids(cent)
+            a.load_rows(x)
+            steps = args.steps if prec != "fp32" else max(1, min(args.steps, 3))
+            results[prec] = time_resident(a, steps, args.warmup, world)
+            results[prec]["steps"] = steps
+            if prec == args.precisions[0]:
+                e2e_ms = time_e2e(emb, a, x, args.steps, args.warmup, world)
+            a.close()
     head = args.precisions[0]
     r = results[head]
-    value = r["rows_per_s_total"]
+    value = N_ROWS * world / (r["ms_per_step"] / 1e3)
+    flops_per_launch = 2.0 * DIM * K * N_ROWS
+    achieved = flops_per_launch / (r["fast_ms_per_launch"] / 1e3) / 1e12
+    peak = peaks["bf16_tflops_sustained"]
+    tpr = profiled_traffic_per_row()
     line = {
         "metric": METRIC, "value": value, "unit": "rows/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": r["ms_per_step"], "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": {"fp32": "f32", "bf16": "bf16x3->f32", "bf16x1": "bf16->f32"}[head],
-        "data": "synthetic (seeded numpy generator, shapes and distribution of the workload)",
+        "vs_baseline": None, "dtype": DTYPES[head],
+        "data": "synthetic: seeded numpy embedding rows of the workload's shape and distribution",
         "config": {"workload": WORKLOAD, "rows_per_gpu": N_ROWS, "d": DIM, "k": K, "precision": head,
-                   "l2": "inputs (512 MB of rows) larger than L2", "parallelism": f"replicas x{world}"},
-        "per_precision": {p: {"rows_per_s": results[p]["rows_per_s_total"], "ms_per_step": results[p]["ms_per_step"],
-                              "refined_rows": results[p]["refined"], "researched_rows": results[p]["researched"]}
-                          for p in results},
+                   "parity": "labels and distances bit-exact with the reference CpuAssigner (AVX-512 rounding)",
+                   "l2": "no flush: the 512 MB of resident rows per pass exceed the 126 MB L2",
+                   "parallelism": f"{world} independent replicas (rows shard, no collective)"},
+        "e2e": {"value": N_ROWS * world / (e2e_ms / 1e3), "unit": "rows/s", "h2d_bytes_per_step": N_ROWS * DIM * 4,
+                "d2h_bytes_per_step": N_ROWS * 8},
+        "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                     "frac": achieved / peak, "peak_note": f"bf16 sustained {peaks['source']}",
+                     "kernel": "k_assign_tc (fast contraction)",
+                     "algorithmic_flops_per_launch": flops_per_launch,
+                     "executed_flops_per_launch": flops_per_launch * {"bf16": 3, "bf16x1": 1, "fp32": 1}[head],
+                     "traffic": None if tpr is None else tpr * N_ROWS},
+        "per_precision": {p: {"rows_per_s": N_ROWS * world / (results[p]["ms_per_step"] / 1e3),
+                              "ms_per_step": results[p]["ms_per_step"], "steps": results[p]["steps"],
+                              "fast_kernel_ms": results[p]["fast_ms_per_launch"],
+                              "refined_rows_per_step": results[p]["refined_per_step"],
+                              "exhaustive_rows_per_step": results[p]["researched_per_step"]} for p in results},
         "gpu_launches": r["launches"],
+        "clocks": sampler.summary(),
     }
+    if "fp32" in results and head != "fp32":
+        line["speedup_vs_fp32_path"] = results["fp32"]["ms_per_step"] / r["ms_per_step"]
+    if rank == 0 and world == 1 and not args.no_cpu:
+        line["cpu_baseline"] = cpu_baseline(x, cent)
     if rank == 0:
         print(json.dumps(line), flush=True)
-
-
-def time_resident(a, emb, args, prec, world):
-    import torch
-
-    for _ in range(args.warmup):
-        a.assign_resident(want_host=False)
-    torch.cuda.synchronize()
     if world > 1:
-        torch.distributed.barrier()
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    ms = []
-    for _ in range(args.steps):
-        a.assign_resident(want_host=False)
-        ms.append(a.stats()["ms_total"])
-    st = a.stats()
-    t = float(np.sum(ms))
-    if world > 1:
-        tt = torch.tensor([t], device="cuda")
-        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
-        t = float(tt.item())
-    rows = N_ROWS * args.steps * world
-    return {"rows_per_s_total": rows / (t / 1e3), "ms_per_step": t / args.steps, "researched": st["rows_researched"],
-            "refined": st["rows_refined"],
-            "launches": st["kernel_launches"] * args.steps}
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
 
 
 def run_reference(args):
@@ -189,18 +291,18 @@ def run_reference(args):
         return
     from oracle import oracle as orc
 
-    _, x = make_workload(seed=0)
-    cent = x[np.random.default_rng(1).choice(len(x), K, replace=False)].copy()
-    sample = 16384
-    cores = os.cpu_count()
+    _, x = make_rows(seed=0)
+    cent = x[np.random.default_rng(1).choice(len(x), K, replace=False)] * np.float32(0.97)
     kern = "avx512" if orc.has_kernel("avx512") else ("avx2" if orc.has_kernel("avx2") else "portable")
-    for _ in range(args.warmup and 1):
-        orc.cpu_assign(x[:1024], cent, kernel=kern)
+    cores = os.cpu_count() or 1
+    sample = min(32768, N_ROWS // 2)  # rows per step: each step a bounded slice of the pass
+    for _ in range(min(args.warmup, 1)):
+        orc.cpu_assign(x[:1024], cent, kernel=kern, nthreads=cores)
     ts = []
     for s in range(args.steps):
         r0 = (s * sample) % (N_ROWS - sample)
         t0 = time.perf_counter()
-        orc.cpu_assign(x[r0:r0 + sample], cent, kernel=kern)
+        orc.cpu_assign(x[r0:r0 + sample], cent, kernel=kern, nthreads=cores)
         ts.append(time.perf_counter() - t0)
     rps = sample * len(ts) / sum(ts)
     line = {"metric": METRIC, "value": rps, "unit": "rows/s", "n_gpus": world, "steps": args.steps,
@@ -208,8 +310,9 @@ def run_reference(args):
             "vs_baseline": None, "dtype": "f32", "data": "synthetic", "impl": "reference",
             "config": {"workload": WORKLOAD, "rows_per_gpu": N_ROWS, "d": DIM, "k": K},
             "cpu_baseline": {"value": rps, "unit": "rows/s", "cores": cores, "kind": "port",
-                             "sample": f"{sample} rows per step x {args.steps} steps of the 1M-row pass, CpuAssigner "
-                                       f"{kern} kernel restated in C++ (OpenMP, {cores} threads)"},
+                             "sample": f"{sample} rows per step x {args.steps} steps of the 1M-row pass; the "
+                                       f"reference CpuAssigner ({kern} kernel) restated in C++, OpenMP, "
+                                       f"{cores} threads"},
             "e2e": {"value": rps, "unit": "rows/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -220,8 +323,11 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--precisions", default="fp32", help="comma list; the first is the headline")
+    ap.add_argument("--precisions", default="bf16x1,bf16,fp32", help="comma list; the first is the headline")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    ap.add_argument("--rows", type=int, default=N_ROWS, help="rows per pass (profiling captures use fewer)")
     args = ap.parse_args()
+    set_rows(args.rows)
     args.precisions = args.precisions.split(",")
     if args.impl == "reference":
         run_reference(args)

@@ -52,7 +52,8 @@ class _Recipe(ctypes.Structure):
 class _Stats(ctypes.Structure):
     _fields_ = [("rows", ctypes.c_uint64), ("rows_certified", ctypes.c_uint64), ("rows_researched", ctypes.c_uint64),
                 ("kernel_launches", ctypes.c_uint64), ("ms_total", ctypes.c_double), ("fast_kernel", ctypes.c_int32),
-                ("fast_aborted", ctypes.c_int32), ("rows_refined", ctypes.c_uint64)]
+                ("fast_aborted", ctypes.c_int32), ("rows_refined", ctypes.c_uint64), ("fast_ms", ctypes.c_double),
+                ("fast_launches", ctypes.c_uint64)]
 
 
 def build(force=False):
@@ -248,6 +249,13 @@ class B200Assigner:
               EMB200_U8: lib().emb200_assign_u8}[_DTYPES[x.dtype]]
         self._check(fn(self._h, _p(x), m, _p(labels), _p(dist)))
         return labels, dist
+
+    def assign_host_ptr(self, x_ptr, dtype, m, labels_ptr, dist_ptr):
+        """Host-memory assign on raw pointers (e.g. pinned torch tensors): the trait
+        call with the caller's own buffers."""
+        fn = {EMB200_F32: lib().emb200_assign_f32, EMB200_I8: lib().emb200_assign_i8,
+              EMB200_U8: lib().emb200_assign_u8}[dtype]
+        self._check(fn(self._h, ctypes.c_void_p(x_ptr), m, ctypes.c_void_p(labels_ptr), ctypes.c_void_p(dist_ptr)))
 
     def assign_device(self, x_ptr, dtype, m, labels_ptr, dist_ptr, stream=None):
         """Device-pointer assign (torch tensors' data_ptr()), enqueued on `stream`."""

@@ -72,6 +72,7 @@ struct emb200_handle {
     std::string err;
     emb200_stats stats{};
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    cudaEvent_t evk0 = nullptr, evk1 = nullptr;  // around the fast contraction kernel
     int sm_count = 148;
 
     // centroids
@@ -95,7 +96,10 @@ struct emb200_handle {
     DevBuf<float> res_dist;
 
     // scratch for assign
-    DevBuf<uint8_t> stage;  // host-path staging of rows
+    DevBuf<uint8_t> stage;  // host-path staging of rows (two chunk buffers)
+    cudaStream_t copy_stream = nullptr;
+    cudaEvent_t ev_copied[2] = {nullptr, nullptr};
+    cudaEvent_t ev_done[2] = {nullptr, nullptr};  // a staging buffer's search is complete
     DevBuf<uint32_t> st_labels;
     DevBuf<float> st_dist;
     DevBuf<float> part_s;
@@ -387,6 +391,7 @@ int assign_rows_dev(emb200_handle* h, const T* x, const uint32_t* gather, size_t
     uint32_t* ctr = h->counters.p;
     CK(cudaMemsetAsync(ctr, 0, 8 * sizeof(uint32_t), st));
     h->stats.fast_kernel = tc ? 1 : 0;
+    CK(cudaEventRecord(h->evk0, st));
     if (tc) {
         int rc = launch_tc<T, false>(h, x, gather, nullptr, m, fast_terms, nullptr, nullptr, nullptr, 0,
                                      (int*)(ctr + 2), st);
@@ -398,6 +403,7 @@ int assign_rows_dev(emb200_handle* h, const T* x, const uint32_t* gather, size_t
                                                          h->part_i.p, vec4);
         CKL();
     }
+    CK(cudaEventRecord(h->evk1, st));
     float ka, kb, ka2, kb2;
     bound_coefficients(tc ? prec : EMB200_PREC_FP32, dtype, h->d, tc, &ka, &kb);
     bound_coefficients(EMB200_PREC_BF16, dtype, h->d, false, &ka2, &kb2);
@@ -411,6 +417,10 @@ int assign_rows_dev(emb200_handle* h, const T* x, const uint32_t* gather, size_t
     uint32_t nredo = 0;
     CK(cudaMemcpyAsync(&nredo, ctr, sizeof nredo, cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
+    float kms = 0.0f;
+    CK(cudaEventElapsedTime(&kms, h->evk0, h->evk1));
+    h->stats.fast_ms += kms;
+    h->stats.fast_launches += 1;
     h->stats.rows_refined += nredo;
     if (nredo == 0) return finish_counters(h, st, false);
     const uint32_t* exhaustive = h->redo_rows.p;
@@ -456,8 +466,10 @@ int check_ready(emb200_handle* h, int dtype) {
     return EMB200_OK;
 }
 
-// Host-memory assign (the trait call): chunks of rows are copied in, searched
-// and copied out.
+// Host-memory assign (the trait call). Rows go through two staging buffers in
+// chunks: the copy of chunk i+1 (its own stream) overlaps the search of chunk i,
+// and each chunk's labels and distances are copied back as soon as they are final.
+// With pinned host memory the transfers run at full PCIe speed.
 int assign_host(emb200_handle* h, int dtype, const void* x, size_t m, uint32_t* labels, float* dist) {
     int rc = check_ready(h, dtype);
     if (rc) return rc;
@@ -465,19 +477,47 @@ int assign_host(emb200_handle* h, int dtype, const void* x, size_t m, uint32_t* 
     if (m > 0xFFFFFFFFull) return fail(h, EMB200_EINVAL, "more than 2^32 - 1 rows in one call");
     h->stats = emb200_stats{};
     cudaStream_t st = h->stream;
+    if (!h->copy_stream) CK(cudaStreamCreateWithFlags(&h->copy_stream, cudaStreamNonBlocking));
+    if (!h->ev_copied[0]) {
+        for (int b = 0; b < 2; b++) {
+            CK(cudaEventCreateWithFlags(&h->ev_copied[b], cudaEventDisableTiming));
+            CK(cudaEventCreateWithFlags(&h->ev_done[b], cudaEventDisableTiming));
+            CK(cudaEventRecord(h->ev_done[b], st));
+        }
+    }
     CK(cudaEventRecord(h->ev0, st));
     const size_t esz = elt_size(dtype);
-    const size_t chunk = std::min(m, (size_t)1 << 20);
-    if (h->stage.ensure(chunk * h->d * esz) || h->st_labels.ensure(chunk) || h->st_dist.ensure(chunk))
+    const size_t row_bytes = h->d * esz;
+    const size_t chunk = std::max<size_t>(1, std::min(m, ((size_t)64 << 20) / row_bytes));  // 64 MB per chunk
+    const size_t nch = (m + chunk - 1) / chunk;
+    if (h->stage.ensure(2 * chunk * row_bytes) || h->st_labels.ensure(chunk) || h->st_dist.ensure(chunk))
         return fail(h, EMB200_ENOMEM, "staging allocation failed");
-    for (size_t r0 = 0; r0 < m; r0 += chunk) {
-        size_t mc = std::min(chunk, m - r0);
-        CK(cudaMemcpyAsync(h->stage.p, (const uint8_t*)x + r0 * h->d * esz, mc * h->d * esz, cudaMemcpyHostToDevice, st));
-        rc = assign_dispatch(h, dtype, h->stage.p, nullptr, mc, h->st_labels.p, h->st_dist.p, st);
+    auto stage_of = [&](size_t i) { return h->stage.p + (i & 1) * chunk * row_bytes; };
+    auto copy_in = [&](size_t i) -> int {
+        const size_t r0 = i * chunk, mc = std::min(chunk, m - r0);
+        CK(cudaStreamWaitEvent(h->copy_stream, h->ev_done[i & 1], 0));  // buffer no longer read
+        CK(cudaMemcpyAsync(stage_of(i), (const uint8_t*)x + r0 * row_bytes, mc * row_bytes, cudaMemcpyHostToDevice,
+                           h->copy_stream));
+        CK(cudaEventRecord(h->ev_copied[i & 1], h->copy_stream));
+        return EMB200_OK;
+    };
+    if (m) {
+        rc = copy_in(0);
         if (rc) return rc;
+    }
+    for (size_t i = 0; i < nch; i++) {
+        const size_t r0 = i * chunk, mc = std::min(chunk, m - r0);
+        // Chunk i + 1 goes into the buffer of chunk i - 1 once that search is done.
+        if (i + 1 < nch) {
+            rc = copy_in(i + 1);
+            if (rc) return rc;
+        }
+        CK(cudaStreamWaitEvent(st, h->ev_copied[i & 1], 0));
+        rc = assign_dispatch(h, dtype, stage_of(i), nullptr, mc, h->st_labels.p, h->st_dist.p, st);
+        if (rc) return rc;
+        CK(cudaEventRecord(h->ev_done[i & 1], st));
         CK(cudaMemcpyAsync(labels + r0, h->st_labels.p, mc * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
         CK(cudaMemcpyAsync(dist + r0, h->st_dist.p, mc * sizeof(float), cudaMemcpyDeviceToHost, st));
-        CK(cudaStreamSynchronize(st));
     }
     CK(cudaEventRecord(h->ev1, st));
     CK(cudaEventSynchronize(h->ev1));
@@ -508,7 +548,8 @@ int emb200_create(int ordinal, const emb200_opts* opts, emb200_handle** out) {
     h->sm_count = prop.multiProcessorCount;
     if (opts) h->opts = *opts;
     if (cudaSetDevice(ordinal) != cudaSuccess || cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) ||
-        cudaEventCreate(&h->ev0) || cudaEventCreate(&h->ev1) || h->bounds.ensure(1)) {
+        cudaEventCreate(&h->ev0) || cudaEventCreate(&h->ev1) || cudaEventCreate(&h->evk0) ||
+        cudaEventCreate(&h->evk1) || h->bounds.ensure(1)) {
         delete h;
         return EMB200_ECUDA;
     }
@@ -529,6 +570,16 @@ int emb200_destroy(emb200_handle* h) {
     h->train.release();
     if (h->ev0) cudaEventDestroy(h->ev0);
     if (h->ev1) cudaEventDestroy(h->ev1);
+    if (h->evk0) cudaEventDestroy(h->evk0);
+    if (h->evk1) cudaEventDestroy(h->evk1);
+    if (h->copy_stream) {
+        cudaStreamSynchronize(h->copy_stream);
+        cudaStreamDestroy(h->copy_stream);
+    }
+    for (int b = 0; b < 2; b++) {
+        if (h->ev_copied[b]) cudaEventDestroy(h->ev_copied[b]);
+        if (h->ev_done[b]) cudaEventDestroy(h->ev_done[b]);
+    }
     if (h->stream) cudaStreamDestroy(h->stream);
     delete h;
     return EMB200_OK;

@@ -98,6 +98,8 @@ typedef struct {
     int32_t fast_kernel;      /* fast contraction used: 0 FP32 SIMT, 1 tcgen05 BF16, 2 exact int8 */
     int32_t fast_aborted;     /* 1 if a bounded wait in the fast kernel gave up (rows then re-searched) */
     uint64_t rows_refined;    /* uncertified rows sent through the candidate-collecting refine pass */
+    double fast_ms;           /* device time of the fast contraction kernel(s) (CUDA events, summed) */
+    uint64_t fast_launches;   /* launches of the fast contraction kernel */
 } emb200_stats;
 
 /* ---- lifecycle ---------------------------------------------------------- */
