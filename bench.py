@@ -226,7 +226,10 @@ def run_ours(args):
 
         dist.init_process_group("nccl", timeout=timedelta(seconds=600))
     emb, x = make_rows(seed=0)
-    cent = trained_centroids(emb, x, local)
+    if args.centroids == "trained":
+        cent = trained_centroids(emb, x, local)
+    else:  # profiling captures: no training launches before the measured ones
+        cent = x[np.random.default_rng(1).choice(len(x), K, replace=False)] * np.float32(0.97)
     peaks = measured_peaks()
     results = {}
     sampler = ClockSampler(local)
@@ -326,6 +329,8 @@ def main():
     ap.add_argument("--precisions", default="bf16x1,bf16,fp32", help="comma list; the first is the headline")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--rows", type=int, default=N_ROWS, help="rows per pass (profiling captures use fewer)")
+    ap.add_argument("--centroids", default="trained", choices=["trained", "sampled"],
+                    help="trained by the engine (default) or a fixed sample of rows (profiling captures)")
     args = ap.parse_args()
     set_rows(args.rows)
     args.precisions = args.precisions.split(",")
