@@ -9,6 +9,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -725,5 +726,101 @@ int emb200_resolve_recipe(size_t n, size_t d, size_t k, const emb200_config* cfg
 double emb200_scheduled_alpha(double alpha0, size_t step, size_t total) { return scheduled_alpha(alpha0, step, total); }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Search without allocation: emb200_assign_f32_noalloc.
+//
+// Some callers cannot call cudaMalloc at the moment they need a search: a host
+// program whose GPU memory is owned by its own pool or budget (a database or
+// serving runtime that forbids allocations outside its allocator), or code on a
+// latency-critical path where an allocation could stall, fragment memory or fail
+// under a full device. For them this entry point takes every input and output
+// from the caller and keeps its own working memory (centroid norms, error
+// bounds, per-row candidate pairs, the list of rows to re-search) in one static
+// device array of kNoAllocScratchBytes, which exists once per GPU that loads the
+// library and is held until the process exits. It runs the FP32 search with the
+// exact certification and re-search (CpuAssigner's bits, like every other entry
+// point), all enqueued on the caller's stream with no host synchronisation.
+//
+// Every call shares that array and finds it as the previous call left it: the
+// counters that must start at zero are cleared by each call. Two calls that
+// overlap on the GPU (concurrent streams, or several host threads) race on it;
+// the caller must order them.
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr size_t kNoAllocMaxRows = 65536;    // EMB200_NOALLOC_MAX_ROWS
+constexpr size_t kNoAllocMaxK = 262144;      // EMB200_NOALLOC_MAX_K
+constexpr size_t kNoAllocPartBytes = (size_t)8 << 20;  // per-row candidate pairs of all column splits
+constexpr size_t kNoAllocScratchBytes = 256 + 256 + kNoAllocMaxK * 4 + kNoAllocPartBytes + kNoAllocMaxRows * 8;
+
+__device__ __align__(256) uint8_t g_noalloc_scratch[kNoAllocScratchBytes];
+
+// Device address of g_noalloc_scratch per device ordinal, taken once with that
+// device current (host code must not use the symbol itself as an address).
+std::mutex g_noalloc_mu;
+void* g_noalloc_ptr[64] = {};
+
+int noalloc_scratch(void** out) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return EMB200_EDEVICE;
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_ptr[dev]) {
+        void* p = nullptr;
+        if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return EMB200_ECUDA;
+        g_noalloc_ptr[dev] = p;
+    }
+    *out = g_noalloc_ptr[dev];
+    return EMB200_OK;
+}
+
+}  // namespace
+
+extern "C" int emb200_assign_f32_noalloc(const float* x_dev, size_t m, size_t d, const float* centroids_dev,
+                                         size_t k, uint32_t* labels_dev, float* dist_dev, int match_kernel,
+                                         void* stream) {
+    if (m > kNoAllocMaxRows || k > kNoAllocMaxK) return EMB200_ELIMIT;
+    if (d == 0 || k == 0 || d > 0x7FFFFFFF) return EMB200_EINVAL;
+    if (match_kernel < 0 || match_kernel > 2) return EMB200_EINVAL;
+    if (m == 0) return EMB200_OK;
+    if (!x_dev || !centroids_dev || !labels_dev || !dist_dev) return EMB200_EINVAL;
+    void* base = nullptr;
+    int rc = noalloc_scratch(&base);
+    if (rc) return rc;
+    cudaStream_t st = (cudaStream_t)stream;
+    uint8_t* p = (uint8_t*)base;
+    Bounds* bounds = (Bounds*)p;
+    uint32_t* ctr = (uint32_t*)(p + 256);  // [0] rows to re-search, [1] certified rows
+    float* norms = (float*)(p + 512);
+    float* part_s = (float*)(p + 512 + kNoAllocMaxK * 4);
+    const int row_tiles = (int)((m + kSimtBM - 1) / kSimtBM);
+    const int ntiles = (int)((k + kSimtBN - 1) / kSimtBN);
+    const size_t pair_bytes = 2 * sizeof(float) + 2 * sizeof(uint32_t);
+    int nsplit = 1;
+    int sms = 148;
+    int dev = 0;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (row_tiles < 2 * sms) nsplit = std::min(ntiles, (2 * sms + row_tiles - 1) / row_tiles);
+    nsplit = (int)std::max<size_t>(1, std::min<size_t>((size_t)nsplit, kNoAllocPartBytes / (m * pair_bytes)));
+    uint32_t* part_i = (uint32_t*)(part_s + (size_t)nsplit * m * 2);
+    uint32_t* redo = (uint32_t*)(p + 512 + kNoAllocMaxK * 4 + kNoAllocPartBytes);
+    float* redo_theta = (float*)(redo + kNoAllocMaxRows);  // written by the certification, unused without refine
+    if (cudaMemsetAsync(p, 0, 512, st) != cudaSuccess) return EMB200_ECUDA;  // bounds and counters start at zero
+    // Norms and the certification bounds (no BF16 split: the search here is FP32).
+    k_prep_centroids<<<(unsigned)((k + 7) / 8), 256, 0, st>>>(centroids_dev, (int)k, (int)d, norms, bounds, nullptr,
+                                                              nullptr, (int)((d + 63) / 64 * 64));
+    const int vec4 = (d % 4 == 0 && ((uintptr_t)x_dev & 15) == 0 && ((uintptr_t)centroids_dev & 15) == 0) ? 1 : 0;
+    k_assign_simt<float><<<dim3(row_tiles, nsplit), kSimtThreads, 0, st>>>(
+        x_dev, nullptr, (int)m, (int)d, centroids_dev, norms, (int)k, part_s, part_i, vec4);
+    float ka, kb;
+    bound_coefficients(EMB200_PREC_FP32, EMB200_F32, d, false, &ka, &kb);
+    // No refine pass here: uncertified rows (rare with FP32 scores) go straight to the exact search.
+    k_certify<float><<<(unsigned)((m + 7) / 8), 256, 0, st>>>(
+        x_dev, nullptr, (int)m, (int)d, centroids_dev, norms, (int)k, part_s, part_i, nsplit, bounds, ka, kb,
+        match_kernel, labels_dev, dist_dev, redo, ctr, ctr + 1, nullptr, redo_theta, 0.0f, 0.0f);
+    k_research_cta<float><<<sms * 2, 256, 0, st>>>(x_dev, nullptr, (int)d, centroids_dev, norms, (int)k,
+                                                    match_kernel, redo, ctr, labels_dev, dist_dev);
+    return cudaGetLastError() == cudaSuccess ? EMB200_OK : EMB200_ECUDA;
+}
 
 #include "engine_train.inc"

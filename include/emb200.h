@@ -33,6 +33,7 @@ typedef struct emb200_handle emb200_handle;
 #define EMB200_ENOMEM -3  /* device allocation failed */
 #define EMB200_ESTATE -4  /* call out of order (e.g. assign before set_centroids) */
 #define EMB200_EDEVICE -5 /* no usable sm_100 device */
+#define EMB200_ELIMIT -6  /* size beyond the limits of emb200_assign_f32_noalloc */
 
 /* Row element types (src/lib.rs:47-71, trait Scalar: f32, i8, u8). */
 #define EMB200_F32 0
@@ -156,6 +157,32 @@ double emb200_scheduled_alpha(double alpha0, size_t step, size_t total);
  * The trained centroids also become the handle's current centroids. */
 int emb200_train(emb200_handle* h, const emb200_config* cfg, size_t k, float* centroids, uint32_t* labels,
                  double* objective, uint64_t* n_splits, emb200_recipe* recipe);
+
+/* ---- search without allocation (no counterpart in the reference) --------
+ *
+ * For callers that cannot allocate device memory when they search: programs
+ * whose GPU memory belongs to their own pool or budget (a database or serving
+ * runtime that forbids cudaMalloc outside its allocator), or latency-critical
+ * code where an allocation could stall, fragment memory or fail on a full
+ * device. The caller passes everything in device memory: x_dev (m x d f32
+ * rows), centroids_dev (k x d f32), labels_dev[m], dist_dev[m]; the work is
+ * enqueued on `stream` (cudaStream_t, NULL = the legacy default stream) with no
+ * host synchronisation, no handle and no allocation of any kind. Results are
+ * those of the FP32 search: labels and distances equal to CpuAssigner's.
+ *
+ * Working memory is one static device array (9.5 MiB) that every GPU
+ * loading the library holds until the process exits; its device address is
+ * looked up on a device's first call (so make that first call before any stream
+ * capture). All calls share it and find the previous call's contents (each call
+ * clears what must start at zero): calls that overlap on the GPU race on it and
+ * must be ordered by the caller.
+ *
+ * Limits: m <= EMB200_NOALLOC_MAX_ROWS, k <= EMB200_NOALLOC_MAX_K; larger
+ * sizes return EMB200_ELIMIT without doing anything. match_kernel: EMB200_MATCH_*. */
+#define EMB200_NOALLOC_MAX_ROWS 65536
+#define EMB200_NOALLOC_MAX_K 262144
+int emb200_assign_f32_noalloc(const float* x_dev, size_t m, size_t d, const float* centroids_dev, size_t k,
+                              uint32_t* labels_dev, float* dist_dev, int match_kernel, void* stream);
 
 #ifdef __cplusplus
 }
