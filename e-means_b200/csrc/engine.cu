@@ -409,11 +409,17 @@ int assign_rows_dev(emb200_handle* h, const T* x, const uint32_t* gather, size_t
     bound_coefficients(tc ? prec : EMB200_PREC_FP32, dtype, h->d, tc, &ka, &kb);
     bound_coefficients(EMB200_PREC_BF16, dtype, h->d, false, &ka2, &kb2);
     const int match = h->opts.match_kernel;
-    k_certify<T><<<(unsigned)((m + 7) / 8), 256, 0, st>>>(x, gather, (int)m, d, h->c.p, h->norms.p, k, h->part_s.p,
-                                                           h->part_i.p, nsplit, h->bounds.p, ka, kb, match, labels,
-                                                           dist, h->redo_rows.p, ctr, ctr + 1,
-                                                           tc ? (const int*)(ctr + 2) : nullptr, h->redo_theta.p,
-                                                           ka2, kb2);
+    if (match == kMatchAvx512) {
+        k_certify16<T><<<(unsigned)((m + 15) / 16), 256, 0, st>>>(
+            x, gather, (int)m, d, h->c.p, h->norms.p, k, h->part_s.p, h->part_i.p, nsplit, h->bounds.p, ka, kb, labels,
+            dist, h->redo_rows.p, ctr, ctr + 1, tc ? (const int*)(ctr + 2) : nullptr, h->redo_theta.p, ka2, kb2);
+    } else {
+        k_certify<T><<<(unsigned)((m + 7) / 8), 256, 0, st>>>(x, gather, (int)m, d, h->c.p, h->norms.p, k, h->part_s.p,
+                                                               h->part_i.p, nsplit, h->bounds.p, ka, kb, match, labels,
+                                                               dist, h->redo_rows.p, ctr, ctr + 1,
+                                                               tc ? (const int*)(ctr + 2) : nullptr, h->redo_theta.p,
+                                                               ka2, kb2);
+    }
     CKL();
     uint32_t nredo = 0;
     CK(cudaMemcpyAsync(&nredo, ctr, sizeof nredo, cudaMemcpyDeviceToHost, st));

@@ -217,6 +217,98 @@ __global__ void k_certify(const T* __restrict__ x, const uint32_t* __restrict__ 
     }
 }
 
+// k_certify specialised to the AVX-512 rounding (the default): one half-warp
+// per row, so a warp certifies two rows, and one pass over the row computes its
+// sqnorm lanes and both candidates' 16 FMA lanes. Same decisions and outputs as
+// k_certify with match = AVX-512.
+template <typename T>
+__global__ void k_certify16(const T* __restrict__ x, const uint32_t* __restrict__ gather, int m, int d,
+                            const float* __restrict__ c, const float* __restrict__ norms, int k,
+                            const float* __restrict__ part_s, const uint32_t* __restrict__ part_i, int nsplit,
+                            const Bounds* __restrict__ bounds, float ka, float kb,
+                            uint32_t* __restrict__ labels, float* __restrict__ dist,
+                            uint32_t* __restrict__ redo_rows, uint32_t* __restrict__ redo_count,
+                            uint32_t* __restrict__ cert_count, const int* __restrict__ fast_err,
+                            float* __restrict__ redo_theta, float ka2, float kb2) {
+    const int lane = threadIdx.x & 31, l = lane & 15, half = lane >> 4;
+    const int row = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 2 + half;
+    const bool live = row < m;
+    const int r = live ? row : m - 1;  // dead half-warps mirror a live row and write nothing
+    const size_t src = gather ? gather[r] : (size_t)r;
+    const T* xr = x + src * (size_t)d;
+    Top2 t;
+    t.init();
+    for (int s = 0; s < nsplit; s++) {
+        const size_t o = ((size_t)s * m + r) * 2;
+        t.push(part_s[o], part_i[o]);
+        t.push(part_s[o + 1], part_i[o + 1]);
+    }
+    const uint32_t j1 = t.i1 < (uint32_t)k ? t.i1 : 0u;
+    const uint32_t j2 = t.i2 < (uint32_t)k ? t.i2 : j1;
+    const float* c1 = c + (size_t)j1 * d;
+    const float* c2 = c + (size_t)j2 * d;
+    const int body = d & ~15, dr = (d + 15) & ~15;
+    float sq = 0.0f, a1 = 0.0f, a2 = 0.0f;
+    for (int i = l; i < dr; i += 16) {
+        const bool in = i < d;
+        const float xv = in ? to_f32(xr[i]) : 0.0f;
+        if (i < body) sq = __fadd_rn(sq, __fmul_rn(xv, xv));
+        a1 = __fmaf_rn(xv, in ? c1[i] : 0.0f, a1);
+        a2 = __fmaf_rn(xv, in ? c2[i] : 0.0f, a2);
+    }
+#pragma unroll
+    for (int o = 8; o; o >>= 1) {
+        a1 = __fadd_rn(a1, __shfl_xor_sync(kFull, a1, o));
+        a2 = __fadd_rn(a2, __shfl_xor_sync(kFull, a2, o));
+    }
+    float xn = -0.0f;
+    const int base = half * 16;
+#pragma unroll
+    for (int q = 0; q < 16; q++) xn = __fadd_rn(xn, __shfl_sync(kFull, sq, base + q));
+    float tail = -0.0f;
+    for (int i = body; i < d; i++) {
+        const float v = to_f32(xr[i]);
+        tail = __fadd_rn(tail, __fmul_rn(v, v));
+    }
+    xn = __fadd_rn(xn, tail);
+    if (!live || l != 0) return;
+    bool ok = t.i1 < (uint32_t)k && (k < 2 || t.i2 < (uint32_t)k);
+    const float s1 = score_ref(norms[j1], a1);
+    float sb = s1;
+    uint32_t jb = j1;
+    if (t.i2 < (uint32_t)k) {
+        const float s2 = score_ref(norms[j2], a2);
+        if (lex_less(s2, j2, sb, jb)) {
+            sb = s2;
+            jb = j2;
+        }
+    }
+    if (ok && k > 2) {
+        const float xnorm = __fmul_ru(__fsqrt_ru(fmaxf(xn, 0.0f)), 1.0000005f);
+        const float E = __fadd_ru(__fmul_ru(__fmul_ru(ka, xnorm), bounds->cmax), __fmul_ru(kb, bounds->nmax));
+        const float thr = __fsub_rd(t.s2, E);
+        ok = isfinite(E) && sb < thr;
+    }
+    if (ok && !(sb < __int_as_float(0x7f800000))) ok = false;
+    if (fast_err && *fast_err) ok = false;
+    if (ok) {
+        labels[row] = jb;
+        dist[row] = fmaxf(__fadd_rn(sb, xn), 0.0f);
+        atomicAdd(cert_count, 1u);
+    } else {
+        float theta = __int_as_float(0x7fc00000);
+        if (t.i1 < (uint32_t)k && sb < __int_as_float(0x7f800000) && sb > -__int_as_float(0x7f800000)) {
+            const float xnorm = __fmul_ru(__fsqrt_ru(fmaxf(xn, 0.0f)), 1.0000005f);
+            const float E2 = __fadd_ru(__fmul_ru(__fmul_ru(ka2, xnorm), bounds->cmax), __fmul_ru(kb2, bounds->nmax));
+            const float th = __fadd_ru(sb, E2);
+            if (isfinite(th)) theta = th;
+        }
+        const uint32_t slot = atomicAdd(redo_count, 1u);
+        redo_rows[slot] = (uint32_t)row;
+        redo_theta[slot] = theta;
+    }
+}
+
 // Exact re-score of the refine pass's candidates (one warp per refined row):
 // the reference's label is the lowest-index minimum of the exact scores of the
 // candidates, because every centroid whose exact score could reach sb was

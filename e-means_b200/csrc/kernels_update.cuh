@@ -244,6 +244,9 @@ __global__ void __launch_bounds__(1024) k_batch_objective(const float* __restric
     }
 }
 
+constexpr uint32_t kReviveSmemSort = 16384;  // donors sorted in shared memory up to this many
+constexpr size_t kReviveSmemBytes = kReviveSmemSort * (sizeof(double) + sizeof(uint32_t));
+
 // State::revive (src/lib.rs:314-344), one CTA of 1024 threads:
 //   total = sum of N (sequential f32), threshold = total tau / k,
 //   unused = {N_j < thr}, donors = {N_j >= thr, N_j > 0} in index order, each
@@ -311,14 +314,21 @@ __global__ void __launch_bounds__(1024) k_revive(int k, int d, float* __restrict
         return;
     }
     // keys/didx have room for next_pow2(k) entries; pad with -inf (sorts last).
+    // Up to kReviveSmemSort entries the sort runs in shared memory.
     uint32_t n2 = 1;
     while (n2 < ndon) n2 <<= 1;
+    extern __shared__ double sort_keys[];
+    const bool in_smem = n2 <= kReviveSmemSort;
+    double* sk = in_smem ? sort_keys : keys;
+    uint32_t* si = in_smem ? (uint32_t*)(sort_keys + kReviveSmemSort) : didx;
     for (uint32_t i = tid; i < n2; i += 1024) {
         if (i < ndon) {
-            keys[i] = log((double)usage[didx[i]]) - gstream[cur + i];
+            const uint32_t j = didx[i];
+            sk[i] = log((double)usage[j]) - gstream[cur + i];
+            si[i] = j;
         } else {
-            keys[i] = -__longlong_as_double(0x7ff0000000000000ll);
-            didx[i] = 0xffffffffu;
+            sk[i] = -__longlong_as_double(0x7ff0000000000000ll);
+            si[i] = 0xffffffffu;
         }
     }
     __syncthreads();
@@ -328,19 +338,23 @@ __global__ void __launch_bounds__(1024) k_revive(int k, int d, float* __restrict
             for (uint32_t i = tid; i < n2; i += 1024) {
                 const uint32_t pi = i ^ jj;
                 if (pi > i) {
-                    const double a = keys[i], b = keys[pi];
+                    const double a = sk[i], b = sk[pi];
                     const bool desc = (i & k2) == 0;
                     if (desc ? (a < b) : (a > b)) {
-                        keys[i] = b;
-                        keys[pi] = a;
-                        const uint32_t t = didx[i];
-                        didx[i] = didx[pi];
-                        didx[pi] = t;
+                        sk[i] = b;
+                        sk[pi] = a;
+                        const uint32_t t = si[i];
+                        si[i] = si[pi];
+                        si[pi] = t;
                     }
                 }
             }
             __syncthreads();
         }
+    }
+    if (in_smem) {
+        for (uint32_t i = tid; i < ndon; i += 1024) didx[i] = si[i];
+        __syncthreads();
     }
     const uint32_t nsplit = min(nun, ndon);
     // Each split pair is independent (distinct donors, distinct unused slots).
