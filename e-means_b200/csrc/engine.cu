@@ -20,6 +20,7 @@
 #include "kernels_i8.cuh"
 #include "kernels_simt.cuh"
 #include "kernels_tc.cuh"
+#include "kernels_tc_i8.cuh"
 #include "kernels_update.cuh"
 
 constexpr int kRefineCap = 32;  // candidates kept per refined row
@@ -88,6 +89,10 @@ struct emb200_handle {
     DevBuf<int8_t> c8;   // I8 centroids (CpuI8Assigner)
     DevBuf<long long> off8;  // I8 offsets: sum c8^2 (+ bias)
     bool bias_set = false;
+    double bias_absmax = 0.0;  // largest |bias| added since set_centroids (inf: unknown, device-computed)
+    CUtensorMap map_c8{};      // TMA descriptor of c8 (128B swizzle, 128 x 256 boxes)
+    bool map_c8_ok = false;
+    DevBuf<int> pkeys;         // per-centroid integer keys of the kind::i8 epilogue
 
     // resident rows
     DevBuf<uint8_t> rows;
@@ -241,12 +246,28 @@ int prepare_centroids(emb200_handle* h) {
                                                               (int)h->kpad);
     CKL();
     if (h->opts.centroid_bits == EMB200_CENTROIDS_I8) {
-        size_t kp8 = (h->d + 31) / 32 * 32;
+        // Rows of c8 padded to whole 128-byte swizzle atoms (the kind::i8 K atom).
+        const size_t kp8 = (h->d + 127) / 128 * 128;
         if (h->c8.ensure((size_t)k * kp8) || h->off8.ensure(k)) return fail(h, EMB200_ENOMEM, "i8 centroid allocation failed");
         k_prep_i8<<<(unsigned)((k + 7) / 8), 256, 0, st>>>(h->c.p, k, d, (int)kp8, h->c8.p, h->off8.p);
         CKL();
+        h->map_c8_ok = false;
+        if (h->d <= 512) {
+            EncodeTiledFn fn = encode_tiled_fn();
+            if (!fn) return fail(h, EMB200_ECUDA, "cuTensorMapEncodeTiled unavailable");
+            cuuint64_t dims[2] = {(cuuint64_t)kp8, (cuuint64_t)h->k};
+            cuuint64_t strides[1] = {(cuuint64_t)kp8};
+            cuuint32_t box[2] = {128, (cuuint32_t)kTcBN};
+            cuuint32_t estr[2] = {1, 1};
+            CUresult r = fn(&h->map_c8, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, h->c8.p, dims, strides, box, estr,
+                            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                            CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+            if (r != CUDA_SUCCESS) return fail(h, EMB200_ECUDA, "cuTensorMapEncodeTiled (i8) failed (%d)", (int)r);
+            h->map_c8_ok = true;
+        }
     }
     h->bias_set = false;
+    h->bias_absmax = 0.0;
     return EMB200_OK;
 }
 
@@ -261,29 +282,86 @@ int apply_bias(emb200_handle* h, const float* bias_dev) {
         CKL();
     }
     h->bias_set = true;
+    h->bias_absmax = INFINITY;  // device-computed bias: magnitude unknown on the host
     return EMB200_OK;
 }
 
 // CpuI8Assigner(I8) semantics: exact integer search, no certification needed.
+// The kind::i8 tensor-core kernel serves d <= 512 with |bias| small enough for
+// its 32-bit keys (see kernels_tc_i8.cuh); other cases use the dp4a kernel.
 int launch_i8_assign(emb200_handle* h, const int8_t* x, const uint32_t* gather, size_t m, uint32_t* labels,
                      float* dist, cudaStream_t st) {
     const int k = (int)h->k, d = (int)h->d;
-    int row_tiles = (int)((m + kI8BM - 1) / kI8BM);
-    int ntiles = (k + kI8BN - 1) / kI8BN;
-    int nsplit = 1, target = 2 * h->sm_count;
+    const size_t kp8 = (h->d + 127) / 128 * 128;
+    const bool tc = h->map_c8_ok && h->d <= 512 && h->bias_absmax <= 8.0e6;
+    int nsplit = 1;
+    const int target = tc ? h->sm_count : 2 * h->sm_count;
+    const int row_tiles = (int)((m + 127) / 128);
+    const int ntiles = tc ? (k + kTcBN - 1) / kTcBN : (k + kI8BN - 1) / kI8BN;
     if (row_tiles < target) nsplit = std::min(ntiles, (target + row_tiles - 1) / row_tiles);
+    nsplit = std::max(nsplit, 1);
     // part_s holds int64 scores here: 2 floats per entry.
-    if (h->part_s.ensure((size_t)nsplit * m * 2) || h->part_i.ensure((size_t)nsplit * m))
+    if (h->part_s.ensure((size_t)nsplit * m * 2) || h->part_i.ensure((size_t)nsplit * m) || h->counters.ensure(8))
         return fail(h, EMB200_ENOMEM, "scratch allocation failed for %zu rows", m);
-    size_t kp = (h->d + 31) / 32 * 32;
-    int xvec = (d % 16 == 0 && ((uintptr_t)x & 15) == 0) ? 1 : 0;
-    dim3 grid(row_tiles, nsplit);
-    k_assign_i8<<<grid, 256, 0, st>>>(x, gather, (int)m, d, h->c8.p, (int)kp, h->off8.p, k,
-                                      (long long*)h->part_s.p, h->part_i.p, xvec);
+    CK(cudaEventRecord(h->evk0, st));
+    if (tc) {
+        const size_t kp = (h->k + kTcBN - 1) / kTcBN * kTcBN;
+        if (h->pkeys.ensure(kp)) return fail(h, EMB200_ENOMEM, "key allocation failed");
+        k_i8_keys<<<(unsigned)((kp + 255) / 256), 256, 0, st>>>(h->off8.p, k, (int)kp, h->pkeys.p);
+        CKL();
+        CK(cudaMemsetAsync(h->counters.p + 2, 0, sizeof(uint32_t), st));
+        TcI8Params p{};
+        p.m = (int)m;
+        p.d = d;
+        p.k = k;
+        p.kpad = (int)kp8;
+        p.gather = gather;
+        p.pkeys = h->pkeys.p;
+        p.part_s = (long long*)h->part_s.p;
+        p.part_i = h->part_i.p;
+        p.err = (int*)(h->counters.p + 2);
+        const TcSmem L = tc_i8_smem_layout(p.kpad);
+        const size_t smem = std::max<size_t>(L.total + 1024, 120 * 1024);
+        static bool attr = false;
+        if (!attr) {
+            CK(cudaFuncSetAttribute(k_assign_tc_i8, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmemLimit));
+            attr = true;
+        }
+        k_assign_tc_i8<<<dim3((unsigned)row_tiles, (unsigned)nsplit), kTcThreads, smem, st>>>(x, h->map_c8, p);
+        CKL();
+    } else {
+        const int xvec = (d % 16 == 0 && ((uintptr_t)x & 15) == 0) ? 1 : 0;
+        k_assign_i8<<<dim3((unsigned)row_tiles, (unsigned)nsplit), 256, 0, st>>>(
+            x, gather, (int)m, d, h->c8.p, (int)kp8, h->off8.p, k, (long long*)h->part_s.p, h->part_i.p, xvec);
+        CKL();
+    }
+    CK(cudaEventRecord(h->evk1, st));
+    h->stats.fast_kernel = tc ? 3 : 2;
+    k_finish_i8<<<(unsigned)((m + 7) / 8), 256, 0, st>>>(x, gather, (int)m, d, (const long long*)h->part_s.p,
+                                                         h->part_i.p, nsplit, labels, dist);
     CKL();
-    k_finish_i8<<<(unsigned)((m + 255) / 256), 256, 0, st>>>(x, gather, (int)m, d, (const long long*)h->part_s.p,
-                                                             h->part_i.p, nsplit, labels, dist);
-    CKL();
+    if (tc) {  // the bounded waits gave up: redo the call with the exact dp4a kernel
+        uint32_t err = 0;
+        CK(cudaMemcpyAsync(&err, h->counters.p + 2, sizeof err, cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        float kms = 0.0f;
+        CK(cudaEventElapsedTime(&kms, h->evk0, h->evk1));
+        h->stats.fast_ms += kms;
+        h->stats.fast_launches += 1;
+        if (err) {
+            h->stats.fast_aborted = 1;
+            const int xvec = (d % 16 == 0 && ((uintptr_t)x & 15) == 0) ? 1 : 0;
+            const int ns = std::max(1, std::min((k + kI8BN - 1) / kI8BN, (2 * h->sm_count + row_tiles - 1) / row_tiles));
+            if (h->part_s.ensure((size_t)ns * m * 2) || h->part_i.ensure((size_t)ns * m))
+                return fail(h, EMB200_ENOMEM, "scratch allocation failed for %zu rows", m);
+            k_assign_i8<<<dim3((unsigned)row_tiles, (unsigned)ns), 256, 0, st>>>(
+                x, gather, (int)m, d, h->c8.p, (int)kp8, h->off8.p, k, (long long*)h->part_s.p, h->part_i.p, xvec);
+            CKL();
+            k_finish_i8<<<(unsigned)((m + 7) / 8), 256, 0, st>>>(x, gather, (int)m, d, (const long long*)h->part_s.p,
+                                                                 h->part_i.p, ns, labels, dist);
+            CKL();
+        }
+    }
     return EMB200_OK;
 }
 
@@ -648,7 +726,12 @@ int emb200_set_bias(emb200_handle* h, const float* bias, size_t k) {
     if (!h->have_centroids) return fail(h, EMB200_ESTATE, "set_centroids must be called first");
     if (!bias || k != h->k) return fail(h, EMB200_EINVAL, "bias must have k = %zu entries", h->k);
     CK(cudaMemcpyAsync(h->bias.p, bias, k * sizeof(float), cudaMemcpyHostToDevice, h->stream));
+    double amax = 0.0;
+    for (size_t j = 0; j < k; j++) amax = std::max(amax, std::fabs((double)bias[j]));
+    if (!(amax < INFINITY)) amax = INFINITY;
+    const double prev = h->bias_absmax;
     int rc = apply_bias(h, h->bias.p);
+    h->bias_absmax = prev + amax;  // biases accumulate until the next set_centroids
     if (rc) return rc;
     CK(cudaStreamSynchronize(h->stream));
     return EMB200_OK;

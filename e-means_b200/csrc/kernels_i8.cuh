@@ -184,26 +184,29 @@ k_assign_i8(const int8_t* __restrict__ x, const uint32_t* __restrict__ gather, i
 }
 
 // Merge the split partials, dist = max(|x|^2 + best, 0) computed in f64 and
-// rounded to f32 (src/cpu_i8.rs:183-186). One thread per row.
+// rounded to f32 (src/cpu_i8.rs:183-186). One warp per row.
 __global__ void k_finish_i8(const int8_t* __restrict__ x, const uint32_t* __restrict__ gather, int m, int d,
                             const long long* __restrict__ part_s, const uint32_t* __restrict__ part_i, int nsplit,
                             uint32_t* __restrict__ labels, float* __restrict__ dist) {
-    int row = blockIdx.x * blockDim.x + threadIdx.x;
+    const int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
     if (row >= m) return;
+    const size_t src = gather ? gather[row] : (size_t)row;
+    const int8_t* xr = x + src * (size_t)d;
+    long long nrm = 0;
+    for (int t = lane; t < d; t += 32) nrm += (long long)xr[t] * xr[t];
+    for (int o = 16; o; o >>= 1) nrm += __shfl_xor_sync(0xffffffffu, nrm, o);
+    if (lane != 0) return;
     long long b = 0x7fffffffffffffffll;
     uint32_t l = 0;
     for (int s = 0; s < nsplit; s++) {
-        long long v = part_s[(size_t)s * m + row];
-        uint32_t i = part_i[(size_t)s * m + row];
+        const long long v = part_s[(size_t)s * m + row];
+        const uint32_t i = part_i[(size_t)s * m + row];
         if (v < b || (v == b && i < l)) {
             b = v;
             l = i;
         }
     }
-    size_t src = gather ? gather[row] : (size_t)row;
-    const int8_t* xr = x + src * (size_t)d;
-    long long nrm = 0;
-    for (int t = 0; t < d; t++) nrm += (long long)xr[t] * xr[t];
     labels[row] = l;
     dist[row] = (float)fmax((double)nrm + (double)b, 0.0);
 }

@@ -175,6 +175,9 @@ def test_i8_mode_integer_exact(orc, assigners, shape):
     for c in (ci.astype(np.float32), ci.astype(np.float32) * np.float32(0.37) + np.float32(0.5)):
         a.set_centroids(c)
         lab, dist = a.assign(x)
+        st = a.stats()
+        # tcgen05 kind::i8 for d <= 512, the dp4a kernel beyond
+        assert st["fast_kernel"] == (3 if d <= 512 else 2) and st["fast_aborted"] == 0, st
         rl, rd = orc.i8_assign(x, c, bits=8)
         assert np.array_equal(lab, rl) and same_f32(dist, rd)
 
@@ -220,3 +223,17 @@ def test_tcgen05_path_runs_and_certifies(emb, orc, assigners, precision, d):
     assert np.array_equal(lab, rl) and same_f32(dist, rd)
     if precision == "bf16" and d >= 33:  # at d = 1 every centroid ties with others: all rows re-searched
         assert st["rows_researched"] <= 0.02 * len(x), st
+
+
+def test_i8_mode_c3_like_exact(emb, orc, assigners):
+    # The int8 workload's shape at reduced size: unit-norm 64-d-latent rows,
+    # faiss calibration to i8, d = 512, k = 512 centroids taken from the codes.
+    xf = emb.datasets.embeddings(6_000, 512, latent=64, seed=12)
+    codes, _, _ = emb.datasets.faiss_int8(xf)
+    c = codes[np.random.default_rng(3).choice(len(codes), 512, replace=False)].astype(np.float32) + np.float32(0.3)
+    a = assigners("fp32", 8)
+    a.set_centroids(c)
+    lab, dist = a.assign(codes)
+    assert a.stats()["fast_kernel"] == 3
+    rl, rd = orc.i8_assign(codes, c, bits=8)
+    assert np.array_equal(lab, rl) and same_f32(dist, rd)
