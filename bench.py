@@ -288,6 +288,97 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
+def run_c1(args):
+    """Plain e-means, the CPU-runnable configuration: 200,000 x 96 f32 rows from a
+    4096-blob mixture (centres N(0, 4^2 I), std 1, seed 0), k = 1024, 5 epochs,
+    Config::default(); final MSE from an exact assign() pass. The device trains
+    with the BF16 search (bit-exact labels), the oracle's train_cpu is timed on the
+    host cores and compared centroid for centroid."""
+    import torch
+    from __graft_entry__ import load_package
+    from oracle import oracle as orc
+
+    emb = load_package()
+    x = emb.datasets.blobs(200_000, 96, seed=0)
+    times = []
+    for i in range(args.warmup + args.steps):
+        a = emb.B200Assigner(0, precision="bf16")
+        t0 = time.perf_counter()
+        out = emb.train(x, 96, 1024, emb.Config(), assigner=a)
+        lab, dist = a.assign_resident()
+        t1 = time.perf_counter()
+        a.close()
+        if i >= args.warmup:
+            times.append(t1 - t0)
+    t = float(np.median(times))
+    rows = sum(out.recipe.epoch_rows) + len(x)
+    line = {"metric": "e-means train + exact assign, 200k x 96, k=1024, 5 epochs (rows/s)", "value": rows / t,
+            "unit": "rows/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3,
+            "higher_is_better": True, "dtype": "bf16x3->f32 search, f32 update",
+            "config": {"workload": "blobs 200,000 x 96, 4096 blobs, k=1024, Config::default()",
+                       "recipe": {"batch": out.recipe.batch_size, "alpha0": out.recipe.alpha0,
+                                  "steps": out.recipe.total_steps}},
+            "final_mse": float(dist.astype(np.float64).mean()), "n_splits": out.n_splits,
+            "note": "wall clock of the whole host call (upload, training, exact pass, copies)"}
+    if not args.no_cpu:
+        t0 = time.perf_counter()
+        ref = orc.train(x, 1024, orc.make_config(), kernel="avx512" if orc.has_kernel("avx512") else "portable",
+                        emulate=not orc.has_kernel("avx512"))
+        rl, rd = orc.cpu_assign(x, ref["centroids"], emulate=not orc.has_kernel("avx512"))
+        tc = time.perf_counter() - t0
+        line["cpu_baseline"] = {"value": rows / tc, "unit": "rows/s", "cores": os.cpu_count(), "kind": "port",
+                                "sample": f"the whole workload: train + assign in {tc:.2f} s"}
+        line["parity"] = {"centroids_bit_exact": bool(np.array_equal(ref["centroids"].view(np.uint32),
+                                                                      out.centroids.view(np.uint32))),
+                          "labels_equal": bool(np.array_equal(rl, lab)),
+                          "final_mse_reference": float(rd.astype(np.float64).mean())}
+    print(json.dumps(line), flush=True)
+
+
+def run_c3(args):
+    """int8 codes: 2,000,000 x 512 unit-norm rows quantised with the faiss
+    calibration, k = 4096 centroids trained by the engine (int8-centroid search,
+    2 epochs, untimed); one exact assign() pass with CpuI8Assigner(I8) semantics on
+    the tcgen05 kind::i8 kernel, rows resident."""
+    from __graft_entry__ import load_package
+    from oracle import oracle as orc
+
+    emb = load_package()
+    n = args.rows if args.rows != N_ROWS else 2_000_000
+    codes, _, _ = emb.datasets.embeddings_int8(n, 512, latent=64, seed=0)
+    a = emb.B200Assigner(0, precision="fp32", centroid_bits=8)
+    a.load_rows(codes)
+    out = a.train_resident(4096, emb.Config(nepochs=2.0))
+    for _ in range(args.warmup):
+        a.assign_resident(want_host=False)
+    ms, fast = [], 0.0
+    for _ in range(args.steps):
+        a.assign_resident(want_host=False)
+        st = a.stats()
+        ms.append(st["ms_total"])
+        fast += st["fast_ms"]
+    t = float(np.mean(ms))
+    ops = 2.0 * 512 * 4096 * n
+    line = {"metric": "rows/s assigned (2M x 512 int8, k=4096, CpuI8Assigner(I8) semantics)",
+            "value": n / (t / 1e3), "unit": "rows/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": t, "higher_is_better": True, "dtype": "s8 x s8 -> s32 (exact)",
+            "config": {"workload": f"{n} x 512 int8 codes (faiss calibration of 64-d-latent unit rows), k=4096",
+                       "fast_kernel": st["fast_kernel"]},
+            "roofline": {"bound": "tensor (int8)", "achieved_tops": ops / (fast / args.steps / 1e3) / 1e12,
+                         "note": "int8 dense peak not measured by the pool; nominal 4500 TOPS"}}
+    if not args.no_cpu:
+        sample = min(8192, n)
+        cores = os.cpu_count() or 1
+        t0 = time.perf_counter()
+        orc.i8_assign(codes[:sample], out.centroids, bits=8, nthreads=cores)
+        tc = time.perf_counter() - t0
+        line["cpu_baseline"] = {"value": sample / tc, "unit": "rows/s", "cores": cores, "kind": "port",
+                                "sample": f"first {sample} rows: CpuI8Assigner(I8) restated in C++ (portable "
+                                          f"integer kernel), OpenMP {cores} threads, {tc:.2f} s"}
+    a.close()
+    print(json.dumps(line), flush=True)
+
+
 def run_reference(args):
     rank, world, _ = dist_env()
     if rank != 0:
@@ -331,8 +422,14 @@ def main():
     ap.add_argument("--rows", type=int, default=N_ROWS, help="rows per pass (profiling captures use fewer)")
     ap.add_argument("--centroids", default="trained", choices=["trained", "sampled"],
                     help="trained by the engine (default) or a fixed sample of rows (profiling captures)")
+    ap.add_argument("--workload", default="c2", choices=["c2", "c1", "c3"],
+                    help="c2: the headline assign benchmark; c1, c3: the other configurations")
     args = ap.parse_args()
     set_rows(args.rows)
+    if args.workload == "c1" and args.impl == "ours":
+        return run_c1(args)
+    if args.workload == "c3" and args.impl == "ours":
+        return run_c3(args)
     args.precisions = args.precisions.split(",")
     if args.impl == "reference":
         run_reference(args)

@@ -86,3 +86,38 @@ def faiss_int8(x, target_peak=112.0):
         r[fix] -= np.copysign(np.float32(1.0), v[fix])
         codes[r0:r0 + 262_144] = np.clip(r, -128, 127).astype(np.int8)
     return codes, shift, np.float32(scale)
+
+
+def embeddings_int8(n=2_000_000, d=512, latent=64, noise=0.1, seed=0, chunk=262_144, target_peak=112.0):
+    """The int8 workload: unit-norm embedding rows (as `embeddings`) quantised with
+    the faiss calibration (per-dimension mean shift, one power-of-two scale putting
+    the largest centred magnitude at or below `target_peak`, round half away from
+    zero, clamp). Two passes over regenerated chunks, so only the int8 codes are
+    held. Returns (codes, shift, scale)."""
+    def chunks():
+        rng = np.random.default_rng(seed)
+        w = rng.standard_normal((latent, d), dtype=np.float32)
+        for r0 in range(0, n, chunk):
+            m = min(chunk, n - r0)
+            z = rng.standard_normal((m, latent), dtype=np.float32)
+            v = z @ w
+            v += rng.standard_normal((m, d), dtype=np.float32) * np.float32(noise)
+            v /= np.linalg.norm(v, axis=1, keepdims=True)
+            yield r0, v
+    total = np.zeros(d, np.float64)
+    for _, v in chunks():
+        total += v.astype(np.float64).sum(0)
+    shift = (total / n).astype(np.float32)
+    peak = np.float32(0.0)
+    for _, v in chunks():
+        peak = max(peak, np.abs(v - shift).max())
+    scale = np.float32(target_peak) / peak if peak > 0 else np.float32(1.0)
+    scale = np.float32(2.0) ** np.float32(np.floor(np.log2(np.float32(scale))))
+    codes = np.empty((n, d), np.int8)
+    for r0, v in chunks():
+        t = (v - shift) * scale
+        r = np.trunc(t + np.copysign(np.float32(0.5), t))
+        fix = np.abs(r - t) > np.float32(0.5)
+        r[fix] -= np.copysign(np.float32(1.0), t[fix])
+        codes[r0:r0 + len(v)] = np.clip(r, -128, 127).astype(np.int8)
+    return codes, shift, np.float32(scale)
