@@ -35,7 +35,7 @@ class EngineError(RuntimeError):
 
 class _Opts(ctypes.Structure):
     _fields_ = [("precision", ctypes.c_int), ("centroid_bits", ctypes.c_int), ("match_kernel", ctypes.c_int),
-                ("reserved", ctypes.c_int * 5)]
+                ("train_eager", ctypes.c_int), ("reserved", ctypes.c_int * 4)]
 
 
 class _Config(ctypes.Structure):
@@ -186,9 +186,9 @@ class B200Assigner:
     kernel's rounding the labels and distances reproduce.
     """
 
-    def __init__(self, ordinal=0, precision="fp32", centroid_bits=0, match="avx512"):
+    def __init__(self, ordinal=0, precision="fp32", centroid_bits=0, match="avx512", train_eager=False):
         self._h = ctypes.c_void_p()
-        self._opts = _Opts(PRECISIONS[precision], centroid_bits, MATCH[match])
+        self._opts = _Opts(PRECISIONS[precision], centroid_bits, MATCH[match], int(train_eager))
         rc = lib().emb200_create(ordinal, ctypes.byref(self._opts), ctypes.byref(self._h))
         if rc != 0:
             raise EngineError(f"emb200_create failed ({rc}): no usable B200 (sm_100) device")

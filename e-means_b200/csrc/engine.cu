@@ -52,12 +52,13 @@ struct DevBuf {
 
 // Device state of a training run (filled by emb200_train).
 struct TrainState {
-    DevBuf<float> usage, sums, pass_sums, batch_dist;
+    DevBuf<float> usage, sums, pass_sums, batch_dist, alphas;
+    DevBuf<int> ctl;  // [0] step, [1] epoch, [2] last pass
     DevBuf<double> pass_sums64, keys, scalars, obj, gstream;
     DevBuf<uint32_t> counts, offsets, slot, list, scratch, batch_labels, labels_all, order, didx, unused;
     DevBuf<unsigned long long> pass_counts;
     void release() {
-        usage.release(); sums.release(); pass_sums.release(); batch_dist.release();
+        usage.release(); sums.release(); pass_sums.release(); batch_dist.release(); alphas.release(); ctl.release();
         pass_sums64.release(); keys.release(); scalars.release(); obj.release(); gstream.release();
         counts.release(); offsets.release(); slot.release(); list.release(); scratch.release();
         batch_labels.release(); labels_all.release(); order.release(); didx.release(); unused.release();
@@ -290,7 +291,7 @@ int apply_bias(emb200_handle* h, const float* bias_dev) {
 // The kind::i8 tensor-core kernel serves d <= 512 with |bias| small enough for
 // its 32-bit keys (see kernels_tc_i8.cuh); other cases use the dp4a kernel.
 int launch_i8_assign(emb200_handle* h, const int8_t* x, const uint32_t* gather, size_t m, uint32_t* labels,
-                     float* dist, cudaStream_t st) {
+                     float* dist, cudaStream_t st, bool graph = false) {
     const int k = (int)h->k, d = (int)h->d;
     const size_t kp8 = (h->d + 127) / 128 * 128;
     const bool tc = h->map_c8_ok && h->d <= 512 && h->bias_absmax <= 8.0e6;
@@ -303,13 +304,14 @@ int launch_i8_assign(emb200_handle* h, const int8_t* x, const uint32_t* gather, 
     // part_s holds int64 scores here: 2 floats per entry.
     if (h->part_s.ensure((size_t)nsplit * m * 2) || h->part_i.ensure((size_t)nsplit * m) || h->counters.ensure(8))
         return fail(h, EMB200_ENOMEM, "scratch allocation failed for %zu rows", m);
-    CK(cudaEventRecord(h->evk0, st));
+    if (!graph) CK(cudaEventRecord(h->evk0, st));
     if (tc) {
         const size_t kp = (h->k + kTcBN - 1) / kTcBN * kTcBN;
         if (h->pkeys.ensure(kp)) return fail(h, EMB200_ENOMEM, "key allocation failed");
         k_i8_keys<<<(unsigned)((kp + 255) / 256), 256, 0, st>>>(h->off8.p, k, (int)kp, h->pkeys.p);
         CKL();
-        CK(cudaMemsetAsync(h->counters.p + 2, 0, sizeof(uint32_t), st));
+        // Graph replay keeps the flag sticky: the training loop clears it once and reads it at the end.
+        if (!graph) CK(cudaMemsetAsync(h->counters.p + 2, 0, sizeof(uint32_t), st));
         TcI8Params p{};
         p.m = (int)m;
         p.d = d;
@@ -335,12 +337,12 @@ int launch_i8_assign(emb200_handle* h, const int8_t* x, const uint32_t* gather, 
             x, gather, (int)m, d, h->c8.p, (int)kp8, h->off8.p, k, (long long*)h->part_s.p, h->part_i.p, xvec);
         CKL();
     }
-    CK(cudaEventRecord(h->evk1, st));
+    if (!graph) CK(cudaEventRecord(h->evk1, st));
     h->stats.fast_kernel = tc ? 3 : 2;
     k_finish_i8<<<(unsigned)((m + 7) / 8), 256, 0, st>>>(x, gather, (int)m, d, (const long long*)h->part_s.p,
                                                          h->part_i.p, nsplit, labels, dist);
     CKL();
-    if (tc) {  // the bounded waits gave up: redo the call with the exact dp4a kernel
+    if (tc && !graph) {  // the bounded waits gave up: redo the call with the exact dp4a kernel
         uint32_t err = 0;
         CK(cudaMemcpyAsync(&err, h->counters.p + 2, sizeof err, cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
@@ -387,7 +389,8 @@ int tc_nsplit(const emb200_handle* h, size_t m) {
 
 template <typename T, bool COLLECT>
 int launch_tc(emb200_handle* h, const T* x, const uint32_t* gather, const uint32_t* gather2, size_t m, int nterms,
-              const float* theta, uint32_t* cand, uint32_t* cand_count, int cap, int* err, cudaStream_t st) {
+              const float* theta, uint32_t* cand, uint32_t* cand_count, int cap, int* err, cudaStream_t st,
+              const uint32_t* m_dev = nullptr, int nsplit_override = 0) {
     TcParams p{};
     p.m = (int)m;
     p.d = (int)h->d;
@@ -405,6 +408,7 @@ int launch_tc(emb200_handle* h, const T* x, const uint32_t* gather, const uint32
     p.cand = cand;
     p.cand_count = cand_count;
     p.cand_cap = cap;
+    p.m_dev = m_dev;
     TcSmem L = tc_smem_layout(p.kpad, p.nterms);
     // At least 120 KB so that two CTAs never share an SM: each holds all 512 TMEM columns.
     size_t smem = std::max<size_t>(L.total + 1024, 120 * 1024);
@@ -413,7 +417,7 @@ int launch_tc(emb200_handle* h, const T* x, const uint32_t* gather, const uint32
         CK(cudaFuncSetAttribute(k_assign_tc<T, COLLECT>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
         attr_set = true;
     }
-    int nsplit = tc_nsplit(h, m);
+    int nsplit = nsplit_override > 0 ? nsplit_override : tc_nsplit(h, m);
     dim3 grid((unsigned)((m + kTcBM - 1) / kTcBM), (unsigned)nsplit);
     k_assign_tc<T, COLLECT><<<grid, kTcThreads, smem, st>>>(x, h->map_hi, h->map_lo, p);
     CKL();
@@ -443,13 +447,13 @@ int finish_counters(emb200_handle* h, cudaStream_t st, bool refined) {
 // [3] exhaustive rows, [4] refine abort.
 template <typename T>
 int assign_rows_dev(emb200_handle* h, const T* x, const uint32_t* gather, size_t m, uint32_t* labels, float* dist,
-                    cudaStream_t st) {
+                    cudaStream_t st, bool graph = false) {
     const int dtype = std::is_same<T, float>::value ? EMB200_F32 : (std::is_same<T, int8_t>::value ? EMB200_I8 : EMB200_U8);
     const int k = (int)h->k, d = (int)h->d;
     if (m == 0) return EMB200_OK;
     if (use_i8_mode(h, dtype)) {
         h->stats.fast_kernel = 2;
-        return launch_i8_assign(h, (const int8_t*)x, gather, m, labels, dist, st);
+        return launch_i8_assign(h, (const int8_t*)x, gather, m, labels, dist, st, graph);
     }
     const int prec = h->opts.precision;
     const int row_tiles = (int)((m + kSimtBM - 1) / kSimtBM);
@@ -470,7 +474,7 @@ int assign_rows_dev(emb200_handle* h, const T* x, const uint32_t* gather, size_t
     uint32_t* ctr = h->counters.p;
     CK(cudaMemsetAsync(ctr, 0, 8 * sizeof(uint32_t), st));
     h->stats.fast_kernel = tc ? 1 : 0;
-    CK(cudaEventRecord(h->evk0, st));
+    if (!graph) CK(cudaEventRecord(h->evk0, st));
     if (tc) {
         int rc = launch_tc<T, false>(h, x, gather, nullptr, m, fast_terms, nullptr, nullptr, nullptr, 0,
                                      (int*)(ctr + 2), st);
@@ -482,7 +486,7 @@ int assign_rows_dev(emb200_handle* h, const T* x, const uint32_t* gather, size_t
                                                          h->part_i.p, vec4);
         CKL();
     }
-    CK(cudaEventRecord(h->evk1, st));
+    if (!graph) CK(cudaEventRecord(h->evk1, st));
     float ka, kb, ka2, kb2;
     bound_coefficients(tc ? prec : EMB200_PREC_FP32, dtype, h->d, tc, &ka, &kb);
     bound_coefficients(EMB200_PREC_BF16, dtype, h->d, false, &ka2, &kb2);
@@ -499,6 +503,32 @@ int assign_rows_dev(emb200_handle* h, const T* x, const uint32_t* gather, size_t
                                                                ka2, kb2);
     }
     CKL();
+    if (graph) {
+        // No host reads: every later launch takes its row count from the device
+        // counters (grids sized for all m rows, surplus CTAs leave at once).
+        const uint32_t* exhaustive = h->redo_rows.p;
+        const uint32_t* exhaustive_count = ctr;
+        if (tc_supported(h, refine_terms)) {
+            const int cap = kRefineCap;
+            if (h->cand.ensure(m * cap) || h->cand_count.ensure(m) || h->redo2_rows.ensure(m))
+                return fail(h, EMB200_ENOMEM, "refine allocation failed for %zu rows", m);
+            CK(cudaMemsetAsync(h->cand_count.p, 0, m * sizeof(uint32_t), st));
+            const int ntl = (int)((h->k + kTcBN - 1) / kTcBN);
+            int rc = launch_tc<T, true>(h, x, gather, h->redo_rows.p, m, refine_terms, h->redo_theta.p, h->cand.p,
+                                        h->cand_count.p, cap, (int*)(ctr + 4), st, ctr, std::min(ntl, 4));
+            if (rc) return rc;
+            k_rescore_cands<T><<<(unsigned)((m + 7) / 8), 256, 0, st>>>(
+                x, gather, d, h->c.p, h->norms.p, match, h->redo_rows.p, ctr, h->cand.p, h->cand_count.p, cap,
+                (const int*)(ctr + 4), labels, dist, h->redo2_rows.p, ctr + 3);
+            CKL();
+            exhaustive = h->redo2_rows.p;
+            exhaustive_count = ctr + 3;
+        }
+        k_research_cta<T><<<h->sm_count * 2, 256, 0, st>>>(x, gather, d, h->c.p, h->norms.p, k, match, exhaustive,
+                                                            exhaustive_count, labels, dist);
+        CKL();
+        return EMB200_OK;
+    }
     uint32_t nredo = 0;
     CK(cudaMemcpyAsync(&nredo, ctr, sizeof nredo, cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));

@@ -56,6 +56,7 @@ struct TcParams {
     uint32_t* cand;           // COLLECT: [m][cand_cap] centroid indices
     uint32_t* cand_count;     // COLLECT: [m] candidates found (may exceed cand_cap)
     int cand_cap;
+    const uint32_t* m_dev;    // COLLECT: if set, the row count is min(m, *m_dev), read on the device
 };
 
 // ---- PTX wrappers -----------------------------------------------------------
@@ -208,7 +209,8 @@ EMB_DEV uint32_t sw128_offset(int r, int kc, int rows) {
 }
 
 template <typename T>
-EMB_DEV void tc_load_rows(uint8_t* smem, const TcSmem& L, const T* __restrict__ x, const TcParams& p, int row0) {
+EMB_DEV void tc_load_rows(uint8_t* smem, const TcSmem& L, const T* __restrict__ x, const TcParams& p, int row0,
+                          int m) {
     // 128 rows x (kpad / 8) chunks of 8 elements; each thread converts chunks.
     const int nchunk = p.kpad / 8;
     const int total = kTcBM * nchunk;
@@ -216,7 +218,7 @@ EMB_DEV void tc_load_rows(uint8_t* smem, const TcSmem& L, const T* __restrict__ 
         int r = t / nchunk, kc = t % nchunk;
         int g = row0 + r;
         float v[8];
-        if (g < p.m) {
+        if (g < m) {
             size_t src = p.gather2 ? (size_t)p.gather2[g] : (size_t)g;
             if (p.gather) src = p.gather[src];
             const T* xr = x + src * (size_t)p.d;
@@ -356,6 +358,13 @@ k_assign_tc(const T* __restrict__ x, const __grid_constant__ CUtensorMap map_hi,
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int row0 = blockIdx.x * kTcBM;
+    int m = p.m;
+    if (COLLECT && p.m_dev) {
+        // Row count known only on the device (graph-captured refine): CTAs past it leave at once.
+        const int md = (int)*p.m_dev;
+        m = md < m ? md : m;
+        if (row0 >= m) return;
+    }
     const int nsplit = gridDim.y;
     const int ntiles_all = (p.k + kTcBN - 1) / kTcBN;
     const int my_tiles = (int)blockIdx.y < ntiles_all ? (ntiles_all - (int)blockIdx.y + nsplit - 1) / nsplit : 0;
@@ -375,7 +384,7 @@ k_assign_tc(const T* __restrict__ x, const __grid_constant__ CUtensorMap map_hi,
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     if (warp == 1) tmem_alloc(tmem_slot, kTcTmemCols);
-    tc_load_rows(smem, L, x, p, row0);
+    tc_load_rows(smem, L, x, p, row0, m);
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     tc_fence_before();
     __syncthreads();
@@ -476,7 +485,7 @@ k_assign_tc(const T* __restrict__ x, const __grid_constant__ CUtensorMap map_hi,
         Top2 top;
         top.init();
         float theta = 0.0f;
-        if (COLLECT) theta = row < p.m ? p.theta[row] : __int_as_float(0x7fc00000);
+        if (COLLECT) theta = row < m ? p.theta[row] : __int_as_float(0x7fc00000);
         for (int t = 0; t < my_tiles; t++) {
             const int b = t & 1;
             const uint32_t bph = (uint32_t)(t >> 1) & 1u;
@@ -527,7 +536,7 @@ k_assign_tc(const T* __restrict__ x, const __grid_constant__ CUtensorMap map_hi,
                 e[3] = top.i2;
             }
             asm volatile("bar.sync 1, %0;" ::"n"(kTcEpiWarps * 32) : "memory");
-            if (cq == 0 && row < p.m) {
+            if (cq == 0 && row < m) {
 #pragma unroll
                 for (int o = 0; o < 3; o++) {
                     const uint32_t* e = mg + (o * kTcBM + r) * 4;

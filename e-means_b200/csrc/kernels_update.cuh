@@ -110,7 +110,7 @@ template <typename T>
 __global__ void k_segment_sums(const T* __restrict__ x, const uint32_t* __restrict__ rows, int d, int k,
                                const uint32_t* __restrict__ counts, const uint32_t* __restrict__ offsets,
                                uint32_t* __restrict__ list, uint32_t* __restrict__ scratch, float* __restrict__ sums,
-                               int is_last,
+                               const int* __restrict__ last_pass,
                                unsigned long long* __restrict__ pass_counts, float* __restrict__ pass_sums,
                                double* __restrict__ pass_sums64) {
     const int l = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -118,6 +118,7 @@ __global__ void k_segment_sums(const T* __restrict__ x, const uint32_t* __restri
     if (l >= k) return;
     const uint32_t c = counts[l];
     if (c == 0) return;
+    const int is_last = *last_pass;
     // Segment l sorts in scratch[2 offsets[l] ...): next_pow2(c) <= 2c entries,
     // disjoint from every other segment's region.
     const uint32_t* seg = warp_sort_segment(list + offsets[l], c, scratch + 2 * (size_t)offsets[l], lane);
@@ -143,19 +144,21 @@ __global__ void k_segment_sums(const T* __restrict__ x, const uint32_t* __restri
 
 // Last pass: labels[i] = l for every row of the batch (src/lib.rs:438-440).
 __global__ void k_store_labels(const uint32_t* __restrict__ batch_labels, const uint32_t* __restrict__ rows, int m,
-                               uint32_t* __restrict__ labels_all) {
+                               uint32_t* __restrict__ labels_all, const int* __restrict__ last_pass) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < m) labels_all[rows[i]] = batch_labels[i];
+    if (i < m && *last_pass) labels_all[rows[i]] = batch_labels[i];
 }
 
 // State::apply (src/lib.rs:287-309), one warp per cluster: N *= (1 - a) for all
 // clusters; touched ones take mass = N + a n, w = a n / mass, c += w (s/n - c)
-// (c = s/n when w == 1).
+// (c = s/n when w == 1). alpha = alphas[*step]: the host-computed cosine schedule.
 __global__ void k_apply(int k, int d, float* __restrict__ c, float* __restrict__ usage,
-                        const uint32_t* __restrict__ counts, const float* __restrict__ sums, float alpha) {
+                        const uint32_t* __restrict__ counts, const float* __restrict__ sums,
+                        const float* __restrict__ alphas, const int* __restrict__ step) {
     const int j = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (j >= k) return;
+    const float alpha = alphas[*step];
     const bool replace = alpha == 1.0f;
     float u = usage[j];
     if (!replace) u = __fmul_rn(u, __fsub_rn(1.0f, alpha));
@@ -212,7 +215,7 @@ __global__ void k_unbias_dist(float* __restrict__ dist, const uint32_t* __restri
 // the sequential sum itself when the value feeds the balance penalty.
 // One CTA of 1024; writes obj[0] += batch, mean_sqdist = batch / m.
 __global__ void __launch_bounds__(1024) k_batch_objective(const float* __restrict__ dist, int m, int sequential,
-                                                          double* __restrict__ epoch_obj,
+                                                          double* __restrict__ objective, const int* __restrict__ epoch,
                                                           double* __restrict__ mean_sqdist) {
     __shared__ double part[1024];
     double s = 0.0;
@@ -239,7 +242,7 @@ __global__ void __launch_bounds__(1024) k_batch_objective(const float* __restric
         s = part[0];
     }
     if (threadIdx.x == 0) {
-        *epoch_obj += s;
+        objective[*epoch] += s;
         *mean_sqdist = s / (double)m;
     }
 }
@@ -260,10 +263,12 @@ __global__ void __launch_bounds__(1024) k_revive(int k, int d, float* __restrict
                                                  unsigned long long* __restrict__ cursor, double* __restrict__ keys,
                                                  uint32_t* __restrict__ didx, uint32_t* __restrict__ unused,
                                                  unsigned long long* __restrict__ n_splits,
-                                                 unsigned long long capacity) {
+                                                 unsigned long long capacity, const int* __restrict__ step,
+                                                 int every) {
     __shared__ float thr_s;
     __shared__ uint32_t wsum_u[32], wsum_d[32];
     __shared__ uint32_t nun_s, ndon_s;
+    if ((*step + 1) % every != 0 || !(tau > 0.0f)) return;  // every 5th step (src/lib.rs:463-465)
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     if (tid == 0) {
         float total = -0.0f;
@@ -385,6 +390,8 @@ __global__ void __launch_bounds__(1024) k_revive(int k, int d, float* __restrict
         *n_splits += nsplit;
     }
 }
+
+__global__ void k_step_incr(int* step) { *step += 1; }
 
 // Closing mean (src/lib.rs:481-489): c_j = pass_sum_j * (1 / pass_count_j) when
 // the last pass assigned rows to j (f32), or the FP64 sums divided in f64.

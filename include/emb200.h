@@ -63,7 +63,9 @@ typedef struct {
     int precision;     /* EMB200_PREC_* (default FP32) */
     int centroid_bits; /* EMB200_CENTROIDS_* (default F32) */
     int match_kernel;  /* EMB200_MATCH_* (default AVX512) */
-    int reserved[5];
+    int train_eager;   /* 1: launch the training loop's kernels one by one instead of
+                          capturing each epoch as a CUDA graph and replaying it (default 0) */
+    int reserved[4];
 } emb200_opts;
 
 /* Config, src/lib.rs:104-124. Optional fields use sentinels:

@@ -130,3 +130,18 @@ def test_assign_after_training_uses_trained_centroids(emb, orc):
     rl, rd = orc.cpu_assign(x, out.centroids, emulate=True)
     assert np.array_equal(lab, rl) and same_f32(dist, rd)
     a.close()
+
+
+@pytest.mark.parametrize("precision", ["fp32", "bf16"])
+def test_graph_replay_equals_eager_launches(emb, orc, precision):
+    # The training loop replays one captured CUDA graph per epoch length; launching
+    # the same kernels one by one must give the same bits (and both the oracle's).
+    x = emb.datasets.blobs(12_000, 24, n_blobs=80, seed=14)
+    outs = []
+    for eager in (False, True):
+        a = emb.B200Assigner(0, precision=precision, train_eager=eager)
+        outs.append(emb.train(x, 24, 60, emb.Config(nepochs=2.5), assigner=a))
+        a.close()
+    ref = orc.train(x, 60, orc.make_config(nepochs=2.5), emulate=not orc.has_kernel("avx512"))
+    for out in outs:
+        check_same(out, ref)
