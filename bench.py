@@ -379,6 +379,72 @@ def run_c3(args):
     print(json.dumps(line), flush=True)
 
 
+def run_c4(args):
+    """Batched uneven instances (configuration 4): (a) PQ training, 4,000,000 x 128
+    Gaussian-mixture rows split into 16 sub-spaces of d=8, k=256 each; (b) 48 IVF
+    lists, d=64, log-normal sizes (median 20,000, clipped to [2,000, 200,000]),
+    k = max(16, n/256). 5 epochs each. All instances of a case train at once
+    (emb200_train_batched: one stream and one graph-replayed epoch loop per
+    instance); the same instances trained one after the other with per-kernel
+    launches are timed beside it."""
+    from __graft_entry__ import load_package
+    from oracle import oracle as orc
+
+    emb = load_package()
+    case = args.workload[-1]
+    if case == "a":
+        x = emb.datasets.pq_subspaces(4_000_000, 128, 16, seed=0)
+        n = 4_000_000
+        inst = [(s * n, n, 256) for s in range(16)]
+        label = "PQ: 4,000,000 x 128 Gaussian mixture, 16 sub-spaces of d=8, k=256 each"
+    else:
+        x, sizes, ks = emb.datasets.ivf_lists(48, 64, seed=0)
+        starts = np.concatenate([[0], np.cumsum(sizes)[:-1]])
+        inst = [(int(a), int(b), int(c)) for a, b, c in zip(starts, sizes, ks)]
+        label = f"IVF: 48 lists of d=64, {int(sizes.sum())} rows, sizes {int(sizes.min())}..{int(sizes.max())}"
+    cfg = emb.Config()
+    a = emb.B200Assigner(0, precision="fp32")
+    a.load_rows(x)
+    d = x.shape[1]
+    epoch_rows = sum(sum(emb.resolve_recipe(nn, d, kk, cfg).epoch_rows) for (_, nn, kk) in inst)
+    times = []
+    for i in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        outs = a.train_batched(inst, cfg, max_concurrency=16)
+        t1 = time.perf_counter()
+        if i >= args.warmup:
+            times.append(t1 - t0)
+    t = float(np.median(times))
+    a.close()
+    # Sequential, per-kernel launches, one instance after the other.
+    b = emb.B200Assigner(0, precision="fp32", train_eager=True)
+    b.load_rows(x)
+    t0 = time.perf_counter()
+    seq = b.train_batched(inst, cfg, max_concurrency=1)
+    t_seq = time.perf_counter() - t0
+    b.close()
+    same = all(np.array_equal(o.centroids.view(np.uint32), q.centroids.view(np.uint32)) for o, q in zip(outs, seq))
+    line = {"metric": f"batched e-means training, rows/s over all instances ({label}, 5 epochs)",
+            "value": epoch_rows / t, "unit": "rows/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": t * 1e3, "higher_is_better": True, "dtype": "f32",
+            "config": {"workload": label, "instances": len(inst), "epoch_rows_total": epoch_rows,
+                       "recipe_first": vars(emb.resolve_recipe(inst[0][1], d, inst[0][2], cfg))},
+            "sequential_eager_ms": t_seq * 1e3, "speedup_vs_sequential_eager": t_seq / t,
+            "batched_equals_sequential": bool(same),
+            "note": "wall clock of the whole host call, rows resident"}
+    if not args.no_cpu:
+        r0, nn, kk = inst[0]
+        t0 = time.perf_counter()
+        orc.train(x[r0:r0 + nn], kk, orc.make_config(), kernel="avx512" if orc.has_kernel("avx512") else "portable",
+                  emulate=not orc.has_kernel("avx512"))
+        tc = time.perf_counter() - t0
+        rows0 = sum(emb.resolve_recipe(nn, d, kk, cfg).epoch_rows)
+        line["cpu_baseline"] = {"value": rows0 / tc, "unit": "rows/s", "cores": os.cpu_count(), "kind": "port",
+                                "sample": f"instance 0 of {len(inst)} ({nn} rows, k={kk}) trained by the oracle's "
+                                          f"train_cpu restatement in {tc:.2f} s"}
+    print(json.dumps(line), flush=True)
+
+
 def run_reference(args):
     rank, world, _ = dist_env()
     if rank != 0:
@@ -422,7 +488,7 @@ def main():
     ap.add_argument("--rows", type=int, default=N_ROWS, help="rows per pass (profiling captures use fewer)")
     ap.add_argument("--centroids", default="trained", choices=["trained", "sampled"],
                     help="trained by the engine (default) or a fixed sample of rows (profiling captures)")
-    ap.add_argument("--workload", default="c2", choices=["c2", "c1", "c3"],
+    ap.add_argument("--workload", default="c2", choices=["c2", "c1", "c3", "c4a", "c4b"],
                     help="c2: the headline assign benchmark; c1, c3: the other configurations")
     args = ap.parse_args()
     set_rows(args.rows)
@@ -430,6 +496,8 @@ def main():
         return run_c1(args)
     if args.workload == "c3" and args.impl == "ours":
         return run_c3(args)
+    if args.workload in ("c4a", "c4b") and args.impl == "ours":
+        return run_c4(args)
     args.precisions = args.precisions.split(",")
     if args.impl == "reference":
         run_reference(args)

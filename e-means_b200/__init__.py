@@ -92,6 +92,7 @@ def lib():
     L.emb200_scheduled_alpha.restype = ctypes.c_double
     L.emb200_scheduled_alpha.argtypes = [ctypes.c_double, S, S]
     L.emb200_train.argtypes = [P, ctypes.POINTER(_Config), S, P, P, P, P, ctypes.POINTER(_Recipe)]
+    L.emb200_train_batched.argtypes = [P, ctypes.POINTER(_Config), P, S, S, P, P, P, P]
     _lib = L
     return L
 
@@ -280,6 +281,32 @@ class B200Assigner:
         s = _Stats()
         self._check(lib().emb200_get_stats(self._h, ctypes.byref(s)))
         return {f: getattr(s, f) for f, _ in _Stats._fields_}
+
+    def train_batched(self, instances, cfg: Optional[Config] = None, max_concurrency=0):
+        """train() for independent instances over row ranges of the resident rows.
+
+        instances: [(row0, n, k), ...]. Returns one Output per instance (labels in
+        the instance's own row order). The instances run concurrently on their own
+        streams with graph-replayed epochs."""
+        cfg = cfg or Config()
+        n_all, d = self.rows_shape
+        inst = np.array([[r0, n, k] for (r0, n, k) in instances], np.uint64).reshape(-1, 3)
+        recs = [resolve_recipe(int(n), d, int(k), cfg) for (_, n, k) in instances]
+        cent = np.empty(int(sum(int(k) for (_, _, k) in instances)) * d, np.float32)
+        labels = np.empty(int(sum(int(n) for (_, n, _) in instances)), np.uint32)
+        obj = np.empty(sum(len(r.epoch_rows) for r in recs), np.float64)
+        ns = np.zeros(len(instances), np.uint64)
+        c = cfg._c()
+        self._check(lib().emb200_train_batched(self._h, ctypes.byref(c), _p(inst), len(instances), max_concurrency,
+                                               _p(cent), _p(labels), _p(obj), _p(ns)))
+        outs, co, lo, oo = [], 0, 0, 0
+        for i, (_, n, k) in enumerate(instances):
+            n, k = int(n), int(k)
+            ne = len(recs[i].epoch_rows)
+            outs.append(Output(cent[co:co + k * d].reshape(k, d), labels[lo:lo + n], obj[oo:oo + ne], int(ns[i]),
+                               recs[i]))
+            co, lo, oo = co + k * d, lo + n, oo + ne
+        return outs
 
     def train_resident(self, k, cfg: Optional[Config] = None) -> Output:
         """train (src/lib.rs:348-491) on the resident rows, entirely on the device."""

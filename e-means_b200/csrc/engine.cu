@@ -8,8 +8,10 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <atomic>
 #include <cstring>
 #include <mutex>
+#include <thread>
 #include <string>
 #include <vector>
 
@@ -97,6 +99,7 @@ struct emb200_handle {
 
     // resident rows
     DevBuf<uint8_t> rows;
+    const void* rows_view = nullptr;  // rows owned by another handle (batched instances)
     int rows_dtype = -1;
     size_t rows_n = 0, rows_d = 0;
     DevBuf<uint32_t> res_labels;
@@ -189,15 +192,14 @@ typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t,
 
 EncodeTiledFn encode_tiled_fn() {
     static EncodeTiledFn fn = nullptr;
-    static bool tried = false;
-    if (!tried) {
-        tried = true;
+    static std::once_flag once;
+    std::call_once(once, [] {
         void* p = nullptr;
         cudaDriverEntryPointQueryResult q;
         if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
             q == cudaDriverEntryPointSuccess)
             fn = (EncodeTiledFn)p;
-    }
+    });
     return fn;
 }
 

@@ -121,3 +121,31 @@ def embeddings_int8(n=2_000_000, d=512, latent=64, noise=0.1, seed=0, chunk=262_
         r[fix] -= np.copysign(np.float32(1.0), t[fix])
         codes[r0:r0 + len(v)] = np.clip(r, -128, 127).astype(np.int8)
     return codes, shift, np.float32(scale)
+
+
+def pq_subspaces(n=4_000_000, d=128, sub=16, seed=0):
+    """Product-quantisation training data: `gaussian_mixture` rows split into `sub`
+    contiguous sub-spaces of d/sub dimensions, returned sub-space-major as one
+    (sub * n) x (d / sub) matrix: sub-space s is rows [s n, (s + 1) n)."""
+    x = gaussian_mixture(n, d, seed=seed)
+    ds = d // sub
+    out = np.empty((sub * n, ds), np.float32)
+    for s in range(sub):
+        out[s * n:(s + 1) * n] = x[:, s * ds:(s + 1) * ds]
+    return out
+
+
+def ivf_lists(lists=48, d=64, median=20_000, seed=0):
+    """IVF-list refinement data: per list a local Gaussian mixture (its own centre,
+    64 sub-clusters of spread 0.5 around it), list sizes log-normal with median
+    `median` clipped to [2,000, 200,000]. Returns (rows concatenated list by list,
+    sizes, k per list = max(16, n // 256))."""
+    sizes, ks = ivf_list_sizes(lists, median, seed=seed)
+    rng = np.random.default_rng(seed + 1)
+    parts = []
+    for n in sizes:
+        centre = rng.standard_normal(d, dtype=np.float32) * np.float32(4.0)
+        subs = centre + rng.standard_normal((64, d), dtype=np.float32)
+        rows = subs[rng.integers(0, 64, int(n))] + rng.standard_normal((int(n), d), dtype=np.float32) * np.float32(0.5)
+        parts.append(rows.astype(np.float32))
+    return np.concatenate(parts), sizes, ks

@@ -160,6 +160,24 @@ double emb200_scheduled_alpha(double alpha0, size_t step, size_t total);
 int emb200_train(emb200_handle* h, const emb200_config* cfg, size_t k, float* centroids, uint32_t* labels,
                  double* objective, uint64_t* n_splits, emb200_recipe* recipe);
 
+/* ---- batched instances (PQ sub-codebooks, IVF lists) ----
+ *
+ * train() (src/lib.rs:348-491) run for `count` independent instances at once,
+ * each over rows [row0, row0 + n) of the resident rows (same d and dtype, same
+ * config) with its own k. Instances run concurrently, each on its own stream
+ * with its epochs replayed as CUDA graphs, at most max_concurrency at a time
+ * (0: 16). Outputs are concatenated in instance order: centroids sum(k_i) x d,
+ * labels sum(n_i) (instance-local row order), objective sum(n_epochs_i),
+ * n_splits[count]. Each instance's results equal a single train() call's. */
+typedef struct {
+    uint64_t row0;
+    uint64_t n;
+    uint64_t k;
+} emb200_instance;
+int emb200_train_batched(emb200_handle* h, const emb200_config* cfg, const emb200_instance* inst, size_t count,
+                         size_t max_concurrency, float* centroids, uint32_t* labels, double* objective,
+                         uint64_t* n_splits);
+
 /* ---- search without allocation (no counterpart in the reference) --------
  *
  * For callers that cannot allocate device memory when they search: programs

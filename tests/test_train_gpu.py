@@ -145,3 +145,29 @@ def test_graph_replay_equals_eager_launches(emb, orc, precision):
     ref = orc.train(x, 60, orc.make_config(nepochs=2.5), emulate=not orc.has_kernel("avx512"))
     for out in outs:
         check_same(out, ref)
+
+
+def test_batched_instances_equal_single_runs(emb, orc):
+    # Uneven instances over row ranges of one resident matrix (IVF-list-like):
+    # each result must equal its own train() call, bit for bit.
+    rng = np.random.default_rng(15)
+    sizes = [3000, 9000, 1500, 6000, 12000, 2500]
+    ks = [16, 40, 16, 30, 60, 20]
+    parts = [emb.datasets.blobs(n, 32, n_blobs=50, seed=100 + i) + rng.standard_normal(32).astype(np.float32) * 5
+             for i, n in enumerate(sizes)]
+    x = np.concatenate(parts).astype(np.float32)
+    starts = np.concatenate([[0], np.cumsum(sizes)[:-1]])
+    cfg = emb.Config(nepochs=3.0)
+    a = emb.B200Assigner(0, precision="fp32")
+    a.load_rows(x)
+    outs = a.train_batched([(int(s0), n, k) for s0, n, k in zip(starts, sizes, ks)], cfg, max_concurrency=4)
+    a.close()
+    for i, (n, k) in enumerate(zip(sizes, ks)):
+        b = emb.B200Assigner(0, precision="fp32")
+        single = emb.train(parts[i], 32, k, cfg, assigner=b)
+        b.close()
+        assert np.array_equal(outs[i].labels, single.labels)
+        assert same_f32(outs[i].centroids, single.centroids)
+        assert outs[i].n_splits == single.n_splits
+    ref = orc.train(parts[4], ks[4], orc.make_config(nepochs=3.0), emulate=not orc.has_kernel("avx512"))
+    check_same(outs[4], ref)
