@@ -59,7 +59,12 @@ struct TrainState {
     DevBuf<double> pass_sums64, keys, scalars, obj, gstream;
     DevBuf<uint32_t> counts, offsets, slot, list, scratch, batch_labels, labels_all, order, didx, unused;
     DevBuf<unsigned long long> pass_counts;
+    uint32_t* order_host = nullptr;  // pinned staging of the epoch's row order
+    size_t order_host_n = 0;
     void release() {
+        if (order_host) cudaFreeHost(order_host);
+        order_host = nullptr;
+        order_host_n = 0;
         usage.release(); sums.release(); pass_sums.release(); batch_dist.release(); alphas.release(); ctl.release();
         pass_sums64.release(); keys.release(); scalars.release(); obj.release(); gstream.release();
         counts.release(); offsets.release(); slot.release(); list.release(); scratch.release();
