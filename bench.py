@@ -445,6 +445,118 @@ def run_c4(args):
     print(json.dumps(line), flush=True)
 
 
+def run_c5(args):
+    """Learned proposer at large k: 10,000,000 x 96 heavy-tailed rows (Student-t
+    nu=3 latents in 32 dims through a random 32 x 96 map, 8192-component mixture),
+    k = 65536 centroids trained by the engine (5 epochs, BF16 search, untimed).
+    The proposer groups the centroids into 256 groups (e-means on the centroids),
+    its network 96 -> 512 -> 512 -> 256 is trained on the training run's labels,
+    and the final assign scores each row against its top 8 groups only. Timed
+    beside it: the full exact search (tcgen05 BF16 and the plain FP32 path) and
+    the same grouped search driven by the nearest group centroids."""
+    from __graft_entry__ import load_package
+    from oracle import oracle as orc
+
+    emb = load_package()
+    n = args.rows if args.rows != N_ROWS else 10_000_000
+    d, k, groups, top = 96, 65536, 256, 8
+    t0 = time.perf_counter()
+    x = emb.datasets.heavy_tailed(n, d, latent=32, components=8192, nu=3.0, seed=0)
+    t_data = time.perf_counter() - t0
+    a = emb.B200Assigner(0, precision="bf16x1")
+    a.load_rows(x)
+    t0 = time.perf_counter()
+    out = a.train_resident(k, emb.Config(nepochs=5.0))
+    t_train = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    a.proposer_init(groups=groups, hidden=512, top=top, seed=7)
+    t_group = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    losses = a.proposer_train(out.labels, args.proposer_steps)
+    t_fit = time.perf_counter() - t0
+
+    def timed(fn):
+        for _ in range(args.warmup):
+            fn()
+        ms, st = [], None
+        for _ in range(args.steps):
+            fn()
+            st = a.stats()
+            ms.append(st["ms_total"])
+        return float(np.mean(ms)), st
+
+    sampler = ClockSampler(0)
+    with sampler:
+        t_full, st_full = timed(lambda: a.assign_resident(want_host=False))
+        a.proposer_set("mlp", top, args.confidence)
+        t_mlp, st_mlp = timed(lambda: a.assign_proposed(want_host=False))
+        a.proposer_set("centroids", top, 0.0)
+        t_cen, st_cen = timed(lambda: a.assign_proposed(want_host=False))
+    lab_f, dist_f = a.assign_resident()
+    a.proposer_set("mlp", top, args.confidence)
+    lab_m, dist_m = a.assign_proposed()
+    a.proposer_set("centroids", top, 0.0)
+    lab_c, dist_c = a.assign_proposed()
+    mse_f = float(dist_f.astype(np.float64).mean())
+    # FP64 brute force on a sample of rows: agreement of each path's labels
+    sample = np.random.default_rng(3).choice(n, 4096, replace=False)
+    bl, _ = orc.bruteforce_f64(x[sample], out.centroids)
+    a.close()
+    # the plain FP32 path on the first rows (its pass over all rows would take minutes)
+    m32 = min(n, 1_000_000)
+    b = emb.B200Assigner(0, precision="fp32")
+    b.set_centroids(out.centroids)
+    b.load_rows(x[:m32])
+    b.assign_resident(want_host=False)
+    b.assign_resident(want_host=False)
+    t_fp32 = b.stats()["ms_total"] * n / m32
+    b.close()
+    flops_row = 2.0 * (96 * 512 + 512 * 512 + 512 * 256)
+    peaks = measured_peaks()
+
+    def entry(t, st, lab, dist):
+        return {"rows_per_s": n / (t / 1e3), "ms_per_step": t, "recall_at_1": float(np.mean(lab == lab_f)),
+                "mse_delta": float(dist.astype(np.float64).mean()) / mse_f - 1.0,
+                "agreement_fp64_sample": float(np.mean(lab[sample] == bl)),
+                "propose_ms": st["propose_ms"], "grouped_search_ms": st["fast_ms"],
+                "rows_lowconf": st["rows_lowconf"], "rows_refined": st["rows_refined"],
+                "rows_researched": st["rows_researched"], "kernel_launches": st["kernel_launches"]}
+
+    line = {"metric": "rows/s assigned (10M x 96 heavy-tailed, k=65536): learned proposer vs full search",
+            "value": n / (t_mlp / 1e3), "unit": "rows/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": t_mlp, "higher_is_better": True, "dtype": "bf16 -> f32 accumulate",
+            "config": {"workload": f"{n} x {d} heavy-tailed rows (Student-t nu=3, 8192 components), k={k}, "
+                                   f"{groups} groups, top {top}, network 96-512-512-256",
+                       "confidence": args.confidence, "proposer_steps": args.proposer_steps,
+                       "l2": "no flush: the resident rows (3.8 GB) exceed the 126 MB L2"},
+            "learned": entry(t_mlp, st_mlp, lab_m, dist_m),
+            "group_centroids": entry(t_cen, st_cen, lab_c, dist_c),
+            "full_search_bf16": {"rows_per_s": n / (t_full / 1e3), "ms_per_step": t_full,
+                                 "agreement_fp64_sample": float(np.mean(lab_f[sample] == bl)),
+                                 "fast_kernel_ms": st_full["fast_ms"]},
+            "full_search_fp32": {"rows_per_s": n / (t_fp32 / 1e3), "ms_per_step": t_fp32,
+                                 "note": f"timed on the first {m32} rows, scaled"},
+            "speedup_vs_full_bf16": t_full / t_mlp, "speedup_vs_fp32_path": t_fp32 / t_mlp,
+            "network_roofline": {"bound": "tensor", "achieved": flops_row * n / (st_mlp["propose_ms"] / 1e3) / 1e12,
+                                 "peak": peaks["bf16_tflops_sustained"], "unit": "TFLOP/s",
+                                 "kernel": "k_gemm_bf16 x3 + k_mlp_input + k_topm_groups (forward pass)"},
+            "times_s": {"data": t_data, "train": t_train, "grouping": t_group, "network_fit": t_fit},
+            "fit_loss_first_last": [float(losses[:20].mean()), float(losses[-20:].mean())],
+            "gpu_launches": st_mlp["kernel_launches"], "clocks": sampler.summary()}
+    line["network_roofline"]["frac"] = line["network_roofline"]["achieved"] / line["network_roofline"]["peak"]
+    if not args.no_cpu:
+        cores = os.cpu_count() or 1
+        rows = 8192
+        kern = "avx512" if orc.has_kernel("avx512") else "portable"
+        t0 = time.perf_counter()
+        orc.cpu_assign(x[:rows], out.centroids, kernel=kern, nthreads=cores)
+        tc = time.perf_counter() - t0
+        line["cpu_baseline"] = {"value": rows / tc, "unit": "rows/s", "cores": cores, "kind": "port",
+                                "sample": f"first {rows} rows, k={k}: CpuAssigner ({kern}) restated in C++, "
+                                          f"OpenMP {cores} threads, {tc:.2f} s"}
+    print(json.dumps(line), flush=True)
+
+
 def run_reference(args):
     rank, world, _ = dist_env()
     if rank != 0:
@@ -488,8 +600,10 @@ def main():
     ap.add_argument("--rows", type=int, default=N_ROWS, help="rows per pass (profiling captures use fewer)")
     ap.add_argument("--centroids", default="trained", choices=["trained", "sampled"],
                     help="trained by the engine (default) or a fixed sample of rows (profiling captures)")
-    ap.add_argument("--workload", default="c2", choices=["c2", "c1", "c3", "c4a", "c4b"],
-                    help="c2: the headline assign benchmark; c1, c3: the other configurations")
+    ap.add_argument("--workload", default="c2", choices=["c2", "c1", "c3", "c4a", "c4b", "c5"],
+                    help="c2: the headline assign benchmark; the others: the remaining configurations")
+    ap.add_argument("--proposer-steps", type=int, default=2000, help="c5: Adam steps of the network")
+    ap.add_argument("--confidence", type=float, default=0.0, help="c5: confidence threshold of the proposer")
     args = ap.parse_args()
     set_rows(args.rows)
     if args.workload == "c1" and args.impl == "ours":
@@ -498,6 +612,8 @@ def main():
         return run_c3(args)
     if args.workload in ("c4a", "c4b") and args.impl == "ours":
         return run_c4(args)
+    if args.workload == "c5" and args.impl == "ours":
+        return run_c5(args)
     args.precisions = args.precisions.split(",")
     if args.impl == "reference":
         run_reference(args)

@@ -53,7 +53,18 @@ class _Stats(ctypes.Structure):
     _fields_ = [("rows", ctypes.c_uint64), ("rows_certified", ctypes.c_uint64), ("rows_researched", ctypes.c_uint64),
                 ("kernel_launches", ctypes.c_uint64), ("ms_total", ctypes.c_double), ("fast_kernel", ctypes.c_int32),
                 ("fast_aborted", ctypes.c_int32), ("rows_refined", ctypes.c_uint64), ("fast_ms", ctypes.c_double),
-                ("fast_launches", ctypes.c_uint64)]
+                ("fast_launches", ctypes.c_uint64), ("rows_proposed", ctypes.c_uint64),
+                ("rows_lowconf", ctypes.c_uint64), ("propose_ms", ctypes.c_double)]
+
+
+class _ProposerConfig(ctypes.Structure):
+    _fields_ = [("groups", ctypes.c_uint32), ("hidden", ctypes.c_uint32), ("top", ctypes.c_uint32),
+                ("mode", ctypes.c_uint32), ("confidence", ctypes.c_float), ("batch", ctypes.c_uint32),
+                ("lr", ctypes.c_float), ("group_epochs", ctypes.c_float), ("seed", ctypes.c_uint64),
+                ("reserved", ctypes.c_uint32 * 4)]
+
+
+PROPOSER_MODES = {"mlp": 0, "centroids": 1}
 
 
 def build(force=False):
@@ -93,6 +104,18 @@ def lib():
     L.emb200_scheduled_alpha.argtypes = [ctypes.c_double, S, S]
     L.emb200_train.argtypes = [P, ctypes.POINTER(_Config), S, P, P, P, P, ctypes.POINTER(_Recipe)]
     L.emb200_train_batched.argtypes = [P, ctypes.POINTER(_Config), P, S, S, P, P, P, P]
+    L.emb200_proposer_init.argtypes = [P, ctypes.POINTER(_ProposerConfig)]
+    L.emb200_proposer_train.argtypes = [P, P, S, ctypes.c_uint32, P]
+    L.emb200_proposer_set.argtypes = [P, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_float]
+    L.emb200_proposer_param_count.restype = S
+    L.emb200_proposer_param_count.argtypes = [P]
+    L.emb200_proposer_get_params.argtypes = [P, P, S]
+    L.emb200_proposer_set_params.argtypes = [P, P, S]
+    L.emb200_proposer_grad.argtypes = [P, P, P, S, P, P]
+    L.emb200_proposer_groups.argtypes = [P, P]
+    L.emb200_propose.argtypes = [P, P, S, P, P]
+    L.emb200_assign_proposed_resident.argtypes = [P, P, P]
+    L.emb200_assign_proposed_device.argtypes = [P, P, S, P, P, P]
     _lib = L
     return L
 
@@ -307,6 +330,73 @@ class B200Assigner:
                                recs[i]))
             co, lo, oo = co + k * d, lo + n, oo + ne
         return outs
+
+    # ---- learned proposer ------------------------------------------------
+    def proposer_init(self, groups=256, hidden=512, top=8, mode="mlp", confidence=0.0, batch=4096, lr=2e-3,
+                      group_epochs=5.0, seed=1234):
+        """Group the current centroids (e-means with k = groups on the centroids),
+        build the group-sorted copy and initialise the network d -> hidden ->
+        hidden -> groups (input statistics from the resident rows)."""
+        c = _ProposerConfig(groups, hidden, top, PROPOSER_MODES[mode], confidence, batch, lr, group_epochs, seed)
+        self._check(lib().emb200_proposer_init(self._h, ctypes.byref(c)))
+        self.proposer_top = top
+
+    def proposer_train(self, labels, steps):
+        """Adam steps on mini-batches of resident rows labelled by `labels` (one
+        per resident row, UINT32_MAX = skip). Returns the per-step mean losses."""
+        lab = np.ascontiguousarray(labels, np.uint32)
+        losses = np.zeros(steps, np.float32)
+        self._check(lib().emb200_proposer_train(self._h, _p(lab), lab.size, steps, _p(losses)))
+        return losses
+
+    def proposer_set(self, mode="mlp", top=8, confidence=0.0):
+        self._check(lib().emb200_proposer_set(self._h, PROPOSER_MODES[mode], top, confidence))
+        self.proposer_top = top
+
+    def proposer_params(self):
+        n = lib().emb200_proposer_param_count(self._h)
+        out = np.empty(n, np.float32)
+        self._check(lib().emb200_proposer_get_params(self._h, _p(out), n))
+        return out
+
+    def set_proposer_params(self, params):
+        p = np.ascontiguousarray(params, np.float32)
+        self._check(lib().emb200_proposer_set_params(self._h, _p(p), p.size))
+
+    def proposer_grad(self, x, targets):
+        """(mean cross-entropy, gradient in the parameter layout) on host rows."""
+        x = np.ascontiguousarray(x, np.float32)
+        t = np.ascontiguousarray(targets, np.uint32)
+        g = np.empty(lib().emb200_proposer_param_count(self._h), np.float32)
+        loss = ctypes.c_float()
+        self._check(lib().emb200_proposer_grad(self._h, _p(x), _p(t), t.size, _p(g), ctypes.byref(loss)))
+        return float(loss.value), g
+
+    def proposer_groups(self):
+        out = np.empty(self.k, np.uint32)
+        self._check(lib().emb200_proposer_groups(self._h, _p(out)))
+        return out
+
+    def propose(self, x):
+        """(groups[m][top] most likely first, confidence[m]) for host rows."""
+        x = np.ascontiguousarray(x, np.float32).reshape(-1, self.d)
+        g = np.empty((x.shape[0], self.proposer_top), np.uint32)
+        conf = np.empty(x.shape[0], np.float32)
+        self._check(lib().emb200_propose(self._h, _p(x), x.shape[0], _p(g), _p(conf)))
+        return g, conf
+
+    def assign_proposed(self, want_host=True):
+        """The proposer assign over the resident rows."""
+        n = self.rows_shape[0]
+        labels = np.empty(n, np.uint32) if want_host else None
+        dist = np.empty(n, np.float32) if want_host else None
+        self._check(lib().emb200_assign_proposed_resident(self._h, _p(labels), _p(dist)))
+        return labels, dist
+
+    def assign_proposed_device(self, x_ptr, m, labels_ptr, dist_ptr, stream=None):
+        self._check(lib().emb200_assign_proposed_device(self._h, ctypes.c_void_p(x_ptr), m,
+                                                        ctypes.c_void_p(labels_ptr), ctypes.c_void_p(dist_ptr),
+                                                        ctypes.c_void_p(stream or 0)))
 
     def train_resident(self, k, cfg: Optional[Config] = None) -> Output:
         """train (src/lib.rs:348-491) on the resident rows, entirely on the device."""

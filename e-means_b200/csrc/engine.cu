@@ -24,12 +24,17 @@
 #include "kernels_tc.cuh"
 #include "kernels_tc_i8.cuh"
 #include "kernels_update.cuh"
+#include "kernels_mlp.cuh"
+#include "kernels_proposer.cuh"
 
 constexpr int kRefineCap = 32;  // candidates kept per refined row
 
 using namespace emb;
 
 namespace {
+
+struct Proposer;
+void proposer_release(emb200_handle* h);
 
 // Device buffer owned by a handle.
 template <typename T>
@@ -126,6 +131,10 @@ struct emb200_handle {
 
     // training state
     TrainState train;
+
+    // learned proposer (emb200_proposer_*), and a counter of centroid changes it tracks
+    Proposer* prop = nullptr;
+    uint64_t centroid_version = 0;
 };
 
 namespace {
@@ -397,7 +406,8 @@ int tc_nsplit(const emb200_handle* h, size_t m) {
 template <typename T, bool COLLECT>
 int launch_tc(emb200_handle* h, const T* x, const uint32_t* gather, const uint32_t* gather2, size_t m, int nterms,
               const float* theta, uint32_t* cand, uint32_t* cand_count, int cap, int* err, cudaStream_t st,
-              const uint32_t* m_dev = nullptr, int nsplit_override = 0) {
+              const uint32_t* m_dev = nullptr, int nsplit_override = 0, const int* tile_group = nullptr,
+              const int* grp_cbeg = nullptr, const int* grp_ntiles = nullptr) {
     TcParams p{};
     p.m = (int)m;
     p.d = (int)h->d;
@@ -416,6 +426,9 @@ int launch_tc(emb200_handle* h, const T* x, const uint32_t* gather, const uint32
     p.cand_count = cand_count;
     p.cand_cap = cap;
     p.m_dev = m_dev;
+    p.tile_group = tile_group;  // grouped search: m is a whole number of bucket tiles
+    p.grp_cbeg = grp_cbeg;
+    p.grp_ntiles = grp_ntiles;
     TcSmem L = tc_smem_layout(p.kpad, p.nterms);
     // At least 120 KB so that two CTAs never share an SM: each holds all 512 TMEM columns.
     size_t smem = std::max<size_t>(L.total + 1024, 120 * 1024);
@@ -424,7 +437,7 @@ int launch_tc(emb200_handle* h, const T* x, const uint32_t* gather, const uint32
         CK(cudaFuncSetAttribute(k_assign_tc<T, COLLECT>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
         attr_set = true;
     }
-    int nsplit = nsplit_override > 0 ? nsplit_override : tc_nsplit(h, m);
+    int nsplit = tile_group ? 1 : nsplit_override > 0 ? nsplit_override : tc_nsplit(h, m);
     dim3 grid((unsigned)((m + kTcBM - 1) / kTcBM), (unsigned)nsplit);
     k_assign_tc<T, COLLECT><<<grid, kTcThreads, smem, st>>>(x, h->map_hi, h->map_lo, p);
     CKL();
@@ -453,6 +466,10 @@ int finish_counters(emb200_handle* h, cudaStream_t st, bool refined) {
 // Counters (device): [0] uncertified rows, [1] certified rows, [2] fast-kernel abort,
 // [3] exhaustive rows, [4] refine abort.
 template <typename T>
+int settle_rows(emb200_handle* h, const T* x, const uint32_t* gather, size_t m, uint32_t* labels, float* dist,
+                cudaStream_t st, bool graph, int nsplit, int fast_prec, bool tc);
+
+template <typename T>
 int assign_rows_dev(emb200_handle* h, const T* x, const uint32_t* gather, size_t m, uint32_t* labels, float* dist,
                     cudaStream_t st, bool graph = false) {
     const int dtype = std::is_same<T, float>::value ? EMB200_F32 : (std::is_same<T, int8_t>::value ? EMB200_I8 : EMB200_U8);
@@ -466,7 +483,6 @@ int assign_rows_dev(emb200_handle* h, const T* x, const uint32_t* gather, size_t
     const int row_tiles = (int)((m + kSimtBM - 1) / kSimtBM);
     const int ntiles = (k + kSimtBN - 1) / kSimtBN;
     const int fast_terms = tc_terms(prec, dtype);
-    const int refine_terms = tc_terms(EMB200_PREC_BF16, dtype);
     const bool tc = prec != EMB200_PREC_FP32 && tc_supported(h, fast_terms);
     int nsplit = 1;
     if (tc) {
@@ -494,8 +510,23 @@ int assign_rows_dev(emb200_handle* h, const T* x, const uint32_t* gather, size_t
         CKL();
     }
     if (!graph) CK(cudaEventRecord(h->evk1, st));
+    return settle_rows(h, x, gather, m, labels, dist, st, graph, nsplit, tc ? prec : EMB200_PREC_FP32, tc);
+}
+
+// Steps 2-4 of the pipeline for m rows whose fast-contraction top-2 partials are
+// in h->part_s / h->part_i (nsplit splits), with the device counters zeroed before
+// the fast kernel (which may have set the abort flag, counter 2).
+template <typename T>
+int settle_rows(emb200_handle* h, const T* x, const uint32_t* gather, size_t m, uint32_t* labels, float* dist,
+                cudaStream_t st, bool graph, int nsplit, int fast_prec, bool tc) {
+    const int dtype = std::is_same<T, float>::value ? EMB200_F32 : (std::is_same<T, int8_t>::value ? EMB200_I8 : EMB200_U8);
+    const int k = (int)h->k, d = (int)h->d;
+    const int refine_terms = tc_terms(EMB200_PREC_BF16, dtype);
+    if (h->redo_rows.ensure(m) || h->redo_theta.ensure(m) || h->counters.ensure(8))
+        return fail(h, EMB200_ENOMEM, "scratch allocation failed for %zu rows", m);
+    uint32_t* ctr = h->counters.p;
     float ka, kb, ka2, kb2;
-    bound_coefficients(tc ? prec : EMB200_PREC_FP32, dtype, h->d, tc, &ka, &kb);
+    bound_coefficients(fast_prec, dtype, h->d, tc, &ka, &kb);
     bound_coefficients(EMB200_PREC_BF16, dtype, h->d, false, &ka2, &kb2);
     const int match = h->opts.match_kernel;
     if (match == kMatchAvx512) {
@@ -690,6 +721,7 @@ int emb200_destroy(emb200_handle* h) {
     h->part_s.release(); h->part_i.release(); h->redo_rows.release(); h->counters.release();
     h->redo_theta.release(); h->cand.release(); h->cand_count.release(); h->redo2_rows.release();
     h->train.release();
+    proposer_release(h);
     if (h->ev0) cudaEventDestroy(h->ev0);
     if (h->ev1) cudaEventDestroy(h->ev1);
     if (h->evk0) cudaEventDestroy(h->evk0);
@@ -755,6 +787,7 @@ int emb200_set_centroids(emb200_handle* h, const float* centroids, size_t k, siz
     if (rc) return rc;
     CK(cudaStreamSynchronize(h->stream));
     h->have_centroids = true;
+    h->centroid_version++;
     return EMB200_OK;
 }
 
@@ -950,3 +983,4 @@ extern "C" int emb200_assign_f32_noalloc(const float* x_dev, size_t m, size_t d,
 }
 
 #include "engine_train.inc"
+#include "engine_proposer.inc"

@@ -57,6 +57,12 @@ struct TcParams {
     uint32_t* cand_count;     // COLLECT: [m] candidates found (may exceed cand_cap)
     int cand_cap;
     const uint32_t* m_dev;    // COLLECT: if set, the row count is min(m, *m_dev), read on the device
+    // Grouped search (centroid groups of a group-sorted matrix): row tile t scores
+    // only group tile_group[t] (-1: no work), columns [grp_cbeg[g], + 256 grp_ntiles[g]).
+    // Column starts are multiples of 32, so packed keys and the norms copy stay aligned.
+    const int* tile_group;
+    const int* grp_cbeg;
+    const int* grp_ntiles;
 };
 
 // ---- PTX wrappers -----------------------------------------------------------
@@ -336,6 +342,7 @@ EMB_DEV void tc_regs_ready(uint32_t (&v)[32]) {
 }
 
 // Grid: (ceil(m / 128), nsplit); CTA (bx, by) walks centroid tiles by, by + nsplit, ...
+// (grouped search: grid (bucket tiles, 1), CTA bx walks the tiles of group tile_group[bx]).
 // COLLECT = false: per-row top-2 of approximate scores to part_s/part_i.
 // COLLECT = true : every centroid with approximate score <= theta[row] is appended
 //                  to cand[row][*] (cand_count[row] counts all, capped storage).
@@ -367,7 +374,16 @@ k_assign_tc(const T* __restrict__ x, const __grid_constant__ CUtensorMap map_hi,
     }
     const int nsplit = gridDim.y;
     const int ntiles_all = (p.k + kTcBN - 1) / kTcBN;
-    const int my_tiles = (int)blockIdx.y < ntiles_all ? (ntiles_all - (int)blockIdx.y + nsplit - 1) / nsplit : 0;
+    int my_tiles = (int)blockIdx.y < ntiles_all ? (ntiles_all - (int)blockIdx.y + nsplit - 1) / nsplit : 0;
+    // Column of this CTA's tile t: col_first + t * col_step.
+    int col_first = (int)blockIdx.y * kTcBN, col_step = nsplit * kTcBN;
+    if (p.tile_group) {
+        const int g = p.tile_group[blockIdx.x];
+        if (g < 0) return;  // past the last bucket tile: the whole CTA leaves before any setup
+        my_tiles = p.grp_ntiles[g];
+        col_first = p.grp_cbeg[g];
+        col_step = kTcBN;
+    }
     const int natoms = p.kpad / 64;
 
     if (threadIdx.x == 0) {
@@ -401,15 +417,15 @@ k_assign_tc(const T* __restrict__ x, const __grid_constant__ CUtensorMap map_hi,
                 const int s = u % S;
                 const uint32_t ph = (uint32_t)(u / S) & 1u;
                 if (!mbar_wait(&empty[s], ph ^ 1u, abort_flag)) break;
-                const int tile = blockIdx.y + t * nsplit;
+                const int col = col_first + t * col_step;
                 uint8_t* stage = smem + L.b0 + s * L.stage_bytes;
                 mbar_expect_tx(&full[s], L.stage_bytes);
-                tma_load_2d(stage, &map_hi, &full[s], a * 64, tile * kTcBN);
-                if (p.nterms > 1) tma_load_2d(stage + L.term_bytes, &map_lo, &full[s], a * 64, tile * kTcBN);
+                tma_load_2d(stage, &map_hi, &full[s], a * 64, col);
+                if (p.nterms > 1) tma_load_2d(stage + L.term_bytes, &map_lo, &full[s], a * 64, col);
                 if (a == 0) {
                     const int ns = t % kTcNormSlots;
                     mbar_expect_tx(&norms_full[ns], kTcBN * 4);
-                    bulk_load(norms_s + ns * kTcBN, p.norms + (size_t)tile * kTcBN, kTcBN * 4, &norms_full[ns]);
+                    bulk_load(norms_s + ns * kTcBN, p.norms + (size_t)col, kTcBN * 4, &norms_full[ns]);
                 }
                 issued = u + 1;
             }
@@ -492,7 +508,7 @@ k_assign_tc(const T* __restrict__ x, const __grid_constant__ CUtensorMap map_hi,
             if (!mbar_wait(&acc_full[b], bph, abort_flag, 20000)) break;
             if (!mbar_wait(&norms_full[t % kTcNormSlots], (uint32_t)(t / kTcNormSlots) & 1u, abort_flag)) break;
             tc_fence_after();
-            const int cq0 = (blockIdx.y + t * nsplit) * kTcBN + cq * 64;
+            const int cq0 = col_first + t * col_step + cq * 64;
             const float* nrm = norms_s + (t % kTcNormSlots) * kTcBN + cq * 64;
             const uint32_t taddr = tmem_base + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * kTcBN + cq * 64);
 #pragma unroll

@@ -103,6 +103,9 @@ typedef struct {
     uint64_t rows_refined;    /* uncertified rows sent through the candidate-collecting refine pass */
     double fast_ms;           /* device time of the fast contraction kernel(s) (CUDA events, summed) */
     uint64_t fast_launches;   /* launches of the fast contraction kernel */
+    uint64_t rows_proposed;   /* proposer assign: rows searched in their proposed groups only */
+    uint64_t rows_lowconf;    /* proposer assign: rows below the confidence threshold (full search) */
+    double propose_ms;        /* proposer assign: device time of the proposals (network or group centroids) */
 } emb200_stats;
 
 /* ---- lifecycle ---------------------------------------------------------- */
@@ -160,7 +163,7 @@ double emb200_scheduled_alpha(double alpha0, size_t step, size_t total);
 int emb200_train(emb200_handle* h, const emb200_config* cfg, size_t k, float* centroids, uint32_t* labels,
                  double* objective, uint64_t* n_splits, emb200_recipe* recipe);
 
-/* ---- batched instances (PQ sub-codebooks, IVF lists) ----
+/* ---- batched instances (PQ sub-codebooks, per-list IVF refinements) ----------
  *
  * train() (src/lib.rs:348-491) run for `count` independent instances at once,
  * each over rows [row0, row0 + n) of the resident rows (same d and dtype, same
@@ -177,6 +180,67 @@ typedef struct {
 int emb200_train_batched(emb200_handle* h, const emb200_config* cfg, const emb200_instance* inst, size_t count,
                          size_t max_concurrency, float* centroids, uint32_t* labels, double* objective,
                          uint64_t* n_splits);
+
+/* ---- learned proposer (no counterpart in the reference's code) -----------
+ *
+ * For large k: the centroids are partitioned into G groups by e-means on the
+ * centroids themselves (this engine's own train(), k = G), and a small BF16
+ * network d -> H -> H -> G (ReLU, FP32 accumulation, trained on the GPU with
+ * this library's forward and backward kernels and Adam) predicts from a row the
+ * group of its nearest centroid. The proposer assign scores each row exactly
+ * against the centroids of its `top` most likely groups only (tcgen05, over a
+ * group-sorted copy of the centroids), re-scores the two best in the
+ * reference's f32 rounding, and certifies the label against the error bound of
+ * the fast contraction. Rows whose top-`top` softmax mass is below `confidence`,
+ * or whose margin among the candidates the bound cannot certify, take the full
+ * exact search instead. Labels are therefore the exact argmin over the
+ * proposed groups, and equal the full search's wherever the nearest centroid
+ * lies in them (recall@1 is measured, not guaranteed).
+ *
+ * mode EMB200_PROPOSER_CENTROIDS replaces the network by the nearest `top`
+ * group centroids (the method without a learned part). */
+#define EMB200_PROPOSER_MLP 0
+#define EMB200_PROPOSER_CENTROIDS 1
+typedef struct {
+    uint32_t groups;      /* G <= 512; 0 = 256 */
+    uint32_t hidden;      /* H, a multiple of 8; 0 = 512 */
+    uint32_t top;         /* groups searched per row, <= 32 and <= G; 0 = 8 */
+    uint32_t mode;        /* EMB200_PROPOSER_* */
+    float confidence;     /* MLP mode: rows below this top-`top` softmax mass take the full search */
+    uint32_t batch;       /* training mini-batch rows; 0 = 4096 */
+    float lr;             /* Adam learning rate (decays linearly to lr/10 over a train call); 0 = 2e-3 */
+    float group_epochs;   /* e-means epochs of the grouping; 0 = 5 */
+    uint64_t seed;        /* grouping and initialisation seed */
+    uint32_t reserved[4];
+} emb200_proposer_config;
+
+/* Groups the current centroids, builds the group-sorted copy and initialises the
+ * network (input standardisation from the resident rows when present). */
+int emb200_proposer_init(emb200_handle* h, const emb200_proposer_config* cfg);
+/* Adam steps on mini-batches of resident rows with known labels (host array of
+ * rows_n labels, e.g. train()'s output; UINT32_MAX rows are skipped): targets
+ * are the labels' groups. losses: optional host array of `steps` mean losses. */
+int emb200_proposer_train(emb200_handle* h, const uint32_t* labels, size_t n, uint32_t steps, float* losses);
+/* Mode, groups per row and confidence threshold for later assigns. */
+int emb200_proposer_set(emb200_handle* h, uint32_t mode, uint32_t top, float confidence);
+/* Network parameters as one f32 array: input mean[d], input 1/std[d], W1[H][d],
+ * b1[H], W2[H][H], b2[H], W3[G][H], b3[G], each block starting at a multiple of 8. */
+size_t emb200_proposer_param_count(const emb200_handle* h);
+int emb200_proposer_get_params(emb200_handle* h, float* params, size_t count);
+int emb200_proposer_set_params(emb200_handle* h, const float* params, size_t count);
+/* Mean cross-entropy loss of m host rows against target groups, and its gradient
+ * in the parameter layout (input statistics entries zero). */
+int emb200_proposer_grad(emb200_handle* h, const float* x, const uint32_t* targets, size_t m, float* grads,
+                         float* loss);
+/* Group of every centroid (k entries). */
+int emb200_proposer_groups(emb200_handle* h, uint32_t* group_of);
+/* Proposals for m host rows: groups[m][top] (most likely first) and confidence[m]. */
+int emb200_propose(emb200_handle* h, const float* x, size_t m, uint32_t* groups, float* confidence);
+/* The proposer assign over the resident f32 rows (labels/dist host arrays of n,
+ * or NULL to keep them on the device), or over m device rows on `stream`. */
+int emb200_assign_proposed_resident(emb200_handle* h, uint32_t* labels, float* dist);
+int emb200_assign_proposed_device(emb200_handle* h, const float* x_dev, size_t m, uint32_t* labels_dev,
+                                  float* dist_dev, void* stream);
 
 /* ---- search without allocation (no counterpart in the reference) --------
  *

@@ -1,0 +1,191 @@
+"""The learned proposer: its network's gradients against the FP64 oracle
+(oracle/mlp_oracle.py, itself pinned by finite differences here on the CPU),
+the proposer assign's guarantees against the full exact search, and what the
+trained network gains over the nearest-group-centroid proposer.
+"""
+import numpy as np
+import pytest
+
+from oracle import mlp_oracle as mo
+
+
+# ---- CPU: the oracle itself -------------------------------------------------
+
+def _random_params(rng, d, H, G, scale=0.5):
+    L = mo.layout(d, H, G)
+    p = np.zeros(L["total"], np.float32)
+    for name in ("w1", "b1", "w2", "b2", "w3", "b3"):
+        o, n = L[name]
+        p[o:o + n] = rng.standard_normal(n).astype(np.float32) * np.float32(scale)
+    o, n = L["mean"]
+    p[o:o + n] = rng.standard_normal(n).astype(np.float32) * np.float32(0.1)
+    o, n = L["istd"]
+    p[o:o + n] = (1.0 + rng.random(n)).astype(np.float32)
+    return p
+
+
+def test_oracle_gradient_matches_finite_differences():
+    rng = np.random.default_rng(0)
+    d, H, G, m = 6, 8, 5, 7
+    params = _random_params(rng, d, H, G)
+    p, _ = mo.unpack(params, d, H, G, weights_bf16=False)
+    x0 = rng.standard_normal((m, d))
+    t = rng.integers(0, G, m)
+    loss, g = mo.loss_and_grad(x0, t, p)
+    assert np.isclose(loss, mo.loss_only(x0, t, p))
+    eps = 1e-6
+    for name in ("w1", "b1", "w2", "b2", "w3", "b3"):
+        num = np.zeros_like(p[name])
+        for idx in np.ndindex(p[name].shape):
+            q = {k: v.copy() for k, v in p.items()}
+            q[name][idx] += eps
+            lp = mo.loss_only(x0, t, q)
+            q[name][idx] -= 2 * eps
+            lm = mo.loss_only(x0, t, q)
+            num[idx] = (lp - lm) / (2 * eps)
+        np.testing.assert_allclose(g[name], num, rtol=1e-5, atol=1e-8, err_msg=name)
+
+
+def test_bf16_rounding_ties_to_even():
+    v = np.array([1.0, 1.0 + 2.0 ** -8, 1.0 + 3 * 2.0 ** -8, 1.0 + 2.0 ** -9, -2.5, 3.0e38], np.float32)
+    r = mo.bf16(v)
+    assert r[0] == 1.0 and r[1] == 1.0 and r[2] == 1.0 + 2.0 ** -6 and r[3] == 1.0 and r[4] == -2.5
+    assert np.isfinite(r[5])
+
+
+def test_layout_blocks_aligned():
+    L = mo.layout(96, 512, 256)
+    assert all(L[n][0] % 8 == 0 for n in ("mean", "istd", "w1", "b1", "w2", "b2", "w3", "b3"))
+    assert L["total"] == L["b3"][0] + 256
+
+
+# ---- GPU ----------------------------------------------------------------------
+
+D, K, G, TOP, HID = 48, 2048, 64, 4, 256
+
+
+@pytest.fixture(scope="module")
+def trained(emb):
+    """Heavy-tailed rows, k = 2048 centroids from this engine's training, a
+    proposer (64 groups, top 4) trained on the training run's labels."""
+    x = emb.datasets.heavy_tailed(120_000, D, latent=16, components=512, seed=21)
+    xt = emb.datasets.heavy_tailed(20_000, D, latent=16, components=512, seed=21 + 1)
+    a = emb.B200Assigner(0, precision="bf16x1")
+    out = emb.train(x, D, K, emb.Config(nepochs=3.0), assigner=a)
+    a.proposer_init(groups=G, hidden=HID, top=TOP, seed=5)
+    losses = a.proposer_train(out.labels, 600)
+    yield a, x, xt, out, losses
+    a.close()
+
+
+@pytest.mark.gpu
+def test_gradients_match_fp64_oracle(emb):
+    rng = np.random.default_rng(3)
+    d, H, Gs, m = 40, 64, 24, 777
+    c = rng.standard_normal((200, d)).astype(np.float32)
+    a = emb.B200Assigner(0, precision="bf16x1")
+    a.set_centroids(c)
+    a.proposer_init(groups=Gs, hidden=H, top=4, seed=1)
+    params = a.proposer_params()
+    L = mo.layout(d, H, Gs)
+    assert params.size == L["total"]
+    params = _random_params(rng, d, H, Gs, scale=0.3)
+    a.set_proposer_params(params)
+    assert np.array_equal(a.proposer_params(), params)
+    x = (rng.standard_normal((m, d)) * 2 + 0.3).astype(np.float32)
+    t = rng.integers(0, Gs, m).astype(np.uint32)
+    loss, g = a.proposer_grad(x, t)
+    a.close()
+    p, _ = mo.unpack(params, d, H, Gs)
+    x0 = mo.network_input(x, p["mean"], p["istd"])
+    ref_loss, ref = mo.loss_and_grad(x0, t, p)
+    # BF16 activations and activation gradients on the GPU, FP64 throughout in the
+    # oracle: per-tensor relative L2 error within 2%, and the loss within 0.5%.
+    assert abs(loss - ref_loss) <= 5e-3 * abs(ref_loss)
+    for name in ("w1", "b1", "w2", "b2", "w3", "b3"):
+        o, n = L[name]
+        gg = g[o:o + n].astype(np.float64)
+        rr = ref[name].reshape(-1)
+        err = np.linalg.norm(gg - rr) / np.linalg.norm(rr)
+        assert err < 2e-2, (name, err)
+    for name in ("mean", "istd"):
+        o, n = L[name]
+        assert not g[o:o + n].any()
+
+
+@pytest.mark.gpu
+def test_training_reduces_loss(trained):
+    _, _, _, _, losses = trained
+    first, last = losses[:50].mean(), losses[-50:].mean()
+    assert np.all(np.isfinite(losses))
+    assert last < 0.5 * first, (first, last)
+
+
+def _recall(groups_of_label, proposals):
+    return float(np.mean([g in row for g, row in zip(groups_of_label, proposals)]))
+
+
+@pytest.mark.gpu
+def test_learned_proposer_beats_group_centroids(trained):
+    a, _, xt, _, _ = trained
+    lab_full, _ = a.assign(xt)
+    gof = a.proposer_groups()
+    target = gof[lab_full]
+    a.proposer_set("mlp", TOP, 0.0)
+    g_mlp, conf = a.propose(xt)
+    a.proposer_set("centroids", TOP, 0.0)
+    g_cen, _ = a.propose(xt)
+    a.proposer_set("mlp", TOP, 0.0)
+    r_mlp, r_cen = _recall(target, g_mlp), _recall(target, g_cen)
+    assert np.all((conf > 0) & (conf <= 1.0 + 1e-6))
+    # Held-out rows: the group of the exact label is among the network's top 4 more
+    # often than among the 4 nearest group centroids.
+    assert r_mlp > r_cen, (r_mlp, r_cen)
+    assert r_mlp > 0.97, r_mlp
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("mode", ["mlp", "centroids"])
+def test_proposer_assign_guarantees(trained, orc, mode):
+    a, x, _, out, _ = trained
+    a.proposer_set(mode, TOP, 0.0)
+    lab_p, dist_p = a.assign_proposed()
+    st = a.stats()
+    lab_f, dist_f = a.assign_resident()
+    n = x.shape[0]
+    assert st["rows_proposed"] + st["rows_lowconf"] == n
+    assert st["fast_aborted"] == 0
+    props, _ = a.propose(x)
+    gof = a.proposer_groups()
+    covered = np.array([gof[l] in row for l, row in zip(lab_f, props)])
+    same = lab_p == lab_f
+    # 1. wherever the exact label's group was proposed, the label is the exact one
+    assert np.all(same[covered])
+    # 2. every distance is the exact distance of the returned label (reference rounding)
+    assert np.array_equal(dist_p[same].view(np.uint32), dist_f[same].view(np.uint32))
+    for i in np.nonzero(~same)[0][:300]:
+        j = int(lab_p[i])
+        _, de = orc.cpu_assign(x[i:i + 1], out.centroids[j:j + 1], emulate=True)
+        assert de[0].view(np.uint32) == dist_p[i].view(np.uint32)
+    # 3. elsewhere the returned label is never nearer than the exact one
+    assert np.all(dist_p >= dist_f)
+    recall = same.mean()
+    assert recall > 0.97, recall
+    a.proposer_set("mlp", TOP, 0.0)
+
+
+@pytest.mark.gpu
+def test_low_confidence_rows_take_the_full_search(trained):
+    a, x, _, _, _ = trained
+    a.proposer_set("mlp", TOP, 1.01)  # no row reaches it
+    lab_p, dist_p = a.assign_proposed()
+    st = a.stats()
+    lab_f, dist_f = a.assign_resident()
+    assert st["rows_lowconf"] == x.shape[0] and st["rows_proposed"] == 0
+    assert np.array_equal(lab_p, lab_f) and np.array_equal(dist_p.view(np.uint32), dist_f.view(np.uint32))
+    a.proposer_set("mlp", TOP, 0.9)
+    lab_p, dist_p = a.assign_proposed()
+    st = a.stats()
+    assert 0 < st["rows_lowconf"] < x.shape[0]
+    assert np.all(dist_p >= dist_f)
+    a.proposer_set("mlp", TOP, 0.0)
