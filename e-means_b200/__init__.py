@@ -113,6 +113,7 @@ def lib():
     L.emb200_proposer_set_params.argtypes = [P, P, S]
     L.emb200_proposer_grad.argtypes = [P, P, P, S, P, P]
     L.emb200_proposer_groups.argtypes = [P, P]
+    L.emb200_proposer_logits.argtypes = [P, P, S, P, I]
     L.emb200_propose.argtypes = [P, P, S, P, P]
     L.emb200_assign_proposed_resident.argtypes = [P, P, P]
     L.emb200_assign_proposed_device.argtypes = [P, P, S, P, P, P]
@@ -340,6 +341,7 @@ class B200Assigner:
         c = _ProposerConfig(groups, hidden, top, PROPOSER_MODES[mode], confidence, batch, lr, group_epochs, seed)
         self._check(lib().emb200_proposer_init(self._h, ctypes.byref(c)))
         self.proposer_top = top
+        self._proposer_groups_n = groups
 
     def proposer_train(self, labels, steps):
         """Adam steps on mini-batches of resident rows labelled by `labels` (one
@@ -371,6 +373,15 @@ class B200Assigner:
         loss = ctypes.c_float()
         self._check(lib().emb200_proposer_grad(self._h, _p(x), _p(t), t.size, _p(g), ctypes.byref(loss)))
         return float(loss.value), g
+
+    def proposer_logits(self, x, fused=True):
+        """Network logits [m][groups] of host rows, by the fused tcgen05 forward
+        pass or by the GEMM forward pass of training."""
+        x = np.ascontiguousarray(x, np.float32).reshape(-1, self.d)
+        g = self._proposer_groups_n
+        out = np.empty((x.shape[0], g), np.float32)
+        self._check(lib().emb200_proposer_logits(self._h, _p(x), x.shape[0], _p(out), int(fused)))
+        return out
 
     def proposer_groups(self):
         out = np.empty(self.k, np.uint32)

@@ -25,6 +25,7 @@
 #include "kernels_tc_i8.cuh"
 #include "kernels_update.cuh"
 #include "kernels_mlp.cuh"
+#include "kernels_mlp_tc.cuh"
 #include "kernels_proposer.cuh"
 
 constexpr int kRefineCap = 32;  // candidates kept per refined row

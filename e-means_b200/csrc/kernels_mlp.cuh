@@ -275,6 +275,7 @@ __global__ void k_topm_groups(const float* __restrict__ logits, int m, int G, in
                 bi = oi;
             }
         }
+        if (bi >= G) bi = 0;  // no finite logit left (a diverged network): any valid group
         if (lane == 0) groups[(size_t)row * top + s] = (uint16_t)bi;
         mass += __expf(bv - mx);
         if ((bi & 31) == lane) {

@@ -232,6 +232,10 @@ int emb200_proposer_set_params(emb200_handle* h, const float* params, size_t cou
  * in the parameter layout (input statistics entries zero). */
 int emb200_proposer_grad(emb200_handle* h, const float* x, const uint32_t* targets, size_t m, float* grads,
                          float* loss);
+/* Network logits of m host rows (m <= 65536), [m][G]: fused = 1 from the fused
+ * tcgen05 forward pass (H of 256 or 512, G of 128 or 256, d a multiple of 8),
+ * fused = 0 from the GEMM forward pass used in training. */
+int emb200_proposer_logits(emb200_handle* h, const float* x, size_t m, float* logits, int fused);
 /* Group of every centroid (k entries). */
 int emb200_proposer_groups(emb200_handle* h, uint32_t* group_of);
 /* Proposals for m host rows: groups[m][top] (most likely first) and confidence[m]. */
