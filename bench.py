@@ -458,8 +458,8 @@ def run_c5(args):
     from oracle import oracle as orc
 
     emb = load_package()
-    n = args.rows if args.rows != N_ROWS else 10_000_000
-    d, k, groups, top = 96, 65536, 256, 8
+    n = args.c5_rows
+    d, k, groups, top_c = 96, 65536, 256, 8
     t0 = time.perf_counter()
     x = emb.datasets.heavy_tailed(n, d, latent=32, components=8192, nu=3.0, seed=0)
     t_data = time.perf_counter() - t0
@@ -469,7 +469,7 @@ def run_c5(args):
     out = a.train_resident(k, emb.Config(nepochs=5.0))
     t_train = time.perf_counter() - t0
     t0 = time.perf_counter()
-    a.proposer_init(groups=groups, hidden=512, top=top, seed=7)
+    a.proposer_init(groups=groups, hidden=512, top=8, seed=7)
     t_group = time.perf_counter() - t0
     t0 = time.perf_counter()
     losses = a.proposer_train(out.labels, args.proposer_steps)
@@ -485,7 +485,9 @@ def run_c5(args):
             ms.append(st["ms_total"])
         return float(np.mean(ms)), st
 
+    configs = [tuple(float(v) for v in c.split(":")) for c in args.proposer_configs.split(",")]
     sampler = ClockSampler(0)
+    runs = []
     with sampler:
         a.set_options(precision="bf16")
         a.set_centroids(out.centroids)
@@ -493,14 +495,14 @@ def run_c5(args):
         a.set_options(precision="bf16x1")
         a.set_centroids(out.centroids)
         t_full, st_full = timed(lambda: a.assign_resident(want_host=False))
-        a.proposer_set("mlp", top, args.confidence)
-        t_mlp, st_mlp = timed(lambda: a.assign_proposed(want_host=False))
-        a.proposer_set("centroids", top, 0.0)
+        for (top, conf, mass) in configs:
+            a.proposer_set("mlp", int(top), conf, mass)
+            t, st = timed(lambda: a.assign_proposed(want_host=False))
+            lab, dist = a.assign_proposed()
+            runs.append(((int(top), conf, mass), t, st, lab, dist))
+        a.proposer_set("centroids", top_c, 0.0)
         t_cen, st_cen = timed(lambda: a.assign_proposed(want_host=False))
     lab_f, dist_f = a.assign_resident()
-    a.proposer_set("mlp", top, args.confidence)
-    lab_m, dist_m = a.assign_proposed()
-    a.proposer_set("centroids", top, 0.0)
     lab_c, dist_c = a.assign_proposed()
     mse_f = float(dist_f.astype(np.float64).mean())
     # FP64 brute force on a sample of rows: agreement of each path's labels
@@ -527,15 +529,19 @@ def run_c5(args):
                 "rows_lowconf": st["rows_lowconf"], "rows_refined": st["rows_refined"],
                 "rows_researched": st["rows_researched"], "kernel_launches": st["kernel_launches"]}
 
+    (top, conf, mass), t_mlp, st_mlp, lab_m, dist_m = runs[0]
     line = {"metric": "rows/s assigned (10M x 96 heavy-tailed, k=65536): learned proposer vs full search",
             "value": n / (t_mlp / 1e3), "unit": "rows/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": t_mlp, "higher_is_better": True, "dtype": "bf16 -> f32 accumulate",
             "config": {"workload": f"{n} x {d} heavy-tailed rows (Student-t nu=3, 8192 components), k={k}, "
-                                   f"{groups} groups, top {top}, network 96-512-512-256",
-                       "confidence": args.confidence, "proposer_steps": args.proposer_steps,
+                                   f"{groups} groups, network 96-512-512-256",
+                       "top": top, "confidence": conf, "mass": mass, "proposer_steps": args.proposer_steps,
                        "l2": "no flush: the resident rows (3.8 GB) exceed the 126 MB L2"},
             "learned": entry(t_mlp, st_mlp, lab_m, dist_m),
-            "group_centroids": entry(t_cen, st_cen, lab_c, dist_c),
+            "learned_settings": [dict(entry(t, st, lab, dist), top=c[0], confidence=c[1], mass=c[2],
+                                      groups_per_row=st["groups_searched"] / max(st["rows_proposed"], 1))
+                                 for (c, t, st, lab, dist) in runs],
+            "group_centroids": dict(entry(t_cen, st_cen, lab_c, dist_c), top=top_c),
             "full_search_bf16x1": {"rows_per_s": n / (t_full / 1e3), "ms_per_step": t_full,
                                    "agreement_fp64_sample": float(np.mean(lab_f[sample] == bl)),
                                    "fast_kernel_ms": st_full["fast_ms"], "rows_refined": st_full["rows_refined"]},
@@ -609,8 +615,10 @@ def main():
                     help="trained by the engine (default) or a fixed sample of rows (profiling captures)")
     ap.add_argument("--workload", default="c2", choices=["c2", "c1", "c3", "c4a", "c4b", "c5"],
                     help="c2: the headline assign benchmark; the others: the remaining configurations")
-    ap.add_argument("--proposer-steps", type=int, default=2000, help="c5: Adam steps of the network")
-    ap.add_argument("--confidence", type=float, default=0.0, help="c5: confidence threshold of the proposer")
+    ap.add_argument("--proposer-steps", type=int, default=8000, help="c5: Adam steps of the network")
+    ap.add_argument("--proposer-configs", default="16:0:0.99,8:0:0,16:0:0.995,16:0:0.999,16:0.9:0.995",
+                    help="c5: top:confidence:mass settings of the proposer assign; the first is the headline")
+    ap.add_argument("--c5-rows", type=int, default=10_000_000, help="c5: rows of the workload")
     args = ap.parse_args()
     set_rows(args.rows)
     if args.workload == "c1" and args.impl == "ours":

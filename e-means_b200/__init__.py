@@ -54,14 +54,15 @@ class _Stats(ctypes.Structure):
                 ("kernel_launches", ctypes.c_uint64), ("ms_total", ctypes.c_double), ("fast_kernel", ctypes.c_int32),
                 ("fast_aborted", ctypes.c_int32), ("rows_refined", ctypes.c_uint64), ("fast_ms", ctypes.c_double),
                 ("fast_launches", ctypes.c_uint64), ("rows_proposed", ctypes.c_uint64),
-                ("rows_lowconf", ctypes.c_uint64), ("propose_ms", ctypes.c_double)]
+                ("rows_lowconf", ctypes.c_uint64), ("propose_ms", ctypes.c_double),
+                ("groups_searched", ctypes.c_uint64)]
 
 
 class _ProposerConfig(ctypes.Structure):
     _fields_ = [("groups", ctypes.c_uint32), ("hidden", ctypes.c_uint32), ("top", ctypes.c_uint32),
                 ("mode", ctypes.c_uint32), ("confidence", ctypes.c_float), ("batch", ctypes.c_uint32),
                 ("lr", ctypes.c_float), ("group_epochs", ctypes.c_float), ("seed", ctypes.c_uint64),
-                ("reserved", ctypes.c_uint32 * 4)]
+                ("mass", ctypes.c_float), ("reserved", ctypes.c_uint32 * 3)]
 
 
 PROPOSER_MODES = {"mlp": 0, "centroids": 1}
@@ -106,7 +107,7 @@ def lib():
     L.emb200_train_batched.argtypes = [P, ctypes.POINTER(_Config), P, S, S, P, P, P, P]
     L.emb200_proposer_init.argtypes = [P, ctypes.POINTER(_ProposerConfig)]
     L.emb200_proposer_train.argtypes = [P, P, S, ctypes.c_uint32, P]
-    L.emb200_proposer_set.argtypes = [P, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_float]
+    L.emb200_proposer_set.argtypes = [P, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_float, ctypes.c_float]
     L.emb200_proposer_param_count.restype = S
     L.emb200_proposer_param_count.argtypes = [P]
     L.emb200_proposer_get_params.argtypes = [P, P, S]
@@ -114,7 +115,7 @@ def lib():
     L.emb200_proposer_grad.argtypes = [P, P, P, S, P, P]
     L.emb200_proposer_groups.argtypes = [P, P]
     L.emb200_proposer_logits.argtypes = [P, P, S, P, I]
-    L.emb200_propose.argtypes = [P, P, S, P, P]
+    L.emb200_propose.argtypes = [P, P, S, P, P, P]
     L.emb200_assign_proposed_resident.argtypes = [P, P, P]
     L.emb200_assign_proposed_device.argtypes = [P, P, S, P, P, P]
     _lib = L
@@ -334,11 +335,12 @@ class B200Assigner:
 
     # ---- learned proposer ------------------------------------------------
     def proposer_init(self, groups=256, hidden=512, top=8, mode="mlp", confidence=0.0, batch=4096, lr=2e-3,
-                      group_epochs=5.0, seed=1234):
+                      group_epochs=5.0, seed=1234, mass=0.0):
         """Group the current centroids (e-means with k = groups on the centroids),
         build the group-sorted copy and initialise the network d -> hidden ->
         hidden -> groups (input statistics from the resident rows)."""
-        c = _ProposerConfig(groups, hidden, top, PROPOSER_MODES[mode], confidence, batch, lr, group_epochs, seed)
+        c = _ProposerConfig(groups, hidden, top, PROPOSER_MODES[mode], confidence, batch, lr, group_epochs, seed,
+                            mass)
         self._check(lib().emb200_proposer_init(self._h, ctypes.byref(c)))
         self.proposer_top = top
         self._proposer_groups_n = groups
@@ -351,8 +353,11 @@ class B200Assigner:
         self._check(lib().emb200_proposer_train(self._h, _p(lab), lab.size, steps, _p(losses)))
         return losses
 
-    def proposer_set(self, mode="mlp", top=8, confidence=0.0):
-        self._check(lib().emb200_proposer_set(self._h, PROPOSER_MODES[mode], top, confidence))
+    def proposer_set(self, mode="mlp", top=8, confidence=0.0, mass=0.0):
+        """mode; at most `top` groups per row; rows whose top-`top` softmax mass is
+        below `confidence` take the full search; each row searches the fewest
+        groups whose mass reaches `mass` (0: all `top`)."""
+        self._check(lib().emb200_proposer_set(self._h, PROPOSER_MODES[mode], top, confidence, mass))
         self.proposer_top = top
 
     def proposer_params(self):
@@ -388,13 +393,15 @@ class B200Assigner:
         self._check(lib().emb200_proposer_groups(self._h, _p(out)))
         return out
 
-    def propose(self, x):
-        """(groups[m][top] most likely first, confidence[m]) for host rows."""
+    def propose(self, x, with_counts=False):
+        """(groups[m][top] most likely first, confidence[m][, counts[m] searched])
+        for host rows."""
         x = np.ascontiguousarray(x, np.float32).reshape(-1, self.d)
         g = np.empty((x.shape[0], self.proposer_top), np.uint32)
         conf = np.empty(x.shape[0], np.float32)
-        self._check(lib().emb200_propose(self._h, _p(x), x.shape[0], _p(g), _p(conf)))
-        return g, conf
+        cnt = np.empty(x.shape[0], np.uint32)
+        self._check(lib().emb200_propose(self._h, _p(x), x.shape[0], _p(g), _p(conf), _p(cnt)))
+        return (g, conf, cnt) if with_counts else (g, conf)
 
     def assign_proposed(self, want_host=True):
         """The proposer assign over the resident rows."""

@@ -129,6 +129,7 @@ struct emb200_handle {
     DevBuf<float> redo_theta;
     DevBuf<uint32_t> cand, cand_count, redo2_rows;  // refine pass
     DevBuf<uint32_t> counters;  // see assign_rows_dev
+    DevBuf<unsigned long long> rkeys;  // exhaustive search: per listed row (score, index) keys
 
     // training state
     TrainState train;
@@ -514,6 +515,26 @@ int assign_rows_dev(emb200_handle* h, const T* x, const uint32_t* gather, size_t
     return settle_rows(h, x, gather, m, labels, dist, st, graph, nsplit, tc ? prec : EMB200_PREC_FP32, tc);
 }
 
+// Exhaustive exact search of the rows listed in rows[0 .. *count) (count on the
+// device, at most m): each row's centroids are split over several CTAs.
+template <typename T>
+int launch_research(emb200_handle* h, const T* x, const uint32_t* gather, size_t m, const uint32_t* rows,
+                    const uint32_t* count, uint32_t* labels, float* dist, cudaStream_t st) {
+    const int k = (int)h->k;
+    const int slices = std::max(1, std::min(64, (k + 2047) / 2048));
+    const int span = (k + slices - 1) / slices;
+    if (h->rkeys.ensure(m)) return fail(h, EMB200_ENOMEM, "scratch allocation failed for %zu rows", m);
+    k_research_keys_init<<<(unsigned)((m + 255) / 256), 256, 0, st>>>(h->rkeys.p, m);
+    CKL();
+    k_research_split<T><<<h->sm_count * 4, 256, 0, st>>>(x, gather, (int)h->d, h->c.p, h->norms.p, k,
+                                                          h->opts.match_kernel, rows, count, slices, span, h->rkeys.p);
+    CKL();
+    k_research_finish<T><<<(unsigned)((m * 32 + 255) / 256), 256, 0, st>>>(x, gather, (int)h->d, rows, count,
+                                                                           h->rkeys.p, labels, dist);
+    CKL();
+    return EMB200_OK;
+}
+
 // Steps 2-4 of the pipeline for m rows whose fast-contraction top-2 partials are
 // in h->part_s / h->part_i (nsplit splits), with the device counters zeroed before
 // the fast kernel (which may have set the abort flag, counter 2).
@@ -563,10 +584,7 @@ int settle_rows(emb200_handle* h, const T* x, const uint32_t* gather, size_t m, 
             exhaustive = h->redo2_rows.p;
             exhaustive_count = ctr + 3;
         }
-        k_research_cta<T><<<h->sm_count * 2, 256, 0, st>>>(x, gather, d, h->c.p, h->norms.p, k, match, exhaustive,
-                                                            exhaustive_count, labels, dist);
-        CKL();
-        return EMB200_OK;
+        return launch_research(h, x, gather, m, exhaustive, exhaustive_count, labels, dist, st);
     }
     uint32_t nredo = 0;
     CK(cudaMemcpyAsync(&nredo, ctr, sizeof nredo, cudaMemcpyDeviceToHost, st));
@@ -595,9 +613,8 @@ int settle_rows(emb200_handle* h, const T* x, const uint32_t* gather, size_t m, 
         exhaustive = h->redo2_rows.p;
         exhaustive_count = ctr + 3;
     }
-    k_research_cta<T><<<h->sm_count * 2, 256, 0, st>>>(x, gather, d, h->c.p, h->norms.p, k, match, exhaustive,
-                                                        exhaustive_count, labels, dist);
-    CKL();
+    const int rc = launch_research(h, x, gather, m, exhaustive, exhaustive_count, labels, dist, st);
+    if (rc) return rc;
     return finish_counters(h, st, exhaustive_count == ctr + 3);
 }
 
@@ -721,6 +738,7 @@ int emb200_destroy(emb200_handle* h) {
     h->stage.release(); h->st_labels.release(); h->st_dist.release();
     h->part_s.release(); h->part_i.release(); h->redo_rows.release(); h->counters.release();
     h->redo_theta.release(); h->cand.release(); h->cand_count.release(); h->redo2_rows.release();
+    h->rkeys.release();
     h->train.release();
     proposer_release(h);
     if (h->ev0) cudaEventDestroy(h->ev0);

@@ -434,6 +434,93 @@ __global__ void __launch_bounds__(256) k_research_cta(const T* __restrict__ x, c
     }
 }
 
+// Exhaustive exact search spread over many CTAs per row: CTA p takes row
+// p / slices and the centroids [span (p % slices), span (p % slices + 1)), scores
+// them as k_research_cta does, and folds its best into keys[r] with a 64-bit
+// atomicMin on (order-preserving score bits, index), so the lowest index wins
+// exact ties as in the reference's strict-< scan. keys start at (+inf, 0): a
+// row whose scores never beat +inf keeps label 0, the reference's result.
+EMB_DEV unsigned long long research_key(float s, uint32_t j) {
+    const uint32_t b = __float_as_uint(__fadd_rn(s, 0.0f));  // -0 -> +0: the two compare equal
+    const uint32_t o = (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+    return ((unsigned long long)o << 32) | j;
+}
+EMB_DEV float research_key_score(unsigned long long key) {
+    const uint32_t o = (uint32_t)(key >> 32);
+    return __uint_as_float((o & 0x80000000u) ? (o & 0x7fffffffu) : ~o);
+}
+
+__global__ void k_research_keys_init(unsigned long long* __restrict__ keys, size_t n) {
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) keys[i] = ((unsigned long long)0xff800000u << 32);  // (+inf, label 0)
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_research_split(const T* __restrict__ x, const uint32_t* __restrict__ gather,
+                                                        int d, const float* __restrict__ c,
+                                                        const float* __restrict__ norms, int k, int match,
+                                                        const uint32_t* __restrict__ rows,
+                                                        const uint32_t* __restrict__ count, int slices, int span,
+                                                        unsigned long long* __restrict__ keys) {
+    __shared__ unsigned long long sk[32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int gsz = match == kMatchAvx512 ? 16 : 8;
+    const int gpw = 32 / gsz;
+    const int G = 8 * gpw;
+    const int g = warp * gpw + lane / gsz;
+    const size_t total = (size_t)*count * (size_t)slices;
+    for (size_t p = blockIdx.x; p < total; p += gridDim.x) {
+        const uint32_t r = (uint32_t)(p / slices);
+        const int j_lo = (int)(p % slices) * span;
+        const int j_hi = j_lo + span < k ? j_lo + span : k;
+        const uint32_t row = rows[r];
+        const size_t src = gather ? gather[row] : (size_t)row;
+        const T* xr = x + src * (size_t)d;
+        unsigned long long best = ~0ull;
+        for (int j0 = j_lo; j0 < j_hi; j0 += 2 * G) {
+            const int ja = j0 + g, jb = j0 + G + g;
+            const int jac = ja < j_hi ? ja : j_hi - 1, jbc = jb < j_hi ? jb : j_hi - 1;
+            const float da = group_dot_ref(match, xr, c + (size_t)jac * d, d, lane);
+            const float db = group_dot_ref(match, xr, c + (size_t)jbc * d, d, lane);
+            if (ja < j_hi) {
+                const float s = score_ref(norms[ja], da);
+                if (s < __int_as_float(0x7f800000)) best = min(best, research_key(s, (uint32_t)ja));
+            }
+            if (jb < j_hi) {
+                const float s = score_ref(norms[jb], db);
+                if (s < __int_as_float(0x7f800000)) best = min(best, research_key(s, (uint32_t)jb));
+            }
+        }
+        if ((lane & (gsz - 1)) == 0) sk[g] = best;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            unsigned long long b = ~0ull;
+            for (int q = 0; q < G; q++) b = min(b, sk[q]);
+            if (b != ~0ull) atomicMin(&keys[r], b);
+        }
+        __syncthreads();
+    }
+}
+
+// Labels and distances of the split search: dist = max(best + sqnorm(x), 0). One warp per row.
+template <typename T>
+__global__ void k_research_finish(const T* __restrict__ x, const uint32_t* __restrict__ gather, int d,
+                                  const uint32_t* __restrict__ rows, const uint32_t* __restrict__ count,
+                                  const unsigned long long* __restrict__ keys, uint32_t* __restrict__ labels,
+                                  float* __restrict__ dist) {
+    const uint32_t r = (uint32_t)(((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31;
+    if (r >= *count) return;
+    const uint32_t row = rows[r];
+    const size_t src = gather ? gather[row] : (size_t)row;
+    const float xn = warp_sqnorm_ref(x + src * (size_t)d, d, lane);
+    if (lane == 0) {
+        const unsigned long long key = keys[r];
+        labels[row] = (uint32_t)(key & 0xffffffffu);
+        dist[row] = fmaxf(__fadd_rn(research_key_score(key), xn), 0.0f);
+    }
+}
+
 // Exact re-search (src/cpu.rs:108-167 semantics) of the rows in redo_rows:
 // every centroid scored in the reference rounding, strict < in ascending j
 // (lowest index on ties), best starts at +inf with label 0; dist =

@@ -237,10 +237,12 @@ __global__ void k_adam(float* __restrict__ w, __nv_bfloat16* __restrict__ wb, co
     if (wb) wb[i] = __float2bfloat16_rn(v);
 }
 
-// Top-m groups per row from G logits (one warp per row), and the softmax mass
-// those m groups carry (the proposer's confidence).
+// Top-m groups per row from G logits (one warp per row), the softmax mass those
+// m groups carry (the proposer's confidence), and how many of them to search:
+// the fewest whose mass reaches mass_target (all m when mass_target <= 0 or
+// when the m together fall short).
 __global__ void k_topm_groups(const float* __restrict__ logits, int m, int G, int top, uint16_t* __restrict__ groups,
-                              float* __restrict__ conf) {
+                              float* __restrict__ conf, float mass_target, uint8_t* __restrict__ cnt) {
     const int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
     if (row >= m) return;
     const float* l = logits + (size_t)row * G;
@@ -258,6 +260,7 @@ __global__ void k_topm_groups(const float* __restrict__ logits, int m, int G, in
     for (int i = 0; i < 16; i++) se += (v[i] > -INFINITY) ? __expf(v[i] - mx) : 0.0f;
     for (int o = 16; o; o >>= 1) se += __shfl_xor_sync(0xffffffffu, se, o);
     float mass = 0.0f;
+    int n_search = top;
     for (int s = 0; s < top; s++) {
         float bv = -INFINITY;
         int bi = 0x7fffffff;
@@ -278,13 +281,17 @@ __global__ void k_topm_groups(const float* __restrict__ logits, int m, int G, in
         if (bi >= G) bi = 0;  // no finite logit left (a diverged network): any valid group
         if (lane == 0) groups[(size_t)row * top + s] = (uint16_t)bi;
         mass += __expf(bv - mx);
+        if (mass_target > 0.0f && n_search == top && mass >= mass_target * se) n_search = s + 1;
         if ((bi & 31) == lane) {
 #pragma unroll
             for (int i = 0; i < 16; i++)
                 if (lane + 32 * i == bi) v[i] = -INFINITY;
         }
     }
-    if (lane == 0) conf[row] = mass / se;
+    if (lane == 0) {
+        conf[row] = mass / se;
+        cnt[row] = (uint8_t)n_search;
+    }
 }
 
 }  // namespace emb

@@ -34,6 +34,8 @@ struct MlpTcParams {
     float* conf;               // [m]
     float* logits;             // optional [m][G]
     int* err;                  // set to 1 if a bounded wait gave up
+    float mass_target;         // search the fewest groups whose mass reaches it (<= 0: all `top`)
+    uint8_t* cnt;              // [m] groups to search
 };
 
 struct MlpTcSmem {
@@ -41,9 +43,13 @@ struct MlpTcSmem {
     int nstages;
 };
 
-__host__ __device__ inline MlpTcSmem mlp_tc_smem(int kin, int H) {
+// The activation buffer also holds the layer-3 merge records, 4 x 128 rows x
+// (2 topc + 2) floats, once the tile's last MMAs have completed.
+__host__ __device__ inline MlpTcSmem mlp_tc_smem(int kin, int H, int topc) {
     MlpTcSmem s;
-    const uint32_t act = (uint32_t)kTcBM * 2 * (uint32_t)(kin > H ? kin : H);
+    const uint32_t acts = (uint32_t)kTcBM * 2 * (uint32_t)(kin > H ? kin : H);
+    const uint32_t merge = 4u * kTcBM * (uint32_t)(2 * topc + 2) * 4u;
+    const uint32_t act = acts > merge ? acts : merge;
     const uint32_t stage = 256u * 128u;  // 256 output columns x 64 BF16
     s.act = 0;
     s.stages = act;
@@ -101,7 +107,7 @@ k_mlp_tc(const __grid_constant__ CUtensorMap map_w1, const __grid_constant__ CUt
          const __grid_constant__ CUtensorMap map_w3, const MlpTcParams p) {
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
-    const MlpTcSmem L = mlp_tc_smem(p.kin, p.H);
+    const MlpTcSmem L = mlp_tc_smem(p.kin, p.H, TOPC);
     const int S = L.nstages;
     uint64_t* full = (uint64_t*)(smem + L.bars);  // [kMlpMaxStages]
     uint64_t* empty = full + kMlpMaxStages;       // [kMlpMaxStages]
@@ -334,6 +340,7 @@ k_mlp_tc(const __grid_constant__ CUtensorMap map_w1, const __grid_constant__ CUt
                     Ssum += f[2 * TOPC + 1] * __expf(f[2 * TOPC] - M);
                 }
                 float mass = 0.0f;
+                int n_search = p.top;
                 for (int s = 0; s < p.top; s++) {
                     float bv = -INFINITY;
                     int bi = 0x7fffffff, bo = 0;
@@ -353,8 +360,10 @@ k_mlp_tc(const __grid_constant__ CUtensorMap map_w1, const __grid_constant__ CUt
                     if (bi < 0 || bi >= p.G) bi = 0;  // no finite logit left (a diverged network): any valid group
                     p.groups[(size_t)row * p.top + s] = (uint16_t)bi;
                     mass += __expf(bv - M);
+                    if (p.mass_target > 0.0f && n_search == p.top && mass >= p.mass_target * Ssum) n_search = s + 1;
                 }
                 p.conf[row] = mass / Ssum;
+                p.cnt[row] = (uint8_t)n_search;
             }
             // The next tile's input overwrites the merge records.
             asm volatile("bar.sync 1, %0;" ::"n"(kTcEpiWarps * 32) : "memory");

@@ -11,26 +11,58 @@ constexpr int kBucketTile = 128;  // rows per bucket tile (the tensor-core kerne
 
 // Rows whose proposal confidence reaches thr go to the grouped search (hc), the
 // others to the full search (lc). Lists hold absolute row indices (row0 + r) and
-// chunk-local ones; counts in ctr[0] (hc) and ctr[1] (lc).
+// chunk-local ones; counts in ctr[0] (hc) and ctr[1] (lc); one atomic per warp and list.
 __global__ void k_split_confidence(const float* __restrict__ conf, int m, float thr, uint32_t row0,
                                    uint32_t* __restrict__ hc_abs, uint32_t* __restrict__ hc_loc,
                                    uint32_t* __restrict__ lc_abs, uint32_t* __restrict__ lc_loc,
                                    uint32_t* __restrict__ ctr) {
-    const int r = blockIdx.x * blockDim.x + threadIdx.x;
-    if (r >= m) return;
-    const bool hc = conf[r] >= thr;
-    const uint32_t slot = atomicAdd(ctr + (hc ? 0 : 1), 1u);
+    const int r = blockIdx.x * blockDim.x + threadIdx.x, lane = threadIdx.x & 31;
+    const bool in = r < m;
+    const bool hc = in && conf[r] >= thr;
+    const uint32_t mh = __ballot_sync(0xffffffffu, hc), ml = __ballot_sync(0xffffffffu, in && !hc);
+    uint32_t bh = 0, bl = 0;
+    if (lane == 0) {
+        if (mh) bh = atomicAdd(ctr, (uint32_t)__popc(mh));
+        if (ml) bl = atomicAdd(ctr + 1, (uint32_t)__popc(ml));
+    }
+    bh = __shfl_sync(0xffffffffu, bh, 0);
+    bl = __shfl_sync(0xffffffffu, bl, 0);
+    if (!in) return;
+    const uint32_t below = (1u << lane) - 1u;
+    const uint32_t slot = hc ? bh + __popc(mh & below) : bl + __popc(ml & below);
     (hc ? hc_abs : lc_abs)[slot] = row0 + (uint32_t)r;
     (hc ? hc_loc : lc_loc)[slot] = (uint32_t)r;
 }
 
-// counts[g] += number of hc rows proposing group g.
-__global__ void k_bucket_count(const uint16_t* __restrict__ grp, const uint32_t* __restrict__ hc_loc, int n, int top,
-                               uint32_t* __restrict__ counts) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n * top) return;
-    const uint32_t r = hc_loc[i / top];
-    atomicAdd(&counts[grp[(size_t)r * top + i % top]], 1u);
+constexpr int kBucketPairs = 2048;  // (row, slot) pairs per bucketing block (8 per thread)
+
+// counts[g] += number of (hc row, slot < cnt[row]) pairs proposing group g (a
+// shared-memory histogram per block, one global atomic per group and block);
+// pairs_total += all of them.
+__global__ void __launch_bounds__(256) k_bucket_count(const uint16_t* __restrict__ grp, const uint8_t* __restrict__ cnt,
+                                                      const uint32_t* __restrict__ hc_loc, int n, int top, int G,
+                                                      uint32_t* __restrict__ counts,
+                                                      unsigned long long* __restrict__ pairs_total) {
+    __shared__ uint32_t hist[512];
+    __shared__ uint32_t block_pairs;
+    if (threadIdx.x == 0) block_pairs = 0;
+    for (int g = threadIdx.x; g < G; g += blockDim.x) hist[g] = 0;
+    __syncthreads();
+    const int total = n * top, i0 = blockIdx.x * kBucketPairs;
+    const int i1 = i0 + kBucketPairs < total ? i0 + kBucketPairs : total;
+    for (int i = i0 + threadIdx.x; i < i1; i += blockDim.x) {
+        const uint32_t r = hc_loc[i / top];
+        const int s = i % top;
+        if (s < cnt[r]) atomicAdd(&hist[grp[(size_t)r * top + s]], 1u);
+    }
+    __syncthreads();
+    for (int g = threadIdx.x; g < G; g += blockDim.x)
+        if (hist[g]) {
+            atomicAdd(&counts[g], hist[g]);
+            atomicAdd(&block_pairs, hist[g]);
+        }
+    __syncthreads();
+    if (threadIdx.x == 0 && block_pairs) atomicAdd(pairs_total, (unsigned long long)block_pairs);
 }
 
 // One block: group g's bucket starts at the sum of the earlier groups' counts,
@@ -62,18 +94,53 @@ __global__ void k_fill_first(uint32_t* __restrict__ out, size_t n, const uint32_
     if (i < n) out[i] = src[0];
 }
 
-// Place each (hc row, slot) pair in its group's bucket: brow[pos] = absolute row,
-// bpos[i * top + s] = pos. The order inside a bucket does not affect any result.
-__global__ void k_bucket_scatter(const uint16_t* __restrict__ grp, const uint32_t* __restrict__ hc_loc,
-                                 const uint32_t* __restrict__ hc_abs, int n, int top, uint32_t* __restrict__ cursor,
-                                 uint32_t* __restrict__ brow, uint32_t* __restrict__ bpos) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n * top) return;
-    const int q = i / top, s = i % top;
-    const uint32_t g = grp[(size_t)hc_loc[q] * top + s];
-    const uint32_t pos = atomicAdd(&cursor[g], 1u);
-    brow[pos] = hc_abs[q];
-    bpos[i] = pos;
+// Place each (hc row, slot < cnt) pair in its group's bucket: brow[pos] = absolute
+// row, bpos[i * top + s] = pos (UINT32_MAX for slots not searched). Each block
+// ranks its pairs in a shared-memory histogram and reserves one range per group.
+// The order inside a bucket does not affect any result.
+__global__ void __launch_bounds__(256) k_bucket_scatter(const uint16_t* __restrict__ grp,
+                                                        const uint8_t* __restrict__ cnt,
+                                                        const uint32_t* __restrict__ hc_loc,
+                                                        const uint32_t* __restrict__ hc_abs, int n, int top, int G,
+                                                        uint32_t* __restrict__ cursor, uint32_t* __restrict__ brow,
+                                                        uint32_t* __restrict__ bpos) {
+    __shared__ uint32_t hist[512], base[512];
+    for (int g = threadIdx.x; g < G; g += blockDim.x) hist[g] = 0;
+    __syncthreads();
+    const int total = n * top, i0 = blockIdx.x * kBucketPairs;
+    constexpr int per = kBucketPairs / 256;
+    uint32_t rank[per];
+    int gg[per];
+#pragma unroll
+    for (int j = 0; j < per; j++) {
+        const int i = i0 + j * 256 + (int)threadIdx.x;
+        gg[j] = -1;
+        rank[j] = 0;
+        if (i < total) {
+            const uint32_t r = hc_loc[i / top];
+            const int s = i % top;
+            if (s < cnt[r]) {
+                gg[j] = grp[(size_t)r * top + s];
+                rank[j] = atomicAdd(&hist[gg[j]], 1u);
+            }
+        }
+    }
+    __syncthreads();
+    for (int g = threadIdx.x; g < G; g += blockDim.x)
+        if (hist[g]) base[g] = atomicAdd(&cursor[g], hist[g]);
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < per; j++) {
+        const int i = i0 + j * 256 + (int)threadIdx.x;
+        if (i >= total) continue;
+        if (gg[j] < 0) {
+            bpos[i] = 0xffffffffu;
+            continue;
+        }
+        const uint32_t pos = base[gg[j]] + rank[j];
+        brow[pos] = hc_abs[i / top];
+        bpos[i] = pos;
+    }
 }
 
 // Per hc row: merge the top-2 of its `top` bucket positions (columns of the sorted
@@ -88,7 +155,9 @@ __global__ void k_merge_slots(int n, int top, const uint32_t* __restrict__ bpos,
     Top2 t;
     t.init();
     for (int s = 0; s < top; s++) {
-        const size_t pos = bpos[(size_t)i * top + s];
+        const uint32_t bp = bpos[(size_t)i * top + s];
+        if (bp == 0xffffffffu) continue;  // slot not searched
+        const size_t pos = bp;
 #pragma unroll
         for (int e = 0; e < 2; e++) {
             const uint32_t col = gi[pos * 2 + e];

@@ -106,6 +106,7 @@ typedef struct {
     uint64_t rows_proposed;   /* proposer assign: rows searched in their proposed groups only */
     uint64_t rows_lowconf;    /* proposer assign: rows below the confidence threshold (full search) */
     double propose_ms;        /* proposer assign: device time of the proposals (network or group centroids) */
+    uint64_t groups_searched; /* proposer assign: (row, group) pairs scored by the grouped search */
 } emb200_stats;
 
 /* ---- lifecycle ---------------------------------------------------------- */
@@ -211,7 +212,9 @@ typedef struct {
     float lr;             /* Adam learning rate (decays linearly to lr/10 over a train call); 0 = 2e-3 */
     float group_epochs;   /* e-means epochs of the grouping; 0 = 5 */
     uint64_t seed;        /* grouping and initialisation seed */
-    uint32_t reserved[4];
+    float mass;           /* MLP mode: search only the fewest of the `top` groups whose softmax mass
+                             reaches this (<= 0: all `top`) */
+    uint32_t reserved[3];
 } emb200_proposer_config;
 
 /* Groups the current centroids, builds the group-sorted copy and initialises the
@@ -221,8 +224,8 @@ int emb200_proposer_init(emb200_handle* h, const emb200_proposer_config* cfg);
  * rows_n labels, e.g. train()'s output; UINT32_MAX rows are skipped): targets
  * are the labels' groups. losses: optional host array of `steps` mean losses. */
 int emb200_proposer_train(emb200_handle* h, const uint32_t* labels, size_t n, uint32_t steps, float* losses);
-/* Mode, groups per row and confidence threshold for later assigns. */
-int emb200_proposer_set(emb200_handle* h, uint32_t mode, uint32_t top, float confidence);
+/* Mode, groups per row, confidence threshold and mass target for later assigns. */
+int emb200_proposer_set(emb200_handle* h, uint32_t mode, uint32_t top, float confidence, float mass);
 /* Network parameters as one f32 array: input mean[d], input 1/std[d], W1[H][d],
  * b1[H], W2[H][H], b2[H], W3[G][H], b3[G], each block starting at a multiple of 8. */
 size_t emb200_proposer_param_count(const emb200_handle* h);
@@ -238,8 +241,11 @@ int emb200_proposer_grad(emb200_handle* h, const float* x, const uint32_t* targe
 int emb200_proposer_logits(emb200_handle* h, const float* x, size_t m, float* logits, int fused);
 /* Group of every centroid (k entries). */
 int emb200_proposer_groups(emb200_handle* h, uint32_t* group_of);
-/* Proposals for m host rows: groups[m][top] (most likely first) and confidence[m]. */
-int emb200_propose(emb200_handle* h, const float* x, size_t m, uint32_t* groups, float* confidence);
+/* Proposals for m host rows: groups[m][top] (most likely first), confidence[m]
+ * and counts[m] (how many of them the proposer assign searches); confidence and
+ * counts may be NULL. */
+int emb200_propose(emb200_handle* h, const float* x, size_t m, uint32_t* groups, float* confidence,
+                   uint32_t* counts);
 /* The proposer assign over the resident f32 rows (labels/dist host arrays of n,
  * or NULL to keep them on the device), or over m device rows on `stream`. */
 int emb200_assign_proposed_resident(emb200_handle* h, uint32_t* labels, float* dist);

@@ -170,19 +170,26 @@ def test_learned_proposer_beats_group_centroids(trained):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("mode", ["mlp", "centroids"])
-def test_proposer_assign_guarantees(trained, orc, mode):
+@pytest.mark.parametrize("mode,top,mass", [("mlp", TOP, 0.0), ("centroids", TOP, 0.0), ("mlp", 16, 0.99)])
+def test_proposer_assign_guarantees(trained, orc, mode, top, mass):
     a, x, _, out, _ = trained
-    a.proposer_set(mode, TOP, 0.0)
+    a.proposer_set(mode, top, 0.0, mass)
     lab_p, dist_p = a.assign_proposed()
     st = a.stats()
     lab_f, dist_f = a.assign_resident()
     n = x.shape[0]
     assert st["rows_proposed"] + st["rows_lowconf"] == n
     assert st["fast_aborted"] == 0
-    props, _ = a.propose(x)
+    props, _, cnt = a.propose(x, with_counts=True)
+    assert np.all((cnt >= 1) & (cnt <= top))
+    if mass == 0.0:
+        assert np.all(cnt == top)
+    else:
+        assert cnt.mean() < top
+    # the grouped search scored exactly the proposed (row, group) pairs
+    assert st["groups_searched"] == int(cnt.sum())
     gof = a.proposer_groups()
-    covered = np.array([gof[l] in row for l, row in zip(lab_f, props)])
+    covered = np.array([gof[l] in row[:c] for l, row, c in zip(lab_f, props, cnt)])
     same = lab_p == lab_f
     # 1. wherever the exact label's group was proposed, the label is the exact one
     assert np.all(same[covered])
