@@ -23,6 +23,7 @@
 #include "kernels_simt.cuh"
 #include "kernels_tc.cuh"
 #include "kernels_tc_i8.cuh"
+#include "kernels_tc_grouped.cuh"
 #include "kernels_update.cuh"
 #include "kernels_mlp.cuh"
 #include "kernels_mlp_tc.cuh"
@@ -408,8 +409,7 @@ int tc_nsplit(const emb200_handle* h, size_t m) {
 template <typename T, bool COLLECT>
 int launch_tc(emb200_handle* h, const T* x, const uint32_t* gather, const uint32_t* gather2, size_t m, int nterms,
               const float* theta, uint32_t* cand, uint32_t* cand_count, int cap, int* err, cudaStream_t st,
-              const uint32_t* m_dev = nullptr, int nsplit_override = 0, const int* tile_group = nullptr,
-              const int* grp_cbeg = nullptr, const int* grp_ntiles = nullptr) {
+              const uint32_t* m_dev = nullptr, int nsplit_override = 0) {
     TcParams p{};
     p.m = (int)m;
     p.d = (int)h->d;
@@ -428,9 +428,6 @@ int launch_tc(emb200_handle* h, const T* x, const uint32_t* gather, const uint32
     p.cand_count = cand_count;
     p.cand_cap = cap;
     p.m_dev = m_dev;
-    p.tile_group = tile_group;  // grouped search: m is a whole number of bucket tiles
-    p.grp_cbeg = grp_cbeg;
-    p.grp_ntiles = grp_ntiles;
     TcSmem L = tc_smem_layout(p.kpad, p.nterms);
     // At least 120 KB so that two CTAs never share an SM: each holds all 512 TMEM columns.
     size_t smem = std::max<size_t>(L.total + 1024, 120 * 1024);
@@ -439,7 +436,7 @@ int launch_tc(emb200_handle* h, const T* x, const uint32_t* gather, const uint32
         CK(cudaFuncSetAttribute(k_assign_tc<T, COLLECT>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
         attr_set = true;
     }
-    int nsplit = tile_group ? 1 : nsplit_override > 0 ? nsplit_override : tc_nsplit(h, m);
+    int nsplit = nsplit_override > 0 ? nsplit_override : tc_nsplit(h, m);
     dim3 grid((unsigned)((m + kTcBM - 1) / kTcBM), (unsigned)nsplit);
     k_assign_tc<T, COLLECT><<<grid, kTcThreads, smem, st>>>(x, h->map_hi, h->map_lo, p);
     CKL();

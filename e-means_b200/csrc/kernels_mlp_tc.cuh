@@ -61,6 +61,9 @@ __host__ __device__ inline MlpTcSmem mlp_tc_smem(int kin, int H, int topc) {
     return s;
 }
 
+// Each epilogue thread keeps the TOPC best of its 64 (or 32) columns; the merge
+// of the four quarters' lists gives the exact top TOPC, and for top up to 4 TOPC
+// the best of what the lists hold.
 // Insert (v, j) into a descending list of length N (ties keep the earlier column first).
 template <int N>
 EMB_DEV void topn_insert(float (&val)[N], int (&idx)[N], float v, int j) {

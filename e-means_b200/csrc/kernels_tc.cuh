@@ -57,9 +57,10 @@ struct TcParams {
     uint32_t* cand_count;     // COLLECT: [m] candidates found (may exceed cand_cap)
     int cand_cap;
     const uint32_t* m_dev;    // COLLECT: if set, the row count is min(m, *m_dev), read on the device
-    // Grouped search (centroid groups of a group-sorted matrix): row tile t scores
-    // only group tile_group[t] (-1: no work), columns [grp_cbeg[g], + 256 grp_ntiles[g]).
-    // Column starts are multiples of 32, so packed keys and the norms copy stay aligned.
+    // Grouped search (k_assign_grouped, centroid groups of a group-sorted matrix):
+    // bucket tile t scores only group tile_group[t] (-1: past the last tile),
+    // columns [grp_cbeg[g], + 256 grp_ntiles[g]). Column starts are multiples of
+    // 32, so packed keys and the norms copy stay aligned.
     const int* tile_group;
     const int* grp_cbeg;
     const int* grp_ntiles;
@@ -216,43 +217,56 @@ EMB_DEV uint32_t sw128_offset(int r, int kc, int rows) {
 
 template <typename T>
 EMB_DEV void tc_load_rows(uint8_t* smem, const TcSmem& L, const T* __restrict__ x, const TcParams& p, int row0,
-                          int m) {
-    // 128 rows x (kpad / 8) chunks of 8 elements; each thread converts chunks.
+                          int m, int tid, int nthr) {
+    // 128 rows x (kpad / 8) chunks of 8 elements. Each thread issues the loads of
+    // up to four chunks before converting any of them, so that four gathered
+    // rows' latencies overlap instead of following one another.
+    constexpr int kBatch = 4;
     const int nchunk = p.kpad / 8;
     const int total = kTcBM * nchunk;
-    for (int t = threadIdx.x; t < total; t += blockDim.x) {
-        int r = t / nchunk, kc = t % nchunk;
-        int g = row0 + r;
-        float v[8];
-        if (g < m) {
+    for (int base = tid; base < total; base += kBatch * nthr) {
+        float v[kBatch][8];
+#pragma unroll
+        for (int u = 0; u < kBatch; u++) {
+            const int t = base + u * nthr;
+#pragma unroll
+            for (int i = 0; i < 8; i++) v[u][i] = 0.0f;
+            if (t >= total) continue;
+            const int r = t / nchunk, kc = t % nchunk;
+            const int g = row0 + r;
+            if (g >= m) continue;
             size_t src = p.gather2 ? (size_t)p.gather2[g] : (size_t)g;
             if (p.gather) src = p.gather[src];
             const T* xr = x + src * (size_t)p.d;
-            int k0 = kc * 8;
+            const int k0 = kc * 8;
             if (sizeof(T) == 4 && p.xvec && k0 + 8 <= p.d) {
-                float4 a = *reinterpret_cast<const float4*>(xr + k0);
-                float4 b = *reinterpret_cast<const float4*>(xr + k0 + 4);
-                v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w; v[4] = b.x; v[5] = b.y; v[6] = b.z; v[7] = b.w;
+                const float4 a = *reinterpret_cast<const float4*>(xr + k0);
+                const float4 b = *reinterpret_cast<const float4*>(xr + k0 + 4);
+                v[u][0] = a.x; v[u][1] = a.y; v[u][2] = a.z; v[u][3] = a.w;
+                v[u][4] = b.x; v[u][5] = b.y; v[u][6] = b.z; v[u][7] = b.w;
             } else {
 #pragma unroll
-                for (int i = 0; i < 8; i++) v[i] = (k0 + i < p.d) ? to_f32(xr[k0 + i]) : 0.0f;
+                for (int i = 0; i < 8; i++) v[u][i] = (k0 + i < p.d) ? to_f32(xr[k0 + i]) : 0.0f;
             }
-        } else {
-#pragma unroll
-            for (int i = 0; i < 8; i++) v[i] = 0.0f;
         }
-        uint32_t hw[4], lw[4];
 #pragma unroll
-        for (int i = 0; i < 4; i++) {
-            __nv_bfloat16 h0 = __float2bfloat16_rn(v[2 * i]), h1 = __float2bfloat16_rn(v[2 * i + 1]);
-            __nv_bfloat16 l0 = __float2bfloat16_rn(v[2 * i] - __bfloat162float(h0));
-            __nv_bfloat16 l1 = __float2bfloat16_rn(v[2 * i + 1] - __bfloat162float(h1));
-            hw[i] = (uint32_t)__bfloat16_as_ushort(h0) | ((uint32_t)__bfloat16_as_ushort(h1) << 16);
-            lw[i] = (uint32_t)__bfloat16_as_ushort(l0) | ((uint32_t)__bfloat16_as_ushort(l1) << 16);
+        for (int u = 0; u < kBatch; u++) {
+            const int t = base + u * nthr;
+            if (t >= total) continue;
+            const int r = t / nchunk, kc = t % nchunk;
+            uint32_t hw[4], lw[4];
+#pragma unroll
+            for (int i = 0; i < 4; i++) {
+                __nv_bfloat16 h0 = __float2bfloat16_rn(v[u][2 * i]), h1 = __float2bfloat16_rn(v[u][2 * i + 1]);
+                __nv_bfloat16 l0 = __float2bfloat16_rn(v[u][2 * i] - __bfloat162float(h0));
+                __nv_bfloat16 l1 = __float2bfloat16_rn(v[u][2 * i + 1] - __bfloat162float(h1));
+                hw[i] = (uint32_t)__bfloat16_as_ushort(h0) | ((uint32_t)__bfloat16_as_ushort(h1) << 16);
+                lw[i] = (uint32_t)__bfloat16_as_ushort(l0) | ((uint32_t)__bfloat16_as_ushort(l1) << 16);
+            }
+            const uint32_t off = sw128_offset(r, kc, kTcBM);
+            *reinterpret_cast<uint4*>(smem + L.a_hi + off) = make_uint4(hw[0], hw[1], hw[2], hw[3]);
+            if (p.nterms == 3) *reinterpret_cast<uint4*>(smem + L.a_lo + off) = make_uint4(lw[0], lw[1], lw[2], lw[3]);
         }
-        uint32_t off = sw128_offset(r, kc, kTcBM);
-        *reinterpret_cast<uint4*>(smem + L.a_hi + off) = make_uint4(hw[0], hw[1], hw[2], hw[3]);
-        if (p.nterms == 3) *reinterpret_cast<uint4*>(smem + L.a_lo + off) = make_uint4(lw[0], lw[1], lw[2], lw[3]);
     }
 }
 
@@ -342,7 +356,6 @@ EMB_DEV void tc_regs_ready(uint32_t (&v)[32]) {
 }
 
 // Grid: (ceil(m / 128), nsplit); CTA (bx, by) walks centroid tiles by, by + nsplit, ...
-// (grouped search: grid (bucket tiles, 1), CTA bx walks the tiles of group tile_group[bx]).
 // COLLECT = false: per-row top-2 of approximate scores to part_s/part_i.
 // COLLECT = true : every centroid with approximate score <= theta[row] is appended
 //                  to cand[row][*] (cand_count[row] counts all, capped storage).
@@ -374,16 +387,9 @@ k_assign_tc(const T* __restrict__ x, const __grid_constant__ CUtensorMap map_hi,
     }
     const int nsplit = gridDim.y;
     const int ntiles_all = (p.k + kTcBN - 1) / kTcBN;
-    int my_tiles = (int)blockIdx.y < ntiles_all ? (ntiles_all - (int)blockIdx.y + nsplit - 1) / nsplit : 0;
+    const int my_tiles = (int)blockIdx.y < ntiles_all ? (ntiles_all - (int)blockIdx.y + nsplit - 1) / nsplit : 0;
     // Column of this CTA's tile t: col_first + t * col_step.
-    int col_first = (int)blockIdx.y * kTcBN, col_step = nsplit * kTcBN;
-    if (p.tile_group) {
-        const int g = p.tile_group[blockIdx.x];
-        if (g < 0) return;  // past the last bucket tile: the whole CTA leaves before any setup
-        my_tiles = p.grp_ntiles[g];
-        col_first = p.grp_cbeg[g];
-        col_step = kTcBN;
-    }
+    const int col_first = (int)blockIdx.y * kTcBN, col_step = nsplit * kTcBN;
     const int natoms = p.kpad / 64;
 
     if (threadIdx.x == 0) {
@@ -400,7 +406,30 @@ k_assign_tc(const T* __restrict__ x, const __grid_constant__ CUtensorMap map_hi,
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     if (warp == 1) tmem_alloc(tmem_slot, kTcTmemCols);
-    tc_load_rows(smem, L, x, p, row0, m);
+    // ---- TMA producer unit u = (tile t, K atom a) into stage u % S; norms once per tile
+    const int nunits = my_tiles * natoms;
+    auto issue = [&](int u) {
+        const int t = u / natoms, a = u - t * natoms;
+        const int s = u % S;
+        const int col = col_first + t * col_step;
+        uint8_t* stage = smem + L.b0 + s * L.stage_bytes;
+        mbar_expect_tx(&full[s], L.stage_bytes);
+        tma_load_2d(stage, &map_hi, &full[s], a * 64, col);
+        if (p.nterms > 1) tma_load_2d(stage + L.term_bytes, &map_lo, &full[s], a * 64, col);
+        if (a == 0) {
+            const int ns = t % kTcNormSlots;
+            mbar_expect_tx(&norms_full[ns], kTcBN * 4);
+            bulk_load(norms_s + ns * kTcBN, p.norms + (size_t)col, kTcBN * 4, &norms_full[ns]);
+        }
+    };
+    __syncthreads();  // barriers initialised: the first stages load while the rows are gathered
+    int issued = 0;
+    if (warp == 0 && lane == 0) {
+        // The first S stages are free: no wait on `empty` before them.
+        issued = nunits < S ? nunits : S;
+        for (int u = 0; u < issued; u++) issue(u);
+    }
+    tc_load_rows(smem, L, x, p, row0, m, threadIdx.x, blockDim.x);
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     tc_fence_before();
     __syncthreads();
@@ -409,24 +438,11 @@ k_assign_tc(const T* __restrict__ x, const __grid_constant__ CUtensorMap map_hi,
 
     if (warp == 0) {
         if (lane == 0) {
-            // ---- TMA producer: unit u = (tile t, K atom a); norms once per tile
-            const int nunits = my_tiles * natoms;
-            int issued = 0;
-            for (int u = 0; u < nunits; u++) {
-                const int t = u / natoms, a = u - t * natoms;
+            for (int u = issued; u < nunits; u++) {
                 const int s = u % S;
                 const uint32_t ph = (uint32_t)(u / S) & 1u;
                 if (!mbar_wait(&empty[s], ph ^ 1u, abort_flag)) break;
-                const int col = col_first + t * col_step;
-                uint8_t* stage = smem + L.b0 + s * L.stage_bytes;
-                mbar_expect_tx(&full[s], L.stage_bytes);
-                tma_load_2d(stage, &map_hi, &full[s], a * 64, col);
-                if (p.nterms > 1) tma_load_2d(stage + L.term_bytes, &map_lo, &full[s], a * 64, col);
-                if (a == 0) {
-                    const int ns = t % kTcNormSlots;
-                    mbar_expect_tx(&norms_full[ns], kTcBN * 4);
-                    bulk_load(norms_s + ns * kTcBN, p.norms + (size_t)col, kTcBN * 4, &norms_full[ns]);
-                }
+                issue(u);
                 issued = u + 1;
             }
             // After an abort, let the copies still in flight land before the CTA
