@@ -466,7 +466,8 @@ int finish_counters(emb200_handle* h, cudaStream_t st, bool refined) {
 // [3] exhaustive rows, [4] refine abort.
 template <typename T>
 int settle_rows(emb200_handle* h, const T* x, const uint32_t* gather, size_t m, uint32_t* labels, float* dist,
-                cudaStream_t st, bool graph, int nsplit, int fast_prec, bool tc);
+                cudaStream_t st, bool graph, int nsplit, int fast_prec, bool tc,
+                const float2* row_bounds = nullptr);
 
 template <typename T>
 int assign_rows_dev(emb200_handle* h, const T* x, const uint32_t* gather, size_t m, uint32_t* labels, float* dist,
@@ -537,7 +538,7 @@ int launch_research(emb200_handle* h, const T* x, const uint32_t* gather, size_t
 // the fast kernel (which may have set the abort flag, counter 2).
 template <typename T>
 int settle_rows(emb200_handle* h, const T* x, const uint32_t* gather, size_t m, uint32_t* labels, float* dist,
-                cudaStream_t st, bool graph, int nsplit, int fast_prec, bool tc) {
+                cudaStream_t st, bool graph, int nsplit, int fast_prec, bool tc, const float2* row_bounds) {
     const int dtype = std::is_same<T, float>::value ? EMB200_F32 : (std::is_same<T, int8_t>::value ? EMB200_I8 : EMB200_U8);
     const int k = (int)h->k, d = (int)h->d;
     const int refine_terms = tc_terms(EMB200_PREC_BF16, dtype);
@@ -551,13 +552,14 @@ int settle_rows(emb200_handle* h, const T* x, const uint32_t* gather, size_t m, 
     if (match == kMatchAvx512) {
         k_certify16<T><<<(unsigned)((m + 15) / 16), 256, 0, st>>>(
             x, gather, (int)m, d, h->c.p, h->norms.p, k, h->part_s.p, h->part_i.p, nsplit, h->bounds.p, ka, kb, labels,
-            dist, h->redo_rows.p, ctr, ctr + 1, tc ? (const int*)(ctr + 2) : nullptr, h->redo_theta.p, ka2, kb2);
+            dist, h->redo_rows.p, ctr, ctr + 1, tc ? (const int*)(ctr + 2) : nullptr, h->redo_theta.p, ka2, kb2,
+            row_bounds);
     } else {
         k_certify<T><<<(unsigned)((m + 7) / 8), 256, 0, st>>>(x, gather, (int)m, d, h->c.p, h->norms.p, k, h->part_s.p,
                                                                h->part_i.p, nsplit, h->bounds.p, ka, kb, match, labels,
                                                                dist, h->redo_rows.p, ctr, ctr + 1,
                                                                tc ? (const int*)(ctr + 2) : nullptr, h->redo_theta.p,
-                                                               ka2, kb2);
+                                                               ka2, kb2, row_bounds);
     }
     CKL();
     if (graph) {

@@ -153,7 +153,8 @@ __global__ void k_certify(const T* __restrict__ x, const uint32_t* __restrict__ 
                           uint32_t* __restrict__ labels, float* __restrict__ dist,
                           uint32_t* __restrict__ redo_rows, uint32_t* __restrict__ redo_count,
                           uint32_t* __restrict__ cert_count, const int* __restrict__ fast_err,
-                          float* __restrict__ redo_theta, float ka2, float kb2) {
+                          float* __restrict__ redo_theta, float ka2, float kb2,
+                          const float2* __restrict__ row_bounds = nullptr) {
     int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     int lane = threadIdx.x & 31;
     if (row >= m) return;
@@ -190,7 +191,8 @@ __global__ void k_certify(const T* __restrict__ x, const uint32_t* __restrict__ 
     }
     if (ok && k > 2) {
         float xnorm = __fmul_ru(__fsqrt_ru(fmaxf(xn, 0.0f)), 1.0000005f);
-        float E = __fadd_ru(__fmul_ru(__fmul_ru(ka, xnorm), bounds->cmax), __fmul_ru(kb, bounds->nmax));
+        float E = __fadd_ru(__fmul_ru(__fmul_ru(ka, xnorm), row_bounds ? row_bounds[row].x : bounds->cmax),
+                                  __fmul_ru(kb, row_bounds ? row_bounds[row].y : bounds->nmax));
         float thr = __fsub_rd(t.s2, E);
         ok = isfinite(E) && sb < thr;  // NaN-safe: any NaN fails
     }
@@ -220,7 +222,9 @@ __global__ void k_certify(const T* __restrict__ x, const uint32_t* __restrict__ 
 // k_certify specialised to the AVX-512 rounding (the default): one half-warp
 // per row, so a warp certifies two rows, and one pass over the row computes its
 // sqnorm lanes and both candidates' 16 FMA lanes. Same decisions and outputs as
-// k_certify with match = AVX-512.
+// k_certify with match = AVX-512. row_bounds (optional): per row, (max |c|, max |norm|)
+// over the centroids whose approximate scores were compared, in place of the
+// bounds over all k; the refine threshold keeps the bounds over all k.
 template <typename T>
 __global__ void k_certify16(const T* __restrict__ x, const uint32_t* __restrict__ gather, int m, int d,
                             const float* __restrict__ c, const float* __restrict__ norms, int k,
@@ -229,7 +233,8 @@ __global__ void k_certify16(const T* __restrict__ x, const uint32_t* __restrict_
                             uint32_t* __restrict__ labels, float* __restrict__ dist,
                             uint32_t* __restrict__ redo_rows, uint32_t* __restrict__ redo_count,
                             uint32_t* __restrict__ cert_count, const int* __restrict__ fast_err,
-                            float* __restrict__ redo_theta, float ka2, float kb2) {
+                            float* __restrict__ redo_theta, float ka2, float kb2,
+                            const float2* __restrict__ row_bounds = nullptr) {
     const int lane = threadIdx.x & 31, l = lane & 15, half = lane >> 4;
     const int row = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 2 + half;
     const bool live = row < m;
@@ -285,7 +290,8 @@ __global__ void k_certify16(const T* __restrict__ x, const uint32_t* __restrict_
     }
     if (ok && k > 2) {
         const float xnorm = __fmul_ru(__fsqrt_ru(fmaxf(xn, 0.0f)), 1.0000005f);
-        const float E = __fadd_ru(__fmul_ru(__fmul_ru(ka, xnorm), bounds->cmax), __fmul_ru(kb, bounds->nmax));
+        const float E = __fadd_ru(__fmul_ru(__fmul_ru(ka, xnorm), row_bounds ? row_bounds[row].x : bounds->cmax),
+                                  __fmul_ru(kb, row_bounds ? row_bounds[row].y : bounds->nmax));
         const float thr = __fsub_rd(t.s2, E);
         ok = isfinite(E) && sb < thr;
     }

@@ -143,33 +143,109 @@ __global__ void __launch_bounds__(256) k_bucket_scatter(const uint16_t* __restri
     }
 }
 
-// Per hc row: merge the top-2 of its `top` bucket positions (columns of the sorted
-// matrix, mapped to centroid indices through perm; padding columns dropped; a
-// centroid seen twice, when tiles of neighbouring groups overlap, counted once)
-// into the part_s/part_i layout the certification reads (one split).
+// Per group: (max |c|, max |norm|) over the columns its tiles cover in the sorted
+// copy (padding rows excluded; columns of neighbouring groups that a tile
+// reaches included), upper-rounded as the bounds over all k are. One warp per
+// group, a lane per column.
+__global__ void k_group_bounds(const float* __restrict__ c, const float* __restrict__ norms,
+                               const uint32_t* __restrict__ perm, size_t ks, int d, const int* __restrict__ cbeg,
+                               const int* __restrict__ ntiles, int G, float2* __restrict__ gb) {
+    const int g = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (g >= G) return;
+    const size_t c0 = (size_t)cbeg[g];
+    size_t c1 = c0 + (size_t)ntiles[g] * 256;
+    if (c1 > ks) c1 = ks;
+    float cm = 0.0f, nm = 0.0f;
+    for (size_t j = c0 + lane; j < c1; j += 32) {
+        if (perm[j] == 0xffffffffu) continue;
+        float ss = 0.0f;
+        for (int t = 0; t < d; t++) {
+            const float v = c[j * d + t];
+            ss = __fmaf_ru(v, v, ss);
+        }
+        cm = fmaxf(cm, __fmul_ru(__fsqrt_ru(ss), 1.0000005f));
+        nm = fmaxf(nm, fabsf(norms[j]));
+    }
+    for (int o = 16; o; o >>= 1) {
+        cm = fmaxf(cm, __shfl_xor_sync(0xffffffffu, cm, o));
+        nm = fmaxf(nm, __shfl_xor_sync(0xffffffffu, nm, o));
+    }
+    if (lane == 0) gb[g] = make_float2(cm, nm);
+}
+
+// Lexicographic (score, index) minimum of two candidates.
+EMB_DEV void lex_min_into(float& s, uint32_t& j, float s2, uint32_t j2) {
+    if (lex_less(s2, j2, s, j)) {
+        s = s2;
+        j = j2;
+    }
+}
+
+// Per hc row (one warp; lane = slot, top <= 32): merge the top-2 of its bucket
+// positions (columns of the sorted matrix mapped to centroid indices through
+// perm, padding columns dropped) into the part_s/part_i layout the certification
+// reads (one split): the lexicographic (score, index) minimum, then the minimum
+// among the candidates with another index (a centroid seen twice, when tiles of
+// neighbouring groups overlap, counts once). Also the row's bounds: the largest
+// (max |c|, max |norm|) of its searched groups.
 __global__ void k_merge_slots(int n, int top, const uint32_t* __restrict__ bpos, const float* __restrict__ gs,
                               const uint32_t* __restrict__ gi, const uint32_t* __restrict__ perm, uint32_t ks,
-                              float* __restrict__ part_s, uint32_t* __restrict__ part_i) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+                              float* __restrict__ part_s, uint32_t* __restrict__ part_i,
+                              const uint16_t* __restrict__ grp, const uint32_t* __restrict__ hc_loc,
+                              const float2* __restrict__ gb, float2* __restrict__ row_bounds) {
+    const int i = (int)(((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
     if (i >= n) return;
-    Top2 t;
-    t.init();
-    for (int s = 0; s < top; s++) {
-        const uint32_t bp = bpos[(size_t)i * top + s];
-        if (bp == 0xffffffffu) continue;  // slot not searched
-        const size_t pos = bp;
+    const float inf = __int_as_float(0x7f800000);
+    float a_s = inf, b_s = inf;  // this lane's two candidates, a before b
+    uint32_t a_j = 0xffffffffu, b_j = 0xffffffffu;
+    float cm = 0.0f, nm = 0.0f;
+    if (lane < top) {
+        const uint32_t bp = bpos[(size_t)i * top + lane];
+        if (bp != 0xffffffffu) {
+            const float2 b = gb[grp[(size_t)hc_loc[i] * top + lane]];
+            cm = b.x;
+            nm = b.y;
 #pragma unroll
-        for (int e = 0; e < 2; e++) {
-            const uint32_t col = gi[pos * 2 + e];
-            const uint32_t j = col < ks ? perm[col] : 0xffffffffu;
-            if (j == 0xffffffffu || j == t.i1 || j == t.i2) continue;
-            t.push(gs[pos * 2 + e], j);
+            for (int e = 0; e < 2; e++) {
+                const uint32_t col = gi[(size_t)bp * 2 + e];
+                const uint32_t j = col < ks ? perm[col] : 0xffffffffu;
+                if (j == 0xffffffffu) continue;
+                const float sc = gs[(size_t)bp * 2 + e];
+                if (lex_less(sc, j, a_s, a_j)) {
+                    b_s = a_s;
+                    b_j = a_j;
+                    a_s = sc;
+                    a_j = j;
+                } else if (lex_less(sc, j, b_s, b_j)) {
+                    b_s = sc;
+                    b_j = j;
+                }
+            }
         }
     }
-    part_s[(size_t)i * 2] = t.s1;
-    part_s[(size_t)i * 2 + 1] = t.s2;
-    part_i[(size_t)i * 2] = t.i1;
-    part_i[(size_t)i * 2 + 1] = t.i2;
+    float s1 = a_s;
+    uint32_t j1 = a_j;
+    for (int o = 16; o; o >>= 1) {
+        lex_min_into(s1, j1, __shfl_xor_sync(0xffffffffu, s1, o), __shfl_xor_sync(0xffffffffu, j1, o));
+        cm = fmaxf(cm, __shfl_xor_sync(0xffffffffu, cm, o));
+        nm = fmaxf(nm, __shfl_xor_sync(0xffffffffu, nm, o));
+    }
+    // A lane's two candidates are distinct centroids: if its first is the winner, its second competes.
+    float s2 = a_j == j1 ? b_s : a_s;
+    uint32_t j2 = a_j == j1 ? b_j : a_j;
+    if (j2 == j1) {
+        s2 = inf;
+        j2 = 0xffffffffu;
+    }
+    for (int o = 16; o; o >>= 1)
+        lex_min_into(s2, j2, __shfl_xor_sync(0xffffffffu, s2, o), __shfl_xor_sync(0xffffffffu, j2, o));
+    if (lane == 0) {
+        row_bounds[i] = make_float2(cm, nm);
+        part_s[(size_t)i * 2] = s1;
+        part_s[(size_t)i * 2 + 1] = s2;
+        part_i[(size_t)i * 2] = j1;
+        part_i[(size_t)i * 2 + 1] = j2;
+    }
 }
 
 // labels[loc[i]] = src_labels[i] (and dist).

@@ -18,6 +18,23 @@
 
 namespace emb {
 
+// Ask L2 for the rows of a bucket tile ahead of their gather (prefetches are
+// hints: nothing waits on them, and an address is never past its row's end).
+template <typename T>
+EMB_DEV void prefetch_rows_l2(const T* __restrict__ x, const TcParams& p, int row0, int tid, int nthr) {
+    const int row_bytes = p.d * (int)sizeof(T);
+    const int lines = row_bytes / 128 + 2;  // rows need not start on a 128-byte line
+    for (int t = tid; t < kTcBM * lines; t += nthr) {
+        const int r = t / lines, l = t - r * lines;
+        const int g = row0 + r;
+        if (g >= p.m) continue;
+        const size_t src = p.gather ? (size_t)p.gather[g] : (size_t)g;
+        const char* base = (const char*)(x + src * (size_t)p.d);
+        const int off = l * 128 < row_bytes ? l * 128 : row_bytes - 1;
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(base + off));
+    }
+}
+
 template <typename T>
 __global__ void __launch_bounds__(kTcThreads, 1)
 k_assign_grouped(const T* __restrict__ x, const __grid_constant__ CUtensorMap map_hi,
@@ -72,7 +89,7 @@ k_assign_grouped(const T* __restrict__ x, const __grid_constant__ CUtensorMap ma
     if (warp == 0) {
         if (lane == 0) {
             // ---- TMA producer
-            int u = 0, tg = 0, w, g;
+            int u = 0, tg = 0, norms_issued = 0, w, g;
             bool ok = true;
             for (int i = 0; ok && work(i, w, g); i++) {
                 const int nt = p.grp_ntiles[g], c0 = p.grp_cbeg[g];
@@ -93,6 +110,7 @@ k_assign_grouped(const T* __restrict__ x, const __grid_constant__ CUtensorMap ma
                             const int ns = tg % kTcNormSlots;
                             mbar_expect_tx(&norms_full[ns], kTcBN * 4);
                             bulk_load(norms_s + ns * kTcBN, p.norms + (size_t)col, kTcBN * 4, &norms_full[ns]);
+                            norms_issued = tg + 1;
                         }
                     }
                 }
@@ -105,7 +123,7 @@ k_assign_grouped(const T* __restrict__ x, const __grid_constant__ CUtensorMap ma
                     while (!mbar_try(&full[v % S], ph) && global_ns() - t0 < kWaitLimitNs) {
                     }
                 }
-                for (int t = tg > kTcNormSlots ? tg - kTcNormSlots : 0; t < tg; t++) {
+                for (int t = norms_issued > kTcNormSlots ? norms_issued - kTcNormSlots : 0; t < norms_issued; t++) {
                     const uint32_t nph = (uint32_t)(t / kTcNormSlots) & 1u;
                     while (!mbar_try(&norms_full[t % kTcNormSlots], nph) && global_ns() - t0 < kWaitLimitNs) {
                     }
@@ -186,6 +204,7 @@ k_assign_grouped(const T* __restrict__ x, const __grid_constant__ CUtensorMap ma
             const int nt = p.grp_ntiles[g], c0 = p.grp_cbeg[g];
             int wn, gn;
             const bool has_next = work(i + 1, wn, gn);
+            if (has_next && ok) prefetch_rows_l2(x, p, wn * kTcBM, et, kTcEpiWarps * 32);
             const int row = w * kTcBM + r;
             Top2 top;
             top.init();
