@@ -94,8 +94,8 @@ __global__ void k_fill_first(uint32_t* __restrict__ out, size_t n, const uint32_
     if (i < n) out[i] = src[0];
 }
 
-// Place each (hc row, slot < cnt) pair in its group's bucket: brow[pos] = absolute
-// row, bpos[i * top + s] = pos (UINT32_MAX for slots not searched). Each block
+// Place each (hc row, slot < cnt) pair in its group's bucket: brow[pos] =
+// rows[hc row] (the caller's numbering), bpos[i * top + s] = pos (UINT32_MAX for slots not searched). Each block
 // ranks its pairs in a shared-memory histogram and reserves one range per group.
 // The order inside a bucket does not affect any result.
 __global__ void __launch_bounds__(256) k_bucket_scatter(const uint16_t* __restrict__ grp,
@@ -149,11 +149,11 @@ __global__ void __launch_bounds__(256) k_bucket_scatter(const uint16_t* __restri
 // group, a lane per column.
 __global__ void k_group_bounds(const float* __restrict__ c, const float* __restrict__ norms,
                                const uint32_t* __restrict__ perm, size_t ks, int d, const int* __restrict__ cbeg,
-                               const int* __restrict__ ntiles, int G, float2* __restrict__ gb) {
+                               const int* __restrict__ ntiles, int tile_cols, int G, float2* __restrict__ gb) {
     const int g = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
     if (g >= G) return;
     const size_t c0 = (size_t)cbeg[g];
-    size_t c1 = c0 + (size_t)ntiles[g] * 256;
+    size_t c1 = c0 + (size_t)ntiles[g] * tile_cols;
     if (c1 > ks) c1 = ks;
     float cm = 0.0f, nm = 0.0f;
     for (size_t j = c0 + lane; j < c1; j += 32) {
@@ -308,6 +308,31 @@ __global__ void k_gather_sorted(const float* __restrict__ c, const uint32_t* __r
 __global__ void k_pad_norms(float* __restrict__ norms, const uint32_t* __restrict__ perm, size_t ks) {
     const size_t j = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (j < ks && perm[j] == 0xffffffffu) norms[j] = 3.0e38f;
+}
+
+// Rows split into BF16 hi and lo (x = hi + lo to about 2^-16), [m][kpad] with
+// zeros past d: the grouped search gathers them with TMA. One thread per 8 elements.
+__global__ void k_rows_split(const float* __restrict__ x, size_t m, int d, int kpad, __nv_bfloat16* __restrict__ hi,
+                             __nv_bfloat16* __restrict__ lo) {
+    const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int nchunk = kpad / 8;
+    if (t >= m * nchunk) return;
+    const size_t r = t / nchunk;
+    const int k0 = (int)(t - r * nchunk) * 8;
+    const float* xr = x + r * (size_t)d;
+    uint32_t hw[4], lw[4];
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+        const float a = k0 + 2 * i < d ? xr[k0 + 2 * i] : 0.0f;
+        const float b = k0 + 2 * i + 1 < d ? xr[k0 + 2 * i + 1] : 0.0f;
+        const __nv_bfloat16 ha = __float2bfloat16_rn(a), hb = __float2bfloat16_rn(b);
+        const __nv_bfloat16 la = __float2bfloat16_rn(a - __bfloat162float(ha));
+        const __nv_bfloat16 lb = __float2bfloat16_rn(b - __bfloat162float(hb));
+        hw[i] = (uint32_t)__bfloat16_as_ushort(ha) | ((uint32_t)__bfloat16_as_ushort(hb) << 16);
+        lw[i] = (uint32_t)__bfloat16_as_ushort(la) | ((uint32_t)__bfloat16_as_ushort(lb) << 16);
+    }
+    *reinterpret_cast<uint4*>(hi + r * kpad + k0) = make_uint4(hw[0], hw[1], hw[2], hw[3]);
+    *reinterpret_cast<uint4*>(lo + r * kpad + k0) = make_uint4(lw[0], lw[1], lw[2], lw[3]);
 }
 
 // Strided sample of f32 rows (input statistics of the network).

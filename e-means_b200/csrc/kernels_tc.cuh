@@ -64,6 +64,8 @@ struct TcParams {
     const int* tile_group;
     const int* grp_cbeg;
     const int* grp_ntiles;
+    const __nv_bfloat16* rows_hi;  // grouped search: the chunk's rows split into BF16 hi / lo, [rows][kpad]
+    const __nv_bfloat16* rows_lo;
 };
 
 // ---- PTX wrappers -----------------------------------------------------------

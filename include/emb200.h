@@ -218,7 +218,7 @@ typedef struct {
 } emb200_proposer_config;
 
 /* Groups the current centroids, builds the group-sorted copy and initialises the
- * network (input standardisation from the resident rows when present). */
+ * network (input standardisation from the resident rows when present). d <= 128. */
 int emb200_proposer_init(emb200_handle* h, const emb200_proposer_config* cfg);
 /* Adam steps on mini-batches of resident rows with known labels (host array of
  * rows_n labels, e.g. train()'s output; UINT32_MAX rows are skipped): targets
