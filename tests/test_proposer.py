@@ -221,3 +221,26 @@ def test_low_confidence_rows_take_the_full_search(trained):
     assert 0 < st["rows_lowconf"] < x.shape[0]
     assert np.all(dist_p >= dist_f)
     a.proposer_set("mlp", TOP, 0.0)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("d", [96, 32])
+def test_grouped_search_with_a_half_k_atom(emb, orc, d):
+    # d = 96 and d = 32 leave a 32-wide K remainder: the grouped search covers it with
+    # a 64-byte-swizzled half atom; the guarantees must hold exactly as for d = 48.
+    x = emb.datasets.heavy_tailed(50_000, d, latent=12, components=256, seed=31)
+    a = emb.B200Assigner(0, precision="bf16x1")
+    out = emb.train(x, d, 1024, emb.Config(nepochs=2.0), assigner=a)
+    a.proposer_init(groups=128, hidden=256, top=8, seed=3)
+    a.proposer_train(out.labels, 300)
+    lab_p, dist_p = a.assign_proposed()
+    lab_f, dist_f = a.assign_resident()
+    props, _ = a.propose(x)
+    gof = a.proposer_groups()
+    covered = np.array([gof[l] in row for l, row in zip(lab_f, props)])
+    same = lab_p == lab_f
+    assert np.all(same[covered])
+    assert np.array_equal(dist_p[same].view(np.uint32), dist_f[same].view(np.uint32))
+    assert np.all(dist_p >= dist_f)
+    assert same.mean() > 0.9, same.mean()
+    a.close()
