@@ -66,12 +66,14 @@ __global__ void __launch_bounds__(256) k_bucket_count(const uint16_t* __restrict
 }
 
 // One block: group g's bucket starts at the sum of the earlier groups' counts,
-// each rounded up to whole tiles; tile_group maps every bucket tile to its group
-// (-1 past the last), cursor[g] starts at the bucket's first position.
+// each rounded up to whole tiles; tile_info gives every bucket tile its group's
+// (first column, column tiles) ((0, 0) past the last), cursor[g] starts at the
+// bucket's first position.
 __global__ void k_bucket_layout(const uint32_t* __restrict__ counts, int G, int ntile_max,
-                                uint32_t* __restrict__ cursor, int* __restrict__ tile_group) {
+                                const int* __restrict__ cbeg, const int* __restrict__ ntiles,
+                                uint32_t* __restrict__ cursor, int2* __restrict__ tile_info) {
     __shared__ uint32_t start[1025];
-    for (int t = threadIdx.x; t < ntile_max; t += blockDim.x) tile_group[t] = -1;
+    for (int t = threadIdx.x; t < ntile_max; t += blockDim.x) tile_info[t] = make_int2(0, 0);
     if (threadIdx.x == 0) {
         uint32_t acc = 0;
         for (int g = 0; g < G; g++) {
@@ -83,7 +85,8 @@ __global__ void k_bucket_layout(const uint32_t* __restrict__ counts, int G, int 
     __syncthreads();
     for (int g = threadIdx.x; g < G; g += blockDim.x) {
         cursor[g] = start[g];
-        for (uint32_t t = start[g] / kBucketTile; t < start[g + 1] / kBucketTile; t++) tile_group[t] = g;
+        const int2 v = make_int2(cbeg[g], ntiles[g]);
+        for (uint32_t t = start[g] / kBucketTile; t < start[g + 1] / kBucketTile; t++) tile_info[t] = v;
     }
 }
 

@@ -58,12 +58,10 @@ struct TcParams {
     int cand_cap;
     const uint32_t* m_dev;    // COLLECT: if set, the row count is min(m, *m_dev), read on the device
     // Grouped search (k_assign_grouped, centroid groups of a group-sorted matrix):
-    // bucket tile t scores only group tile_group[t] (-1: past the last tile),
-    // columns [grp_cbeg[g], + 256 grp_ntiles[g]). Column starts are multiples of
-    // 32, so packed keys and the norms copy stay aligned.
-    const int* tile_group;
-    const int* grp_cbeg;
-    const int* grp_ntiles;
+    // bucket tile t scores columns [tile_info[t].x, + 128 tile_info[t].y) of its
+    // group (y = 0: past the last tile). Column starts are multiples of 32, so
+    // packed keys and the norms copy stay aligned.
+    const int2* tile_info;
     const __nv_bfloat16* rows_hi;  // grouped search: the chunk's rows split into BF16 hi / lo, [rows][kpad]
     const __nv_bfloat16* rows_lo;
 };

@@ -93,15 +93,16 @@ k_assign_grouped(const __grid_constant__ CUtensorMap map_hi, const __grid_consta
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int nwt = p.m / kTcBM;  // bucket tiles in the launch (m is a whole number of tiles)
-    // Bucket tile of this CTA's i-th work item and its group (false past the last one).
-    auto work = [&](int i, int& w, int& g) -> bool {
-        w = (int)blockIdx.x + i * (int)gridDim.x;
-        if (w >= nwt) return false;
-        g = p.tile_group[w];
-        return g >= 0;
+    // Work item i of this CTA is bucket tile blockIdx.x + i * gridDim.x; its (first
+    // column, column tiles), no tiles past the last bucket tile. Every role loads
+    // the next item's record while it works on the current one.
+    auto info = [&](int i) -> int2 {
+        const int w = (int)blockIdx.x + i * (int)gridDim.x;
+        return w < nwt ? p.tile_info[w] : make_int2(0, 0);
     };
-    int w0, g0;
-    if (!work(0, w0, g0)) return;  // no work: the whole CTA leaves before any setup
+    const int2 info0 = info(0);
+    if (info0.y <= 0) return;  // no work: the whole CTA leaves before any setup
+    const int w0 = (int)blockIdx.x;
     const int natoms = p.kpad / 64;
 
     if (threadIdx.x == 0) {
@@ -130,10 +131,12 @@ k_assign_grouped(const __grid_constant__ CUtensorMap map_hi, const __grid_consta
     if (warp == 0) {
         if (lane == 0) {
             // ---- TMA producer of the centroid stages
-            int u = 0, tg = 0, norms_issued = 0, w, g;
+            int u = 0, tg = 0, norms_issued = 0;
             bool ok = true;
-            for (int i = 0; ok && work(i, w, g); i++) {
-                const int nt = p.grp_ntiles[g], c0 = p.grp_cbeg[g];
+            int2 cur = info0;
+            for (int i = 0; ok && cur.y > 0; i++) {
+                const int2 nxt = info(i + 1);
+                const int nt = cur.y, c0 = cur.x;
                 for (int t = 0; ok && t < nt; t++, tg++) {
                     const int col = c0 + t * kGrpBN;
                     for (int a = 0; a < natoms; a++, u++) {
@@ -155,6 +158,7 @@ k_assign_grouped(const __grid_constant__ CUtensorMap map_hi, const __grid_consta
                         }
                     }
                 }
+                cur = nxt;
             }
             // After an abort, let the copies still in flight land before the CTA exits.
             if (*abort_flag) {
@@ -176,15 +180,17 @@ k_assign_grouped(const __grid_constant__ CUtensorMap map_hi, const __grid_consta
             // ---- MMA issuer
             const uint32_t idesc = idesc_bf16(kTcBM, kGrpBN);
             const uint32_t a_atom = (kTcBM * 128) >> 4;  // descriptor units per A atom
-            int u = 0, tg = 0, w, g;
+            int u = 0, tg = 0;
             bool ok = true;
-            for (int i = 0; ok && work(i, w, g); i++) {
+            int2 cur = info0;
+            for (int i = 0; ok && cur.y > 0; i++) {
+                const int2 nxt = info(i + 1);
                 const int ab = i & 1;
                 if (!mbar_wait(&a_full[ab], (uint32_t)(i >> 1) & 1u, abort_flag)) break;
                 tc_fence_after();
                 const uint64_t a_hi0 = sw128_desc(smem_u32(smem + ab * L.a_buf));
                 const uint64_t a_lo0 = sw128_desc(smem_u32(smem + ab * L.a_buf + L.a_lo));
-                const int nt = p.grp_ntiles[g];
+                const int nt = cur.y;
                 for (int t = 0; ok && t < nt; t++, tg++) {
                     const int b = tg % kGrpAcc;
                     const uint32_t bph = (uint32_t)(tg / kGrpAcc) & 1u;
@@ -224,17 +230,20 @@ k_assign_grouped(const __grid_constant__ CUtensorMap map_hi, const __grid_consta
                     if (ok) mma_commit(&acc_full[b]);
                 }
                 if (ok) mma_commit(&a_empty[ab]);  // the row buffer is free once these MMAs complete
+                cur = nxt;
             }
         }
     } else if (warp == kGrpRowWarp) {
         // ---- row gatherer: lane l gathers rows 4l .. 4l + 3 of every bucket tile
         const int a_terms = p.nterms == 3 ? 2 : 1;
         const uint32_t bytes = (uint32_t)kTcBM * 128u * (uint32_t)natoms * (uint32_t)a_terms;
-        int w, g, issued = 0;
+        int issued = 0;
         bool ok = true;
         uint32_t idx[4];
         for (int j = 0; j < 4; j++) idx[j] = p.gather[(size_t)w0 * kTcBM + lane * 4 + j];
-        for (int i = 0; ok && work(i, w, g); i++) {
+        int2 cur = info0;
+        for (int i = 0; ok && cur.y > 0; i++) {
+            const int2 nxt = info(i + 1);
             const int ab = i & 1;
             if (i >= 2) {
                 // tile i - 2 used this buffer: its MMAs must have completed
@@ -254,8 +263,9 @@ k_assign_grouped(const __grid_constant__ CUtensorMap map_hi, const __grid_consta
                                 (int)idx[2], (int)idx[3]);
             }
             issued = i + 1;
-            int wn, gn;
-            if (work(i + 1, wn, gn)) {
+            cur = nxt;
+            if (nxt.y > 0) {
+                const int wn = (int)blockIdx.x + (i + 1) * (int)gridDim.x;
                 // the next tile's rows: indices now, their lines into L2 while this tile computes
                 for (int j = 0; j < 4; j++) idx[j] = p.gather[(size_t)wn * kTcBM + lane * 4 + j];
                 const int row_bytes = p.kpad * 2;
@@ -280,13 +290,15 @@ k_assign_grouped(const __grid_constant__ CUtensorMap map_hi, const __grid_consta
         const int cq = (warp - 2) >> 2;
         const int r = q * 32 + lane;
         uint32_t* mg = (uint32_t*)(smem + L.merge);
-        int tg = 0, w, g;
+        int tg = 0;
         bool ok = true;
+        int2 cur = info0;
         // After an abort every epilogue warp still walks all work items and reaches
         // every named barrier, skipping the waits and the work.
-        for (int i = 0; work(i, w, g); i++) {
-            const int nt = p.grp_ntiles[g], c0 = p.grp_cbeg[g];
-            const int row = w * kTcBM + r;
+        for (int i = 0; cur.y > 0; i++) {
+            const int2 nxt = info(i + 1);
+            const int nt = cur.y, c0 = cur.x;
+            const int row = ((int)blockIdx.x + i * (int)gridDim.x) * kTcBM + r;
             Top2 top;
             top.init();
             for (int t = 0; t < nt; t++, tg++) {
@@ -338,6 +350,7 @@ k_assign_grouped(const __grid_constant__ CUtensorMap map_hi, const __grid_consta
             }
             // The next work item's chunk records overwrite these.
             asm volatile("bar.sync 1, %0;" ::"n"(kTcEpiWarps * 32) : "memory");
+            cur = nxt;
         }
     }
     tc_fence_before();
