@@ -485,6 +485,23 @@ def run_c5(args):
             ms.append(st["ms_total"])
         return float(np.mean(ms)), st
 
+    if args.profile_proposer:
+        # Profiling captures: one proposer assign (first setting) between
+        # cudaProfilerStart/Stop, for ncu --profile-from-start off.
+        import torch
+
+        top, conf, mass = (float(v) for v in args.proposer_configs.split(",")[0].split(":"))
+        a.proposer_set("mlp", int(top), conf, mass)
+        a.assign_proposed(want_host=False)
+        torch.cuda.synchronize()
+        torch.cuda.profiler.start()
+        a.assign_proposed(want_host=False)
+        torch.cuda.synchronize()
+        torch.cuda.profiler.stop()
+        print(json.dumps({"profiled": "one proposer assign", "rows": n, "stats": a.stats()}), flush=True)
+        a.close()
+        return
+
     configs = [tuple(float(v) for v in c.split(":")) for c in args.proposer_configs.split(",")]
     sampler = ClockSampler(0)
     runs = []
@@ -619,6 +636,8 @@ def main():
     ap.add_argument("--proposer-configs", default="32:0:0.999,32:0:0.9999,16:0:0.99,8:0:0",
                     help="c5: top:confidence:mass settings of the proposer assign; the first is the headline")
     ap.add_argument("--c5-rows", type=int, default=10_000_000, help="c5: rows of the workload")
+    ap.add_argument("--profile-proposer", action="store_true",
+                    help="c5: run one proposer assign between cudaProfilerStart/Stop and exit (profiling captures)")
     args = ap.parse_args()
     set_rows(args.rows)
     if args.workload == "c1" and args.impl == "ours":

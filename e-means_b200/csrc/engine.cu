@@ -320,8 +320,18 @@ int launch_i8_assign(emb200_handle* h, const int8_t* x, const uint32_t* gather, 
     const int ntiles = tc ? (k + kTcBN - 1) / kTcBN : (k + kI8BN - 1) / kI8BN;
     if (row_tiles < target) nsplit = std::min(ntiles, (target + row_tiles - 1) / row_tiles);
     nsplit = std::max(nsplit, 1);
+    // As in assign_rows_dev: in the training loop, size the split partials for every
+    // batch of up to m rows (a smaller batch may use more splits).
+    size_t part_rows = (size_t)nsplit * m;
+    if (graph) {
+        for (size_t rt = 1; rt * 128 < m + 128; rt++) {
+            const size_t mm = std::min(rt * 128, m);
+            const int ns = (int)rt < target ? std::max(1, std::min(ntiles, (target + (int)rt - 1) / (int)rt)) : 1;
+            part_rows = std::max(part_rows, (size_t)ns * mm);
+        }
+    }
     // part_s holds int64 scores here: 2 floats per entry.
-    if (h->part_s.ensure((size_t)nsplit * m * 2) || h->part_i.ensure((size_t)nsplit * m) || h->counters.ensure(8))
+    if (h->part_s.ensure(part_rows * 2) || h->part_i.ensure(part_rows) || h->counters.ensure(8))
         return fail(h, EMB200_ENOMEM, "scratch allocation failed for %zu rows", m);
     if (!graph) CK(cudaEventRecord(h->evk0, st));
     if (tc) {
@@ -491,8 +501,25 @@ int assign_rows_dev(emb200_handle* h, const T* x, const uint32_t* gather, size_t
         int target = 2 * h->sm_count;
         if (row_tiles < target) nsplit = std::min(ntiles, (target + row_tiles - 1) / row_tiles);
     }
-    if (h->part_s.ensure((size_t)nsplit * m * 2) || h->part_i.ensure((size_t)nsplit * m * 2) ||
-        h->redo_rows.ensure(m) || h->redo_theta.ensure(m) || h->counters.ensure(8))
+    // Inside the training loop (graph = true) nothing may allocate while an epoch is
+    // captured, and a smaller batch can need more split partials than a full one
+    // (fewer row tiles, more splits): size them for every batch of up to m rows.
+    size_t part_rows = (size_t)nsplit * m;
+    if (graph) {
+        for (size_t rt = 1; rt * kTcBM < m + kTcBM; rt++) {
+            const size_t mm = std::min(rt * kTcBM, m);
+            int ns = 1;
+            if (tc) {
+                ns = tc_nsplit(h, mm);
+            } else {
+                const int rtiles = (int)((mm + kSimtBM - 1) / kSimtBM), target = 2 * h->sm_count;
+                if (rtiles < target) ns = std::min(ntiles, (target + rtiles - 1) / rtiles);
+            }
+            part_rows = std::max(part_rows, (size_t)ns * mm);
+        }
+    }
+    if (h->part_s.ensure(part_rows * 2) || h->part_i.ensure(part_rows * 2) || h->redo_rows.ensure(m) ||
+        h->redo_theta.ensure(m) || h->counters.ensure(8))
         return fail(h, EMB200_ENOMEM, "scratch allocation failed for %zu rows", m);
     uint32_t* ctr = h->counters.p;
     CK(cudaMemsetAsync(ctr, 0, 8 * sizeof(uint32_t), st));

@@ -171,3 +171,18 @@ def test_batched_instances_equal_single_runs(emb, orc):
         assert outs[i].n_splits == single.n_splits
     ref = orc.train(parts[4], ks[4], orc.make_config(nepochs=3.0), emulate=not orc.has_kernel("avx512"))
     check_same(outs[4], ref)
+
+
+def test_graph_epoch_with_a_short_last_batch(emb):
+    # Full batches of 19,200 rows (150 row tiles: one centroid split) and a last
+    # batch of 18,000 (141 tiles: two splits, more partials than a full batch):
+    # the captured epoch must not need a buffer the dry run did not size.
+    x = emb.datasets.blobs(19_200 * 16 + 18_000, 16, n_blobs=600, seed=16)
+    outs = []
+    for eager in (False, True):
+        a = emb.B200Assigner(0, precision="bf16", train_eager=eager)
+        outs.append(emb.train(x, 16, 512, emb.Config(nepochs=1.0, batch_size=19_200), assigner=a))
+        a.close()
+    assert outs[0].recipe.batch_size == 19_200
+    assert np.array_equal(outs[0].labels, outs[1].labels)
+    assert same_f32(outs[0].centroids, outs[1].centroids)
