@@ -639,7 +639,8 @@ int settle_rows(emb200_handle* h, const T* x, const uint32_t* gather, size_t m, 
         exhaustive = h->redo2_rows.p;
         exhaustive_count = ctr + 3;
     }
-    const int rc = launch_research(h, x, gather, m, exhaustive, exhaustive_count, labels, dist, st);
+    // at most nredo rows reach the exhaustive list: grids sized by it, not by m
+    const int rc = launch_research(h, x, gather, nredo, exhaustive, exhaustive_count, labels, dist, st);
     if (rc) return rc;
     return finish_counters(h, st, exhaustive_count == ctr + 3);
 }
