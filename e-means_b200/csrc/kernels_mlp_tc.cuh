@@ -64,6 +64,20 @@ __host__ __device__ inline MlpTcSmem mlp_tc_smem(int kin, int H, int topc) {
 // Each epilogue thread keeps the TOPC best of its 64 (or 32) columns; the merge
 // of the four quarters' lists gives the exact top TOPC, and for top up to 4 TOPC
 // the best of what the lists hold.
+// relu(a + ba), relu(b + bb) rounded to BF16 and packed (low half: a): the two
+// f32 additions in one packed FMA with multiplier 1 (each rounded once, as a
+// plain add), then ReLU, rounding and packing in one conversion.
+EMB_DEV uint32_t bias_relu_bf16x2(float a, float b, float ba, float bb) {
+    float sa, sb;
+    asm("{\n .reg .b64 ra, rb, rc, rd;\n mov.b64 ra, {%2, %3};\n mov.b64 rb, {%4, %5};\n mov.b64 rc, {%6, %7};\n"
+        " fma.rn.f32x2 rd, ra, rb, rc;\n mov.b64 {%0, %1}, rd;\n}\n"
+        : "=f"(sa), "=f"(sb)
+        : "f"(a), "f"(b), "f"(1.0f), "f"(1.0f), "f"(ba), "f"(bb));
+    uint32_t r;
+    asm("cvt.rn.relu.bf16x2.f32 %0, %1, %2;" : "=r"(r) : "f"(sb), "f"(sa));  // first operand -> upper half
+    return r;
+}
+
 // Insert (v, j) into a descending list of length N (ties keep the earlier column first).
 template <int N>
 EMB_DEV void topn_insert(float (&val)[N], int (&idx)[N], float v, int j) {
@@ -226,12 +240,20 @@ k_mlp_tc(const __grid_constant__ CUtensorMap map_w1, const __grid_constant__ CUt
                 float v[8];
 #pragma unroll
                 for (int i = 0; i < 8; i++) v[i] = 0.0f;
-                if (g < p.m) {
+                if (g < p.m && k0 < p.d) {
+                    // d is a multiple of 8 (fused-pass condition): whole 8-element chunks
                     const size_t src = p.rows ? (size_t)p.rows[g] : (size_t)g;
-                    const float* xr = p.x + src * (size_t)p.d;
+                    const float4* xr = reinterpret_cast<const float4*>(p.x + src * (size_t)p.d + k0);
+                    const float4* mr = reinterpret_cast<const float4*>(p.mean + k0);
+                    const float4* sr = reinterpret_cast<const float4*>(p.istd + k0);
 #pragma unroll
-                    for (int i = 0; i < 8; i++)
-                        if (k0 + i < p.d) v[i] = (xr[k0 + i] - p.mean[k0 + i]) * p.istd[k0 + i];
+                    for (int h = 0; h < 2; h++) {
+                        const float4 xv = xr[h], mv = __ldg(mr + h), sv = __ldg(sr + h);
+                        v[4 * h + 0] = (xv.x - mv.x) * sv.x;
+                        v[4 * h + 1] = (xv.y - mv.y) * sv.y;
+                        v[4 * h + 2] = (xv.z - mv.z) * sv.z;
+                        v[4 * h + 3] = (xv.w - mv.w) * sv.w;
+                    }
                 }
                 uint32_t w[4];
 #pragma unroll
@@ -260,14 +282,14 @@ k_mlp_tc(const __grid_constant__ CUtensorMap map_w1, const __grid_constant__ CUt
                     tc_regs_ready(v);
 #pragma unroll
                     for (int j = 0; j < 32; j += 8) {
+                        const float4 b0 = __ldg(reinterpret_cast<const float4*>(bias + c0 + j));
+                        const float4 b1 = __ldg(reinterpret_cast<const float4*>(bias + c0 + j + 4));
+                        const float bb[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
                         uint32_t w[4];
 #pragma unroll
-                        for (int i = 0; i < 4; i++) {
-                            const float a = fmaxf(__uint_as_float(v[j + 2 * i]) + bias[c0 + j + 2 * i], 0.0f);
-                            const float b = fmaxf(__uint_as_float(v[j + 2 * i + 1]) + bias[c0 + j + 2 * i + 1], 0.0f);
-                            w[i] = (uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(a)) |
-                                   ((uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(b)) << 16);
-                        }
+                        for (int i = 0; i < 4; i++)
+                            w[i] = bias_relu_bf16x2(__uint_as_float(v[j + 2 * i]), __uint_as_float(v[j + 2 * i + 1]),
+                                                    bb[2 * i], bb[2 * i + 1]);
                         *reinterpret_cast<uint4*>(act + sw128_offset(r, (c0 + j) >> 3, kTcBM)) =
                             make_uint4(w[0], w[1], w[2], w[3]);
                     }
