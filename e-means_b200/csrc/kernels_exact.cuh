@@ -527,62 +527,5 @@ __global__ void k_research_finish(const T* __restrict__ x, const uint32_t* __res
     }
 }
 
-// Exact re-search (src/cpu.rs:108-167 semantics) of the rows in redo_rows:
-// every centroid scored in the reference rounding, strict < in ascending j
-// (lowest index on ties), best starts at +inf with label 0; dist =
-// max(best + sqnorm(x), 0). One warp per row; the warp's groups take
-// interleaved centroids. Persistent grid: warps stride over the list.
-template <typename T>
-__global__ void k_research(const T* __restrict__ x, const uint32_t* __restrict__ gather, int d,
-                           const float* __restrict__ c, const float* __restrict__ norms, int k, int match,
-                           const uint32_t* __restrict__ redo_rows, const uint32_t* __restrict__ redo_count,
-                           uint32_t* __restrict__ labels, float* __restrict__ dist) {
-    int lane = threadIdx.x & 31;
-    int gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    int nwarps = (gridDim.x * blockDim.x) >> 5;
-    uint32_t count = *redo_count;
-    int gsz = match == kMatchAvx512 ? 16 : 8;
-    int ngroups = 32 / gsz;
-    int g = lane / gsz;
-    for (uint32_t r = gwarp; r < count; r += nwarps) {
-        uint32_t row = redo_rows[r];
-        size_t src = gather ? gather[row] : (size_t)row;
-        const T* xr = x + src * (size_t)d;
-        float best = __int_as_float(0x7f800000);
-        uint32_t lab = 0;
-        bool any = false;  // whether this group scored at least one centroid
-        for (int j0 = 0; j0 < k; j0 += ngroups) {
-            int j = j0 + g;
-            int jc = j < k ? j : k - 1;
-            float dg = group_dot_ref(match, xr, c + (size_t)jc * d, d, lane);
-            if (j < k) {
-                float s = score_ref(norms[j], dg);
-                if (s < best) {
-                    best = s;
-                    lab = (uint32_t)j;
-                }
-                any = true;
-            }
-        }
-        // Merge the groups in (score, index) order; a group that never beat +inf
-        // keeps label 0 like the reference (its candidate loses to any finite one).
-        float rb = best;
-        uint32_t rl = lab;
-        for (int q = 1; q < ngroups; q++) {
-            float ob = __shfl_sync(kFull, best, q * gsz);
-            uint32_t ol = __shfl_sync(kFull, lab, q * gsz);
-            if (lex_less(ob, ol, rb, rl) && ob < __int_as_float(0x7f800000)) {
-                rb = ob;
-                rl = ol;
-            }
-        }
-        (void)any;
-        float xn = warp_sqnorm_ref(xr, d, lane);
-        if (lane == 0) {
-            labels[row] = rl;
-            dist[row] = fmaxf(__fadd_rn(rb, xn), 0.0f);
-        }
-    }
-}
 
 }  // namespace emb
