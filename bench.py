@@ -336,18 +336,37 @@ def run_c1(args):
 
 
 def run_c3(args):
-    """int8 codes: 2,000,000 x 512 unit-norm rows quantised with the faiss
-    calibration, k = 4096 centroids trained by the engine (int8-centroid search,
-    2 epochs, untimed); one exact assign() pass with CpuI8Assigner(I8) semantics on
-    the tcgen05 kind::i8 kernel, rows resident."""
+    """int8 codes: 2,000,000 x 512 unit-norm f32 rows made resident, then
+    quantised on the device (Int8Quantizer fit + encode, faiss calibration); k =
+    4096 centroids trained by the engine (int8-centroid search, 2 epochs, untimed);
+    one exact assign() pass with CpuI8Assigner(I8) semantics on the tcgen05
+    kind::i8 kernel, rows resident."""
     from __graft_entry__ import load_package
     from oracle import oracle as orc
 
     emb = load_package()
     n = args.rows if args.rows != N_ROWS else 2_000_000
-    codes, _, _ = emb.datasets.embeddings_int8(n, 512, latent=64, seed=0)
+    x = emb.datasets.embeddings(n, 512, latent=64, seed=0)
     a = emb.B200Assigner(0, precision="fp32", centroid_bits=8)
-    a.load_rows(codes)
+    # f32 rows resident, then Int8Quantizer::fit and encode on the device (faiss calibration)
+    a.load_rows(x)
+    t0 = time.perf_counter()
+    q = emb.Int8Quantizer.fit_resident(a, emb.Calibration.faiss())
+    t1 = time.perf_counter()
+    st_fit = a.stats()
+    clipped = q.quantize_resident(a)
+    t2 = time.perf_counter()
+    st_enc = a.stats()
+    enc_ms = st_enc["ms_total"]
+    quant = {"fit_ms": st_fit["ms_total"], "fit_peak_ms": st_fit["fast_ms"], "encode_ms": enc_ms,
+             "fit_wall_ms": (t1 - t0) * 1e3, "encode_wall_ms": (t2 - t1) * 1e3,
+             "scale": float(q.scale), "clipped_fraction": clipped / x.size,
+             "encode_gbs": x.size * 5 / (enc_ms / 1e3) / 1e9,
+             "encode_frac_of_measured_hbm": x.size * 5 / (enc_ms / 1e3) / 1e9 / measured_peaks()["hbm_gbs"],
+             "note": "CUDA-event times of the kernels on resident f32 rows: fit = f64 column sums in row order "
+                     "(a chain of n dependent adds per dimension) + max |x - shift| (fit_peak_ms); encode = one "
+                     "pass reading f32 and writing i8 (5 B per value). Wall times include allocation of the "
+                     "codes and release of the f32 rows"}
     out = a.train_resident(4096, emb.Config(nepochs=2.0))
     for _ in range(args.warmup):
         a.assign_resident(want_host=False)
@@ -365,12 +384,19 @@ def run_c3(args):
             "config": {"workload": f"{n} x 512 int8 codes (faiss calibration of 64-d-latent unit rows), k=4096",
                        "fast_kernel": st["fast_kernel"]},
             "roofline": {"bound": "tensor (int8)", "achieved_tops": ops / (fast / args.steps / 1e3) / 1e12,
-                         "note": "int8 dense peak not measured by the pool; nominal 4500 TOPS"}}
+                         "note": "int8 dense peak not measured by the pool; nominal 4500 TOPS"},
+            "quantizer": quant}
     if not args.no_cpu:
         sample = min(8192, n)
         cores = os.cpu_count() or 1
+        codes = q.encode(x[:sample], assigner=a)
+        qs = min(262_144, n)
         t0 = time.perf_counter()
-        orc.i8_assign(codes[:sample], out.centroids, bits=8, nthreads=cores)
+        orc.quantizer_encode(x[:qs], *orc.quantizer_fit(x[:qs]))
+        quant["cpu_fit_encode_ms_per_1M_rows"] = (time.perf_counter() - t0) * 1e3 * 1e6 / qs
+        quant["cpu_sample"] = f"Int8Quantizer fit + encode restated in C++ (one thread) on the first {qs} rows"
+        t0 = time.perf_counter()
+        orc.i8_assign(codes, out.centroids, bits=8, nthreads=cores)
         tc = time.perf_counter() - t0
         line["cpu_baseline"] = {"value": sample / tc, "unit": "rows/s", "cores": cores, "kind": "port",
                                 "sample": f"first {sample} rows: CpuI8Assigner(I8) restated in C++ (portable "

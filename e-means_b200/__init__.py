@@ -68,6 +68,10 @@ class _ProposerConfig(ctypes.Structure):
 PROPOSER_MODES = {"mlp": 0, "centroids": 1}
 
 
+class _Calibration(ctypes.Structure):
+    _fields_ = [("target_peak", ctypes.c_float), ("power_of_two", ctypes.c_int32), ("quantile", ctypes.c_double)]
+
+
 def build(force=False):
     """Compile libemb200.so in-tree with nvcc for sm_100a."""
     args = ["make", "-s", "-C", _HERE] + (["-B"] if force else [])
@@ -118,6 +122,14 @@ def lib():
     L.emb200_propose.argtypes = [P, P, S, P, P, P]
     L.emb200_assign_proposed_resident.argtypes = [P, P, P]
     L.emb200_assign_proposed_device.argtypes = [P, P, S, P, P, P]
+    C = ctypes.POINTER(_Calibration)
+    L.emb200_quantizer_fit.argtypes = [P, P, S, S, C, P, P]
+    L.emb200_quantizer_fit_device.argtypes = [P, P, S, S, C, P, P]
+    L.emb200_quantizer_fit_resident.argtypes = [P, C, P, P]
+    L.emb200_quantizer_encode.argtypes = [P, P, S, S, P, ctypes.c_float, P, P]
+    L.emb200_quantizer_encode_device.argtypes = [P, P, S, S, P, ctypes.c_float, P, P, P]
+    L.emb200_quantize_resident.argtypes = [P, P, ctypes.c_float, P]
+    L.emb200_quantizer_decode.argtypes = [P, P, S, S, P, ctypes.c_float, P]
     _lib = L
     return L
 
@@ -448,3 +460,122 @@ def assign(x, centroids, d, assigner: B200Assigner):
     c = np.ascontiguousarray(centroids, np.float32).reshape(-1, d)
     assigner.set_centroids(c)
     return assigner.assign(x)
+
+
+# ---- int8 quantizer (src/quantize.rs) ---------------------------------------
+
+@dataclass
+class Calibration:
+    """src/quantize.rs:17-34."""
+
+    target_peak: float
+    quantile: float
+    power_of_two: bool
+
+    @staticmethod
+    def faiss():
+        return Calibration(112.0, 1.0, True)
+
+    @staticmethod
+    def clipped(quantile):
+        return Calibration(127.0, quantile, False)
+
+    def _c(self):
+        return _Calibration(self.target_peak, int(bool(self.power_of_two)), self.quantile)
+
+
+_quant_handle = None
+
+
+def _quantizer_assigner(assigner):
+    """The handle whose GPU runs a quantizer call: the given assigner, else one
+    module-wide handle on device 0."""
+    global _quant_handle
+    if assigner is not None:
+        return assigner
+    if _quant_handle is None:
+        _quant_handle = B200Assigner(0)
+    return _quant_handle
+
+
+class Int8Quantizer:
+    """Int8Quantizer (src/quantize.rs:36-96): one per-dimension shift and one
+    global scale; fit, encode and clipped_fraction run on the B200."""
+
+    def __init__(self, d, shift, scale):
+        self.d = int(d)
+        self.shift = np.ascontiguousarray(shift, np.float32)
+        self.scale = np.float32(scale)
+
+    @classmethod
+    def fit(cls, sample, d, cal: Calibration, assigner: Optional[B200Assigner] = None):
+        """Int8Quantizer::fit (src/quantize.rs:45-62) on a host sample."""
+        x = np.ascontiguousarray(sample, np.float32).reshape(-1)
+        n = x.size // d
+        if n == 0 or x.size != n * d:
+            raise ValueError("the sample must hold n > 0 whole rows of d values")
+        a = _quantizer_assigner(assigner)
+        shift = np.empty(d, np.float32)
+        scale = ctypes.c_float()
+        c = cal._c()
+        a._check(lib().emb200_quantizer_fit(a._h, _p(x), n, d, ctypes.byref(c), _p(shift), ctypes.byref(scale)))
+        return cls(d, shift, scale.value)
+
+    @classmethod
+    def fit_resident(cls, assigner: B200Assigner, cal: Calibration):
+        """fit on the assigner's resident f32 rows (no host copy)."""
+        n, d = assigner.rows_shape
+        shift = np.empty(d, np.float32)
+        scale = ctypes.c_float()
+        c = cal._c()
+        assigner._check(lib().emb200_quantizer_fit_resident(assigner._h, ctypes.byref(c), _p(shift),
+                                                            ctypes.byref(scale)))
+        return cls(d, shift, scale.value)
+
+    def _encode(self, x, codes, assigner):
+        x = np.ascontiguousarray(x, np.float32).reshape(-1)
+        if x.size % self.d:
+            raise ValueError("rows must hold whole rows of d values")
+        a = _quantizer_assigner(assigner)
+        clipped = ctypes.c_uint64()
+        a._check(lib().emb200_quantizer_encode(a._h, _p(x), x.size // self.d, self.d, _p(self.shift),
+                                               float(self.scale), _p(codes), ctypes.byref(clipped)))
+        return clipped.value, x.size
+
+    def encode(self, x, assigner: Optional[B200Assigner] = None):
+        """Int8Quantizer::encode (src/quantize.rs:65-73): codes with x's shape."""
+        x = np.asarray(x, np.float32)
+        codes = np.empty(x.size, np.int8)
+        self._encode(x, codes, assigner)
+        return codes.reshape(x.shape)
+
+    def clipped_fraction(self, x, assigner: Optional[B200Assigner] = None):
+        """Int8Quantizer::clipped_fraction (src/quantize.rs:87-95)."""
+        clipped, size = self._encode(x, None, assigner)
+        return clipped / size
+
+    def decode(self, codes, assigner: Optional[B200Assigner] = None):
+        """Int8Quantizer::decode (src/quantize.rs:76-79): codes (any numeric array,
+        as f32) back to the original units."""
+        c = np.ascontiguousarray(codes, np.float32)
+        flat = c.reshape(-1)
+        if flat.size % self.d:
+            raise ValueError("codes must hold whole rows of d values")
+        out = np.empty(flat.size, np.float32)
+        a = _quantizer_assigner(assigner)
+        a._check(lib().emb200_quantizer_decode(a._h, _p(flat), flat.size // self.d, self.d, _p(self.shift),
+                                               float(self.scale), _p(out)))
+        return out.reshape(c.shape)
+
+    def decode_sqdist(self, sqdist):
+        """src/quantize.rs:82-84 (a scalar or array of f32 squared distances)."""
+        s = np.float32(self.scale)
+        return (np.asarray(sqdist, np.float32) / (s * s)).astype(np.float32)
+
+    def quantize_resident(self, assigner: B200Assigner):
+        """Replace the assigner's resident f32 rows by their codes (resident i8
+        rows); returns the number of values that clipped."""
+        clipped = ctypes.c_uint64()
+        assigner._check(lib().emb200_quantize_resident(assigner._h, _p(self.shift), float(self.scale),
+                                                       ctypes.byref(clipped)))
+        return clipped.value

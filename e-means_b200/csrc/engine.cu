@@ -28,6 +28,7 @@
 #include "kernels_mlp.cuh"
 #include "kernels_mlp_tc.cuh"
 #include "kernels_proposer.cuh"
+#include "kernels_quant.cuh"
 
 constexpr int kRefineCap = 32;  // candidates kept per refined row
 
@@ -138,6 +139,12 @@ struct emb200_handle {
     // learned proposer (emb200_proposer_*), and a counter of centroid changes it tracks
     Proposer* prop = nullptr;
     uint64_t centroid_version = 0;
+
+    // int8 quantizer scratch (emb200_quantizer_*)
+    DevBuf<float> qshift;
+    DevBuf<QuantSelect> qsel;
+    DevBuf<unsigned long long> qclip;
+    DevBuf<uint8_t> qx, qcodes;
 };
 
 namespace {
@@ -766,6 +773,7 @@ int emb200_destroy(emb200_handle* h) {
     h->part_s.release(); h->part_i.release(); h->redo_rows.release(); h->counters.release();
     h->redo_theta.release(); h->cand.release(); h->cand_count.release(); h->redo2_rows.release();
     h->rkeys.release();
+    h->qshift.release(); h->qsel.release(); h->qclip.release(); h->qx.release(); h->qcodes.release();
     h->train.release();
     proposer_release(h);
     if (h->ev0) cudaEventDestroy(h->ev0);
@@ -1030,3 +1038,4 @@ extern "C" int emb200_assign_f32_noalloc(const float* x_dev, size_t m, size_t d,
 
 #include "engine_train.inc"
 #include "engine_proposer.inc"
+#include "engine_quant.inc"

@@ -252,6 +252,49 @@ int emb200_assign_proposed_resident(emb200_handle* h, uint32_t* labels, float* d
 int emb200_assign_proposed_device(emb200_handle* h, const float* x_dev, size_t m, uint32_t* labels_dev,
                                   float* dist_dev, void* stream);
 
+/* ---- int8 quantizer (src/quantize.rs) ------------------------------------
+ *
+ * Int8Quantizer on the GPU, bit-exact with the reference: shift = per-dimension
+ * mean (f64 sums in row order, then f32), peak = the centred magnitude
+ * |x - shift| at rank round((n d - 1) quantile) in f32::total_cmp order, scale =
+ * target_peak / peak (1 if peak is not > 0), rounded down to a power of two if
+ * asked; code = clamp(round_half_away((x - shift) * scale), -128, 127), NaN -> 0.
+ * A quantizer is (d, shift[d], scale), held by the caller. Device pointers
+ * (x_dev, sample_dev, codes_dev) must be 16-byte aligned. */
+
+/* Calibration, src/quantize.rs:17-34 (faiss(): {112, 1, 1.0}; clipped(q): {127, 0, q}). */
+typedef struct emb200_calibration {
+    float target_peak;     /* code magnitude the peak maps to */
+    int32_t power_of_two;  /* non-zero: round the scale down to a power of two */
+    double quantile;       /* which centred magnitude is the peak: 1.0 = the largest */
+} emb200_calibration;
+
+/* Int8Quantizer::fit, src/quantize.rs:45-62, on a host sample (n x d row-major
+ * f32, n > 0): writes shift[d] and *scale. */
+int emb200_quantizer_fit(emb200_handle* h, const float* sample, size_t n, size_t d, const emb200_calibration* cal,
+                         float* shift, float* scale);
+/* The same on a sample in device memory. */
+int emb200_quantizer_fit_device(emb200_handle* h, const float* sample_dev, size_t n, size_t d,
+                                const emb200_calibration* cal, float* shift, float* scale);
+/* The same on the resident f32 rows (emb200_load_rows). */
+int emb200_quantizer_fit_resident(emb200_handle* h, const emb200_calibration* cal, float* shift, float* scale);
+/* Int8Quantizer::encode (src/quantize.rs:65-73) of host rows into host codes
+ * (n x d), and the count of values that clip, the numerator of clipped_fraction
+ * (:87-95). codes or clipped may be NULL: encode only, or count only. */
+int emb200_quantizer_encode(emb200_handle* h, const float* x, size_t n, size_t d, const float* shift, float scale,
+                            int8_t* codes, uint64_t* clipped);
+/* The same on device rows into device codes, enqueued on `stream` (NULL: the
+ * handle's stream); returns when the work is done. */
+int emb200_quantizer_encode_device(emb200_handle* h, const float* x_dev, size_t n, size_t d, const float* shift,
+                                   float scale, int8_t* codes_dev, uint64_t* clipped, void* stream);
+/* Replace the resident f32 rows by their int8 codes: the resident rows become
+ * EMB200_I8 rows for emb200_train / emb200_assign_resident. */
+int emb200_quantize_resident(emb200_handle* h, const float* shift, float scale, uint64_t* clipped);
+/* Int8Quantizer::decode, src/quantize.rs:76-79: out = codes * (1 / scale) + shift
+ * (codes and out host n x d f32, e.g. centroids learned on codes). */
+int emb200_quantizer_decode(emb200_handle* h, const float* codes, size_t n, size_t d, const float* shift, float scale,
+                            float* out);
+
 /* ---- search without allocation (no counterpart in the reference) --------
  *
  * For callers that cannot allocate device memory when they search: programs

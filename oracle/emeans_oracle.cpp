@@ -807,12 +807,29 @@ void orc_quantizer_fit(const float* sample, size_t n, size_t d, float target_pea
     std::vector<float> mags(n * d);
     for (size_t i = 0; i < n; i++)
         for (size_t t = 0; t < d; t++) mags[i * d + t] = std::fabs(sample[i * d + t] - shift[t]);
-    double q = std::min(std::max(quantile, 0.0), 1.0);
+    // ((len - 1) as f64 * quantile.clamp(0, 1)).round() as usize: NaN -> 0
+    double q = std::isnan(quantile) ? 0.0 : std::min(std::max(quantile, 0.0), 1.0);
     size_t idx = (size_t)std::round((double)(mags.size() - 1) * q);
-    std::nth_element(mags.begin(), mags.begin() + idx, mags.end());
+    // select_nth_unstable_by(idx, f32::total_cmp): order by the sign-folded bit pattern
+    auto total_key = [](float v) {
+        int32_t b;
+        std::memcpy(&b, &v, 4);
+        return b ^ (int32_t)((uint32_t)(b >> 31) >> 1);
+    };
+    std::nth_element(mags.begin(), mags.begin() + idx, mags.end(),
+                     [&](float a, float b) { return total_key(a) < total_key(b); });
     float peak = mags[idx];
     float scale = peak > 0.0f ? target_peak / peak : 1.0f;
-    if (power_of_two) scale = std::pow(2.0f, (float)(int)std::floor(std::log2(scale)));
+    if (power_of_two) {
+        // 2f32.powi(scale.log2().floor() as i32): saturating cast, NaN -> 0
+        float l = std::floor(std::log2(scale));
+        int e = std::isnan(l) ? 0 : l >= 2147483647.0f ? INT32_MAX : l <= -2147483648.0f ? INT32_MIN : (int)l;
+        // powi forms 2^|e| by repeated squaring (inf from 2^128 on), then 1 / 2^|e| for e < 0
+        if (e >= 128) scale = INFINITY;
+        else if (e >= 0) scale = std::ldexp(1.0f, e);
+        else if (e > -128) scale = 1.0f / std::ldexp(1.0f, -e);
+        else scale = 0.0f;
+    }
     *scale_out = scale;
 }
 
@@ -828,6 +845,25 @@ void orc_quantizer_encode(const float* x, size_t n, size_t d, const float* shift
             float r = std::min(std::max(std::round(v), -128.0f), 127.0f);
             out[i * d + t] = (int8_t)r;
         }
+}
+
+// Int8Quantizer::clipped_fraction numerator, src/quantize.rs:87-95: values whose
+// scaled centred value lies outside [-128.5, 127.5) (NaN included).
+uint64_t orc_quantizer_clipped(const float* x, size_t n, size_t d, const float* shift, float scale) {
+    uint64_t c = 0;
+    for (size_t i = 0; i < n; i++)
+        for (size_t t = 0; t < d; t++) {
+            float v = (x[i * d + t] - shift[t]) * scale;
+            if (!(v >= -128.5f && v < 127.5f)) c++;
+        }
+    return c;
+}
+
+// Int8Quantizer::decode, src/quantize.rs:76-79.
+void orc_quantizer_decode(const float* codes, size_t n, size_t d, const float* shift, float scale, float* out) {
+    float inv = 1.0f / scale;
+    for (size_t i = 0; i < n; i++)
+        for (size_t t = 0; t < d; t++) out[i * d + t] = codes[i * d + t] * inv + shift[t];
 }
 
 }  // extern "C"

@@ -80,6 +80,9 @@ def lib():
         L.orc_balance_stats.argtypes = [P, S, S, P]
         L.orc_quantizer_fit.argtypes = [P, S, S, ctypes.c_float, ctypes.c_double, ctypes.c_int, P, P]
         L.orc_quantizer_encode.argtypes = [P, S, S, P, ctypes.c_float, P]
+        L.orc_quantizer_clipped.restype = ctypes.c_uint64
+        L.orc_quantizer_clipped.argtypes = [P, S, S, P, ctypes.c_float]
+        L.orc_quantizer_decode.argtypes = [P, S, S, P, ctypes.c_float, P]
         L.orc_cpu_has_kernel.argtypes = [ctypes.c_int]
         _lib = L
     return _lib
@@ -237,6 +240,20 @@ def quantizer_fit(sample, target_peak=112.0, quantile=1.0, power_of_two=True):
     scale = np.zeros(1, np.float32)
     lib().orc_quantizer_fit(_p(s), n, d, target_peak, quantile, int(power_of_two), _p(shift), _p(scale))
     return shift, float(scale[0])
+
+
+def quantizer_clipped(x, shift, scale):
+    x = np.ascontiguousarray(x, np.float32)
+    n, d = x.shape
+    return int(lib().orc_quantizer_clipped(_p(x), n, d, _p(np.ascontiguousarray(shift, np.float32)), scale))
+
+
+def quantizer_decode(codes, shift, scale):
+    c = np.ascontiguousarray(codes, np.float32)
+    n, d = c.shape
+    out = np.zeros((n, d), np.float32)
+    lib().orc_quantizer_decode(_p(c), n, d, _p(np.ascontiguousarray(shift, np.float32)), scale, _p(out))
+    return out
 
 
 def quantizer_encode(x, shift, scale):

@@ -184,6 +184,19 @@ def test_faiss_calibration_and_round_trip(orc):
     back = codes.astype(np.float32) * np.float32(1.0 / scale) + shift
     assert np.array_equal(back, sample)
     assert orc.quantizer_encode(np.array([[1000.0, -3.0]], np.float32), shift, scale).ravel().tolist() == [127, 0]
+    assert np.array_equal(orc.quantizer_decode(codes, shift, scale), sample)
+    assert orc.quantizer_clipped(np.array([[1000.0, -3.0]], np.float32), shift, scale) / 2 == 0.5
+
+
+def test_clipped_calibration(orc):
+    # Calibration::clipped(q) (src/quantize.rs:31-33): the peak is the centred
+    # magnitude at rank round((n d - 1) q), the scale 127 / peak, not a power of two.
+    x = np.array([[0.0], [1.0], [2.0], [3.0], [4.0], [100.0]], np.float32)  # mean 18.333..
+    shift, scale = orc.quantizer_fit(x, 127.0, 0.5, False)
+    mags = np.sort(np.abs(x[:, 0] - shift[0]))
+    assert shift[0] == np.float32(np.float64(110.0) / 6)
+    # rank round(5 x 0.5) = 3: f64::round goes half away from zero
+    assert scale == np.float32(127.0) / mags[3]
 
 
 def test_i8_rows_through_cpu_assigner_equal_f32(orc):
