@@ -68,6 +68,22 @@ class _ProposerConfig(ctypes.Structure):
 PROPOSER_MODES = {"mlp": 0, "centroids": 1}
 
 
+class _ReportConfig(ctypes.Structure):
+    _fields_ = [("family_radius", ctypes.c_float), ("reserved", ctypes.c_uint32), ("min_local_size", ctypes.c_uint64)]
+
+
+class _ReportSummary(ctypes.Structure):
+    _fields_ = [("median_dist", ctypes.c_float), ("median_rms", ctypes.c_float),
+                ("median_nearest_dist", ctypes.c_float), ("n_families", ctypes.c_uint32),
+                ("n_live", ctypes.c_uint32), ("reserved", ctypes.c_uint32 * 3)]
+
+
+# ClusterStats, src/report.rs:37-56, as emb200_cluster_stats (48 bytes, no padding)
+CLUSTER_STATS = np.dtype([("size", "u4"), ("rms", "f4"), ("median", "f4"), ("mad", "f4"), ("p90", "f4"),
+                          ("p99", "f4"), ("max", "f4"), ("looseness", "f4"), ("nearest_centroid", "u4"),
+                          ("nearest_dist", "f4"), ("isolation", "f4"), ("family", "u4")])
+
+
 class _Calibration(ctypes.Structure):
     _fields_ = [("target_peak", ctypes.c_float), ("power_of_two", ctypes.c_int32), ("quantile", ctypes.c_double)]
 
@@ -130,6 +146,10 @@ def lib():
     L.emb200_quantizer_encode_device.argtypes = [P, P, S, S, P, ctypes.c_float, P, P, P]
     L.emb200_quantize_resident.argtypes = [P, P, ctypes.c_float, P]
     L.emb200_quantizer_decode.argtypes = [P, P, S, S, P, ctypes.c_float, P]
+    RC = ctypes.POINTER(_ReportConfig)
+    L.emb200_report.argtypes = [P, P, P, S, P, S, S, RC, P, P, P, ctypes.POINTER(_ReportSummary)]
+    L.emb200_report_resident.argtypes = [P, RC, P, P, P, ctypes.POINTER(_ReportSummary)]
+    L.emb200_report_families.argtypes = [P, P, P, P, P, P]
     _lib = L
     return L
 
@@ -487,9 +507,9 @@ class Calibration:
 _quant_handle = None
 
 
-def _quantizer_assigner(assigner):
-    """The handle whose GPU runs a quantizer call: the given assigner, else one
-    module-wide handle on device 0."""
+def _default_assigner(assigner):
+    """The handle whose GPU runs a quantizer or report call: the given assigner,
+    else one module-wide handle on device 0."""
     global _quant_handle
     if assigner is not None:
         return assigner
@@ -514,7 +534,7 @@ class Int8Quantizer:
         n = x.size // d
         if n == 0 or x.size != n * d:
             raise ValueError("the sample must hold n > 0 whole rows of d values")
-        a = _quantizer_assigner(assigner)
+        a = _default_assigner(assigner)
         shift = np.empty(d, np.float32)
         scale = ctypes.c_float()
         c = cal._c()
@@ -536,7 +556,7 @@ class Int8Quantizer:
         x = np.ascontiguousarray(x, np.float32).reshape(-1)
         if x.size % self.d:
             raise ValueError("rows must hold whole rows of d values")
-        a = _quantizer_assigner(assigner)
+        a = _default_assigner(assigner)
         clipped = ctypes.c_uint64()
         a._check(lib().emb200_quantizer_encode(a._h, _p(x), x.size // self.d, self.d, _p(self.shift),
                                                float(self.scale), _p(codes), ctypes.byref(clipped)))
@@ -562,7 +582,7 @@ class Int8Quantizer:
         if flat.size % self.d:
             raise ValueError("codes must hold whole rows of d values")
         out = np.empty(flat.size, np.float32)
-        a = _quantizer_assigner(assigner)
+        a = _default_assigner(assigner)
         a._check(lib().emb200_quantizer_decode(a._h, _p(flat), flat.size // self.d, self.d, _p(self.shift),
                                                float(self.scale), _p(out)))
         return out.reshape(c.shape)
@@ -579,3 +599,138 @@ class Int8Quantizer:
         assigner._check(lib().emb200_quantize_resident(assigner._h, _p(self.shift), float(self.scale),
                                                        ctypes.byref(clipped)))
         return clipped.value
+
+
+# ---- report (src/report.rs) --------------------------------------------------
+
+@dataclass
+class ReportConfig:
+    """src/report.rs:21-34."""
+
+    family_radius: float = 1.25
+    min_local_size: int = 30
+
+    def _c(self):
+        return _ReportConfig(self.family_radius, 0, self.min_local_size)
+
+
+@dataclass
+class Family:
+    """src/report.rs:58-66."""
+
+    leader: int
+    members: np.ndarray
+    size: int
+    share: float
+
+
+def _order_key(v):
+    """f32::total_cmp as an unsigned order."""
+    b = np.ascontiguousarray(v, np.float32).view(np.uint32)
+    return b ^ np.where(b >> 31 != 0, np.uint32(0xFFFFFFFF), np.uint32(0x80000000))
+
+
+class Report:
+    """Report (src/report.rs:68-81): computed by `report()` on the B200; the
+    methods below (src/report.rs:243-291) are views over its arrays."""
+
+    def __init__(self, clusters, families, local_z, global_z, median_dist, median_rms, median_nearest_dist):
+        self.clusters = clusters  # CLUSTER_STATS array of k
+        self.families = families  # list of Family, largest first
+        self.local_z = local_z
+        self.global_z = global_z
+        self.median_dist = np.float32(median_dist)
+        self.median_rms = np.float32(median_rms)
+        self.median_nearest_dist = np.float32(median_nearest_dist)
+
+    def scores(self):
+        """score() of every row: max(local_z, global_z), NaN ignored as f32::max does."""
+        return np.fmax(self.local_z, self.global_z)
+
+    def score(self, row):
+        """src/report.rs:246-248."""
+        return np.float32(np.fmax(self.local_z[row], self.global_z[row]))
+
+    def top_outliers(self, count):
+        """The `count` highest-scoring rows as (row, score), best first (total_cmp
+        order; equal scores by row index)."""
+        s = self.scores()
+        count = min(count, s.size)
+        key = np.uint32(0xFFFFFFFF) - _order_key(s)
+        idx = np.argsort(key, kind="stable")[:count]
+        return [(int(i), np.float32(s[i])) for i in idx]
+
+    def rare_prototypes(self, max_size_ratio, min_isolation):
+        """(cluster, size, isolation) of small, isolated clusters, most isolated
+        first (src/report.rs:264-276; equal isolation by cluster index)."""
+        c = self.clusters
+        live = max(int(np.count_nonzero(c["size"])), 1)
+        mean = np.float32(self.local_z.size) / np.float32(live)
+        thr = np.float32(max_size_ratio) * mean
+        sel = (c["size"] > 0) & (c["size"].astype(np.float32) <= thr) & (c["isolation"] >= np.float32(min_isolation))
+        js = np.nonzero(sel)[0]
+        key = np.uint32(0xFFFFFFFF) - _order_key(c["isolation"][js])
+        js = js[np.argsort(key, kind="stable")]
+        return [(int(j), int(c["size"][j]), np.float32(c["isolation"][j])) for j in js]
+
+    def write_clusters_tsv(self, w):
+        """src/report.rs:279-290."""
+        w.write("cluster\tsize\trms\tmedian\tmad\tp90\tp99\tmax\tlooseness\tnearest_centroid\tnearest_dist"
+                "\tisolation\tfamily\tfamily_share\n")
+        for j, c in enumerate(self.clusters):
+            share = self.families[int(c["family"])].share if c["size"] > 0 else 0.0
+            w.write(f"{j}\t{c['size']}\t{c['rms']:.5f}\t{c['median']:.5f}\t{c['mad']:.5f}\t{c['p90']:.5f}\t"
+                    f"{c['p99']:.5f}\t{c['max']:.5f}\t{c['looseness']:.3f}\t{c['nearest_centroid']}\t"
+                    f"{c['nearest_dist']:.5f}\t{c['isolation']:.3f}\t{c['family']}\t{share:.6f}\n")
+
+
+def _report_result(a, n, k, clusters, lz, gz, summ):
+    F, live = summ.n_families, summ.n_live
+    leader = np.empty(max(F, 1), np.uint32)
+    size = np.empty(max(F, 1), np.uint64)
+    share = np.empty(max(F, 1), np.float64)
+    offs = np.empty(F + 1, np.uint32)
+    mem = np.empty(max(live, 1), np.uint32)
+    a._check(lib().emb200_report_families(a._h, _p(leader), _p(size), _p(share), _p(offs), _p(mem)))
+    fams = [Family(int(leader[f]), mem[offs[f]:offs[f + 1]].copy(), int(size[f]), float(share[f])) for f in range(F)]
+    return Report(clusters, fams, lz, gz, summ.median_dist, summ.median_rms, summ.median_nearest_dist)
+
+
+def report(labels, sqdist_to_centroid, centroids, d, cfg: Optional[ReportConfig] = None,
+           assigner: Optional[B200Assigner] = None) -> Report:
+    """report() (src/report.rs:121-241) on the B200."""
+    cfg = cfg or ReportConfig()
+    lab = np.ascontiguousarray(labels, np.uint32)
+    sq = np.ascontiguousarray(sqdist_to_centroid, np.float32)
+    c = np.ascontiguousarray(centroids, np.float32).reshape(-1)
+    if lab.size != sq.size:
+        raise ValueError("labels and distances differ in length")
+    k = c.size // d
+    if c.size != k * d:
+        raise ValueError("centroids must be k x d")
+    a = _default_assigner(assigner)
+    n = lab.size
+    clusters = np.zeros(k, CLUSTER_STATS)
+    lz = np.empty(n, np.float32)
+    gz = np.empty(n, np.float32)
+    summ = _ReportSummary()
+    cc = cfg._c()
+    a._check(lib().emb200_report(a._h, _p(lab), _p(sq), n, _p(c), k, d, ctypes.byref(cc), _p(clusters), _p(lz), _p(gz),
+                                 ctypes.byref(summ)))
+    return _report_result(a, n, k, clusters, lz, gz, summ)
+
+
+def report_resident(assigner: B200Assigner, cfg: Optional[ReportConfig] = None) -> Report:
+    """report() over the assigner's last assign_resident results and its
+    centroids, without leaving HBM."""
+    cfg = cfg or ReportConfig()
+    n = assigner.rows_shape[0]
+    k = assigner.k
+    clusters = np.zeros(k, CLUSTER_STATS)
+    lz = np.empty(n, np.float32)
+    gz = np.empty(n, np.float32)
+    summ = _ReportSummary()
+    cc = cfg._c()
+    assigner._check(lib().emb200_report_resident(assigner._h, ctypes.byref(cc), _p(clusters), _p(lz), _p(gz),
+                                                 ctypes.byref(summ)))
+    return _report_result(assigner, n, k, clusters, lz, gz, summ)

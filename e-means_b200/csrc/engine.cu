@@ -29,6 +29,7 @@
 #include "kernels_mlp_tc.cuh"
 #include "kernels_proposer.cuh"
 #include "kernels_quant.cuh"
+#include "kernels_report.cuh"
 
 constexpr int kRefineCap = 32;  // candidates kept per refined row
 
@@ -38,6 +39,8 @@ namespace {
 
 struct Proposer;
 void proposer_release(emb200_handle* h);
+struct ReportState;
+void report_release(emb200_handle* h);
 
 // Device buffer owned by a handle.
 template <typename T>
@@ -117,6 +120,8 @@ struct emb200_handle {
     size_t rows_n = 0, rows_d = 0;
     DevBuf<uint32_t> res_labels;
     DevBuf<float> res_dist;
+    size_t res_n = 0;            // rows of the last emb200_assign_resident (0: none valid)
+    uint64_t res_version = 0;    // centroid version those results belong to
 
     // scratch for assign
     DevBuf<uint8_t> stage;  // host-path staging of rows (two chunk buffers)
@@ -145,6 +150,9 @@ struct emb200_handle {
     DevBuf<QuantSelect> qsel;
     DevBuf<unsigned long long> qclip;
     DevBuf<uint8_t> qx, qcodes;
+
+    // report() state (emb200_report*)
+    ReportState* rep = nullptr;
 };
 
 namespace {
@@ -776,6 +784,7 @@ int emb200_destroy(emb200_handle* h) {
     h->qshift.release(); h->qsel.release(); h->qclip.release(); h->qx.release(); h->qcodes.release();
     h->train.release();
     proposer_release(h);
+    report_release(h);
     if (h->ev0) cudaEventDestroy(h->ev0);
     if (h->ev1) cudaEventDestroy(h->ev1);
     if (h->evk0) cudaEventDestroy(h->evk0);
@@ -849,6 +858,7 @@ int emb200_set_bias(emb200_handle* h, const float* bias, size_t k) {
     if (!h) return EMB200_EINVAL;
     if (!h->have_centroids) return fail(h, EMB200_ESTATE, "set_centroids must be called first");
     if (!bias || k != h->k) return fail(h, EMB200_EINVAL, "bias must have k = %zu entries", h->k);
+    h->res_n = 0;  // resident results no longer match the biased centroids
     CK(cudaMemcpyAsync(h->bias.p, bias, k * sizeof(float), cudaMemcpyHostToDevice, h->stream));
     double amax = 0.0;
     for (size_t j = 0; j < k; j++) amax = std::max(amax, std::fabs((double)bias[j]));
@@ -894,6 +904,7 @@ int emb200_load_rows(emb200_handle* h, int dtype, const void* x, size_t n, size_
     h->rows_dtype = dtype;
     h->rows_n = n;
     h->rows_d = d;
+    h->res_n = 0;
     return EMB200_OK;
 }
 
@@ -905,6 +916,7 @@ int emb200_assign_resident(emb200_handle* h, uint32_t* labels, float* dist) {
     if (h->rows_d != h->d) return fail(h, EMB200_EINVAL, "rows have d = %zu, centroids d = %zu", h->rows_d, h->d);
     if (h->res_labels.ensure(h->rows_n) || h->res_dist.ensure(h->rows_n))
         return fail(h, EMB200_ENOMEM, "result allocation failed");
+    h->res_n = 0;
     h->stats = emb200_stats{};
     cudaStream_t st = h->stream;
     CK(cudaEventRecord(h->ev0, st));
@@ -919,6 +931,8 @@ int emb200_assign_resident(emb200_handle* h, uint32_t* labels, float* dist) {
     h->stats.rows = h->rows_n;
     if (use_i8_mode(h, h->rows_dtype)) h->stats.rows_certified = h->rows_n;
     h->stats.ms_total = ms;
+    h->res_n = h->rows_n;
+    h->res_version = h->centroid_version;
     return EMB200_OK;
 }
 
@@ -1039,3 +1053,4 @@ extern "C" int emb200_assign_f32_noalloc(const float* x_dev, size_t m, size_t d,
 #include "engine_train.inc"
 #include "engine_proposer.inc"
 #include "engine_quant.inc"
+#include "engine_report.inc"

@@ -6,8 +6,8 @@
 //  * mean: the reference adds the rows in order into one f64 accumulator per
 //    dimension (`:48-51`). f64 addition is not associative, so a tree reduction
 //    could differ in the last bit; k_quant_colsum keeps the row order, one
-//    accumulator per dimension, and stages rows through shared memory so that
-//    the chain of dependent adds, not the loads, sets its pace.
+//    accumulator per dimension, and streams rows into shared memory by cp.async
+//    several stages ahead so that the chain of dependent adds sets its pace.
 //  * peak: `select_nth_unstable_by(idx, f32::total_cmp)` over |x - shift|
 //    (`:53-56`). Every magnitude has a clear sign bit, so total_cmp is the
 //    unsigned order of the bit patterns (NaNs above +inf); the select is a
@@ -24,7 +24,8 @@
 namespace emb {
 
 constexpr int kQsumRows = 256;     // rows per shared-memory stage of the column sums
-constexpr int kQsumThreads = 256;  // warp 0 sums, warps 1..7 stage the next chunk
+constexpr int kQsumStages = 4;     // stages in flight (cp.async groups)
+constexpr int kQsumThreads = 256;  // all threads copy; warp 0 sums
 constexpr int kQThreads = 512;     // element-wise passes
 constexpr int kQBins0 = 2048;      // bits 30..20 of a magnitude (bit 31 is always clear)
 constexpr int kQBins = 1024;       // bits 19..10, then bits 9..0
@@ -36,34 +37,60 @@ struct QuantSelect {
     unsigned long long hist[kQBins0];
 };
 
+__device__ __forceinline__ void qs_cp_async16(float* smem, const float* gmem) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void qs_cp_async4(float* smem, const float* gmem) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void qs_cp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void qs_cp_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
 // Per-dimension f64 sums in row order, then shift = (f32)(sum / n)
 // (src/quantize.rs:48-52). One CTA per 32 consecutive dimensions; lane t of
-// warp 0 owns dimension c0 + t. Dynamic shared memory: 2 x kQsumRows x 32 floats.
+// warp 0 owns dimension c0 + t and adds its values in row order. Rows arrive
+// in 256-row stages by cp.async, kQsumStages - 1 stages ahead of the sums (16-
+// byte copies when d % 4 == 0, else 4-byte copies). Dynamic shared memory:
+// kQsumStages x kQsumRows x 32 floats.
 __global__ void __launch_bounds__(kQsumThreads) k_quant_colsum(const float* __restrict__ x, size_t n, size_t d,
                                                                float* __restrict__ shift) {
-    extern __shared__ float qs_stage[];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    extern __shared__ __align__(16) float qs_stage[];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const size_t c0 = (size_t)blockIdx.x * 32;
-    const bool col_ok = c0 + lane < d;
     const size_t nchunks = (n + kQsumRows - 1) / kQsumRows;
-    auto stage = [&](size_t chunk, int buf, int w0, int nw) {
-        const size_t r0 = chunk * kQsumRows;
-        float* dst = qs_stage + buf * kQsumRows * 32;
-#pragma unroll 8
-        for (int r = w0; r < kQsumRows; r += nw) {
-            const size_t row = r0 + r;
-            float v = 0.f;
-            if (row < n && col_ok) v = __ldg(x + row * d + c0 + lane);
-            dst[r * 32 + lane] = v;
+    const bool vec = (d & 3) == 0;
+    auto issue = [&](size_t chunk) {
+        if (chunk < nchunks) {
+            const size_t r0 = chunk * kQsumRows;
+            float* dst = qs_stage + (chunk % kQsumStages) * (kQsumRows * 32);
+            if (vec) {  // 8 x 16 bytes per row slice
+                for (int e = tid; e < kQsumRows * 8; e += kQsumThreads) {
+                    const int r = e >> 3, q = e & 7;
+                    const size_t row = r0 + r, col = c0 + 4 * q;
+                    if (row < n && col < d) qs_cp_async16(dst + r * 32 + 4 * q, x + row * d + col);
+                }
+            } else {
+                for (int e = tid; e < kQsumRows * 32; e += kQsumThreads) {
+                    const int r = e >> 5, t = e & 31;
+                    const size_t row = r0 + r, col = c0 + t;
+                    if (row < n && col < d) qs_cp_async4(dst + r * 32 + t, x + row * d + col);
+                }
+            }
         }
+        qs_cp_commit();  // an empty group past the end keeps the group count uniform
     };
-    stage(0, 0, warp, kQsumThreads / 32);
-    __syncthreads();
+#pragma unroll
+    for (int s = 0; s < kQsumStages - 1; s++) issue(s);
     double acc = 0.0;
     for (size_t c = 0; c < nchunks; c++) {
-        const int b = (int)(c & 1);
+        issue(c + kQsumStages - 1);
+        qs_cp_wait<kQsumStages - 1>();  // this thread's copies of chunk c have landed
+        __syncthreads();                  // everyone's have
         if (warp == 0) {
-            const float* src = qs_stage + b * kQsumRows * 32;
+            const float* src = qs_stage + (c % kQsumStages) * (kQsumRows * 32);
             const int rows = (int)min((size_t)kQsumRows, n - c * kQsumRows);
             int r = 0;
             for (; r + 16 <= rows; r += 16) {  // loads ahead of the dependent adds
@@ -74,12 +101,11 @@ __global__ void __launch_bounds__(kQsumThreads) k_quant_colsum(const float* __re
                 for (int i = 0; i < 16; i++) acc = __dadd_rn(acc, (double)v[i]);
             }
             for (; r < rows; r++) acc = __dadd_rn(acc, (double)src[r * 32 + lane]);
-        } else if (c + 1 < nchunks) {
-            stage(c + 1, b ^ 1, warp - 1, kQsumThreads / 32 - 1);
         }
-        __syncthreads();
+        __syncthreads();  // the stage is free before it is refilled
     }
-    if (warp == 0 && col_ok) shift[c0 + lane] = __double2float_rn(__ddiv_rn(acc, (double)n));
+    qs_cp_wait<0>();
+    if (warp == 0 && c0 + lane < d) shift[c0 + lane] = __double2float_rn(__ddiv_rn(acc, (double)n));
 }
 
 // The element-wise passes visit elements e = 4 * t + j * S (t the global thread

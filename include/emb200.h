@@ -295,6 +295,58 @@ int emb200_quantize_resident(emb200_handle* h, const float* shift, float scale, 
 int emb200_quantizer_decode(emb200_handle* h, const float* codes, size_t n, size_t d, const float* shift, float scale,
                             float* out);
 
+/* ---- report (src/report.rs) ----------------------------------------------
+ *
+ * report() on the GPU: per-cluster statistics of the member distances, the
+ * nearest other live centroid, prototype families and per-row robust z-scores,
+ * from each row's label and squared distance (what assign returns) and the
+ * centroids. Values are bit-identical to the reference's, with one rule where
+ * the reference leaves the order to its unstable sort: clusters of equal size
+ * are taken in index order when families form, and families of equal size
+ * keep the order in which they formed. k <= 131072. */
+
+/* ReportConfig, src/report.rs:21-34 (default {1.25, 30}). */
+typedef struct emb200_report_config {
+    float family_radius;
+    uint32_t reserved;
+    uint64_t min_local_size;
+} emb200_report_config;
+
+/* ClusterStats, src/report.rs:37-56 (distances plain L2; an empty cluster has
+ * size 0 and zero statistics, but its nearest centroid is still filled). */
+typedef struct emb200_cluster_stats {
+    uint32_t size;
+    float rms, median, mad, p90, p99, max, looseness;
+    uint32_t nearest_centroid;
+    float nearest_dist, isolation;
+    uint32_t family;
+} emb200_cluster_stats;
+
+/* Report's scalars (src/report.rs:78-80), and the sizes of the family arrays. */
+typedef struct emb200_report_summary {
+    float median_dist, median_rms, median_nearest_dist;
+    uint32_t n_families;  /* families, largest first */
+    uint32_t n_live;      /* non-empty clusters = total family members */
+    uint32_t reserved[3];
+} emb200_report_summary;
+
+/* report(labels, sqdist, centroids, d, cfg), src/report.rs:121-241, on host
+ * arrays: labels[n] (< k), sqdist[n], centroids k x d. Writes clusters[k],
+ * local_z[n], global_z[n] (either may be NULL) and the summary. */
+int emb200_report(emb200_handle* h, const uint32_t* labels, const float* sqdist, size_t n, const float* centroids,
+                  size_t k, size_t d, const emb200_report_config* cfg, emb200_cluster_stats* clusters,
+                  float* local_z, float* global_z, emb200_report_summary* summary);
+/* The same on the labels and distances of the last emb200_assign_resident (or
+ * emb200_assign_proposed_resident) and the handle's centroids, all in HBM. */
+int emb200_report_resident(emb200_handle* h, const emb200_report_config* cfg, emb200_cluster_stats* clusters,
+                           float* local_z, float* global_z, emb200_report_summary* summary);
+/* Families of the last report (Family, src/report.rs:58-66): leader[F],
+ * size[F], share[F], offsets[F + 1] into members[n_live] (members of family f,
+ * in decreasing cluster size, are members[offsets[f] .. offsets[f + 1])).
+ * F = summary.n_families. Any pointer may be NULL. */
+int emb200_report_families(emb200_handle* h, uint32_t* leader, uint64_t* size, double* share, uint32_t* offsets,
+                           uint32_t* members);
+
 /* ---- search without allocation (no counterpart in the reference) --------
  *
  * For callers that cannot allocate device memory when they search: programs

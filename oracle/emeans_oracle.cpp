@@ -19,6 +19,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdint>
+#include <cfloat>
 #include <cstring>
 #include <vector>
 #include <immintrin.h>
@@ -864,6 +865,186 @@ void orc_quantizer_decode(const float* codes, size_t n, size_t d, const float* s
     float inv = 1.0f / scale;
     for (size_t i = 0; i < n; i++)
         for (size_t t = 0; t < d; t++) out[i * d + t] = codes[i * d + t] * inv + shift[t];
+}
+
+// ---------------------------------------------------------------- report
+// report(), src/report.rs:83-241. Cluster fields in declaration order
+// (src/report.rs:37-56).
+struct OrcClusterStats {
+    uint32_t size;
+    float rms, median, mad, p90, p99, max, looseness;
+    uint32_t nearest_centroid;
+    float nearest_dist, isolation;
+    uint32_t family;
+};
+
+static int32_t rep_total_key(float v) {  // f32::total_cmp as a signed integer order
+    int32_t b;
+    std::memcpy(&b, &v, 4);
+    return b ^ (int32_t)((uint32_t)(b >> 31) >> 1);
+}
+static bool rep_less(float a, float b) { return rep_total_key(a) < rep_total_key(b); }
+
+// quantile, src/report.rs:83-88
+static float rep_quantile(const float* sorted, size_t len, double q) {
+    if (len == 0) return 0.0f;
+    return sorted[(size_t)std::round((double)(len - 1) * q)];
+}
+
+// median_mad, src/report.rs:91-96
+static void rep_median_mad(const float* sorted, size_t len, float* med, float* mad) {
+    *med = rep_quantile(sorted, len, 0.5);
+    std::vector<float> dev(len);
+    for (size_t i = 0; i < len; i++) dev[i] = std::fabs(sorted[i] - *med);
+    std::sort(dev.begin(), dev.end(), rep_less);
+    *mad = rep_quantile(dev.data(), len, 0.5);
+}
+
+// sqdist, src/report.rs:104-114: 16 lane accumulators over whole 16-chunks,
+// a sequential tail, then the lanes summed in order and the tail added.
+static float rep_sqdist(const float* a, const float* b, size_t d) {
+    float acc[16] = {0};
+    const size_t d16 = d / 16 * 16;
+    float tail = 0.0f;
+    for (size_t t = d16; t < d; t++) tail += (a[t] - b[t]) * (a[t] - b[t]);
+    for (size_t c = 0; c < d16; c += 16)
+        for (int i = 0; i < 16; i++) acc[i] += (a[c + i] - b[c + i]) * (a[c + i] - b[c + i]);
+    float s = 0.0f;
+    for (int i = 0; i < 16; i++) s += acc[i];
+    return s + tail;
+}
+
+static float rep_max_ignoring_nan(float a, float b) { return std::isnan(a) ? b : std::isnan(b) ? a : (a > b ? a : b); }
+
+// Equal-size clusters are ordered by index (the reference's sort_unstable_by_key
+// leaves that order to its sort algorithm), and equal-size families by the order
+// they were formed in.
+void orc_report(const uint32_t* labels, const float* sq, size_t n, const float* c, size_t k, size_t d,
+                float family_radius, size_t min_local_size, OrcClusterStats* clusters, float* local_z,
+                float* global_z, float* medians, uint32_t* n_families, uint32_t* fam_leader, uint64_t* fam_size,
+                double* fam_share, uint32_t* fam_offsets, uint32_t* fam_members) {
+    std::vector<float> dist(n);
+    for (size_t i = 0; i < n; i++) dist[i] = std::sqrt(rep_max_ignoring_nan(sq[i], 0.0f));
+    std::vector<size_t> start(k + 1, 0);
+    for (size_t i = 0; i < n; i++) start[labels[i] + 1]++;
+    for (size_t j = 0; j < k; j++) start[j + 1] += start[j];
+    std::vector<size_t> cursor(start.begin(), start.end() - 1);
+    std::vector<float> grouped(n);
+    for (size_t i = 0; i < n; i++) grouped[cursor[labels[i]]++] = dist[i];
+
+    std::vector<float> all(dist);
+    std::sort(all.begin(), all.end(), rep_less);
+    float g_med, g_mad;
+    rep_median_mad(all.data(), n, &g_med, &g_mad);
+    const float g_scale = rep_max_ignoring_nan(1.4826f * g_mad, FLT_MIN);
+
+    for (size_t j = 0; j < k; j++) {
+        OrcClusterStats cs{};
+        const size_t len = start[j + 1] - start[j];
+        if (len) {
+            std::vector<float> m(grouped.begin() + start[j], grouped.begin() + start[j + 1]);
+            std::sort(m.begin(), m.end(), rep_less);
+            rep_median_mad(m.data(), len, &cs.median, &cs.mad);
+            double ss = 0.0;
+            for (float v : m) ss += (double)v * (double)v;
+            cs.size = (uint32_t)len;
+            cs.rms = (float)std::sqrt(ss / (double)len);
+            cs.p90 = rep_quantile(m.data(), len, 0.9);
+            cs.p99 = rep_quantile(m.data(), len, 0.99);
+            cs.max = m.back();
+        }
+        clusters[j] = cs;
+    }
+
+    // nearest other live centroid, src/report.rs:170-183
+    std::vector<uint32_t> nj(k);
+    std::vector<float> nd(k);
+#pragma omp parallel for schedule(dynamic, 16)
+    for (long i = 0; i < (long)k; i++) {
+        uint32_t bj = (uint32_t)i;
+        float bs = INFINITY;
+        for (size_t j = 0; j < k; j++) {
+            if (j == (size_t)i || clusters[j].size == 0) continue;
+            const float s = rep_sqdist(c + i * d, c + j * d, d);
+            if (s < bs) {
+                bs = s;
+                bj = (uint32_t)j;
+            }
+        }
+        nj[i] = bj;
+        nd[i] = std::sqrt(bs);
+    }
+    std::vector<float> rl, nl;
+    for (size_t j = 0; j < k; j++)
+        if (clusters[j].size) {
+            rl.push_back(clusters[j].rms);
+            nl.push_back(nd[j]);
+        }
+    std::sort(rl.begin(), rl.end(), rep_less);
+    std::sort(nl.begin(), nl.end(), rep_less);
+    const float median_rms = rep_quantile(rl.data(), rl.size(), 0.5);
+    const float median_nearest = rep_quantile(nl.data(), nl.size(), 0.5);
+    for (size_t j = 0; j < k; j++) {
+        clusters[j].nearest_centroid = nj[j];
+        clusters[j].nearest_dist = nd[j];
+        clusters[j].looseness = clusters[j].rms / rep_max_ignoring_nan(median_rms, FLT_MIN);
+        clusters[j].isolation = nd[j] / rep_max_ignoring_nan(median_nearest, FLT_MIN);
+    }
+
+    // families, src/report.rs:198-223
+    const float radius = family_radius * median_nearest;
+    std::vector<size_t> order;
+    for (size_t j = 0; j < k; j++)
+        if (clusters[j].size) order.push_back(j);
+    std::stable_sort(order.begin(), order.end(),
+                     [&](size_t a, size_t b) { return clusters[a].size > clusters[b].size; });
+    std::vector<uint32_t> family_of(k, UINT32_MAX);
+    std::vector<uint32_t> lead_of;
+    std::vector<uint64_t> size_of;
+    std::vector<std::vector<uint32_t>> members;
+    for (size_t lead : order) {
+        if (family_of[lead] != UINT32_MAX) continue;
+        std::vector<uint32_t> joins;
+        for (size_t j : order)
+            if (family_of[j] == UINT32_MAX &&
+                (j == lead || std::sqrt(rep_sqdist(c + lead * d, c + j * d, d)) <= radius))
+                joins.push_back((uint32_t)j);
+        uint64_t size = 0;
+        for (uint32_t j : joins) {
+            family_of[j] = (uint32_t)lead_of.size();
+            size += clusters[j].size;
+        }
+        lead_of.push_back((uint32_t)lead);
+        size_of.push_back(size);
+        members.push_back(joins);
+    }
+    std::vector<size_t> rank(lead_of.size());
+    for (size_t f = 0; f < rank.size(); f++) rank[f] = f;
+    std::stable_sort(rank.begin(), rank.end(), [&](size_t a, size_t b) { return size_of[a] > size_of[b]; });
+    size_t off = 0;
+    fam_offsets[0] = 0;
+    for (size_t f = 0; f < rank.size(); f++) {
+        const size_t g = rank[f];
+        fam_leader[f] = lead_of[g];
+        fam_size[f] = size_of[g];
+        fam_share[f] = (double)size_of[g] / (double)n;
+        for (uint32_t j : members[g]) {
+            fam_members[off++] = j;
+            clusters[j].family = (uint32_t)f;
+        }
+        fam_offsets[f + 1] = (uint32_t)off;
+    }
+    *n_families = (uint32_t)rank.size();
+
+    for (size_t i = 0; i < n; i++) {
+        const float gz = (dist[i] - g_med) / g_scale;
+        global_z[i] = gz;
+        const OrcClusterStats& cs = clusters[labels[i]];
+        local_z[i] = ((size_t)cs.size < min_local_size || cs.mad <= 0.0f) ? gz : (dist[i] - cs.median) / (1.4826f * cs.mad);
+    }
+    medians[0] = g_med;
+    medians[1] = median_rms;
+    medians[2] = median_nearest;
 }
 
 }  // extern "C"

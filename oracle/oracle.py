@@ -84,6 +84,7 @@ def lib():
         L.orc_quantizer_clipped.argtypes = [P, S, S, P, ctypes.c_float]
         L.orc_quantizer_decode.argtypes = [P, S, S, P, ctypes.c_float, P]
         L.orc_cpu_has_kernel.argtypes = [ctypes.c_int]
+        L.orc_report.argtypes = [P, P, S, P, S, S, ctypes.c_float, S, P, P, P, P, P, P, P, P, P, P]
         _lib = L
     return _lib
 
@@ -262,3 +263,36 @@ def quantizer_encode(x, shift, scale):
     out = np.zeros((n, d), np.int8)
     lib().orc_quantizer_encode(_p(x), n, d, _p(np.ascontiguousarray(shift, np.float32)), scale, _p(out))
     return out
+
+
+# ClusterStats, src/report.rs:37-56 (field order kept; 48 bytes, no padding)
+CLUSTER_STATS = np.dtype([("size", "u4"), ("rms", "f4"), ("median", "f4"), ("mad", "f4"), ("p90", "f4"),
+                          ("p99", "f4"), ("max", "f4"), ("looseness", "f4"), ("nearest_centroid", "u4"),
+                          ("nearest_dist", "f4"), ("isolation", "f4"), ("family", "u4")])
+
+
+def report(labels, sqdist, centroids, family_radius=1.25, min_local_size=30):
+    """report() (src/report.rs:121-241). Returns a dict: clusters (CLUSTER_STATS
+    array), local_z, global_z, median_dist, median_rms, median_nearest_dist,
+    families (list of (leader, members, size, share))."""
+    labels = np.ascontiguousarray(labels, np.uint32)
+    sq = np.ascontiguousarray(sqdist, np.float32)
+    c = np.ascontiguousarray(centroids, np.float32)
+    k, d = c.shape
+    n = labels.size
+    clusters = np.zeros(k, CLUSTER_STATS)
+    lz = np.zeros(n, np.float32)
+    gz = np.zeros(n, np.float32)
+    med = np.zeros(3, np.float32)
+    nf = np.zeros(1, np.uint32)
+    leader = np.zeros(max(k, 1), np.uint32)
+    fsize = np.zeros(max(k, 1), np.uint64)
+    share = np.zeros(max(k, 1), np.float64)
+    offs = np.zeros(k + 1, np.uint32)
+    mem = np.zeros(max(k, 1), np.uint32)
+    lib().orc_report(_p(labels), _p(sq), n, _p(c), k, d, family_radius, min_local_size, _p(clusters), _p(lz), _p(gz),
+                     _p(med), _p(nf), _p(leader), _p(fsize), _p(share), _p(offs), _p(mem))
+    F = int(nf[0])
+    fams = [(int(leader[f]), mem[offs[f]:offs[f + 1]].copy(), int(fsize[f]), float(share[f])) for f in range(F)]
+    return {"clusters": clusters, "local_z": lz, "global_z": gz, "median_dist": med[0], "median_rms": med[1],
+            "median_nearest_dist": med[2], "families": fams}
