@@ -405,6 +405,71 @@ def run_c3(args):
     print(json.dumps(line), flush=True)
 
 
+def run_report(args):
+    """report() (src/report.rs:121-241) on the 1M x 128 embedding rows with k =
+    16384 engine-trained centroids, after one exact resident assign: per-cluster
+    statistics, medians, nearest other centroid (an exact k^2 d pair pass),
+    families and per-row z-scores. value: rows/s of the device report over the
+    resident results; e2e: the host-array call (labels, distances and centroids
+    uploaded, every output read back); cpu_baseline: the oracle's restatement on
+    the same inputs, checked equal to the device report."""
+    from __graft_entry__ import load_package
+    from oracle import oracle as orc
+
+    emb, x = make_rows(0)
+    n, d = x.shape
+    cent = trained_centroids(emb, x, 0)
+    a = emb.B200Assigner(0, precision="bf16x1")
+    a.load_rows(x)
+    a.set_centroids(cent)
+    labels, sq = a.assign_resident()
+    for _ in range(args.warmup):
+        emb.report_resident(a)
+    ms = []
+    clock = ClockSampler(0)
+    with clock:
+        for _ in range(args.steps):
+            r = emb.report_resident(a)
+            ms.append(a.stats()["ms_total"])
+    t = float(np.mean(ms))
+    e2e = []
+    for _ in range(max(1, min(args.steps, 3))):
+        t0 = time.perf_counter()
+        emb.report(labels, sq, cent, d, assigner=a)
+        e2e.append(time.perf_counter() - t0)
+    te = float(np.mean(e2e))
+    live = int(np.count_nonzero(r.clusters["size"]))
+    pairs = 2.0 * K * K * d  # two exact pair passes (nearest, family radius), each k^2 d
+    line = {"metric": "rows/s reported (report() over 1M x 128 rows, k=16384)", "value": n / (t / 1e3),
+            "unit": "rows/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": t,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32 / f64 (reference rounding)",
+            "data": "synthetic", "gpu_launches": int(a.stats()["kernel_launches"]),
+            "config": {"workload": f"report of {n} x {d} embedding rows, k={K} trained centroids",
+                       "live_clusters": live, "families": len(r.families)},
+            "clocks": clock.summary(),
+            "pair_pass": {"element_ops": pairs, "note": "k^2 d (c_i - c_j)^2 terms per pass, SIMT f32 in the "
+                                                        "reference's sqdist rounding (no tensor cores: the order of "
+                                                        "roundings is the result)"},
+            "e2e": {"value": n / te, "unit": "rows/s", "h2d_bytes_per_step": n * 8 + K * d * 4,
+                    "d2h_bytes_per_step": n * 8 + K * 48 + live * 4}}
+    if not args.no_cpu:
+        cores = os.cpu_count() or 1
+        t0 = time.perf_counter()
+        o = orc.report(labels, sq, cent)
+        tc = time.perf_counter() - t0
+        same = (all(np.array_equal(np.nan_to_num(r.clusters[f]), np.nan_to_num(o["clusters"][f]))
+                    for f in r.clusters.dtype.names)
+                and np.array_equal(r.local_z, o["local_z"]) and np.array_equal(r.global_z, o["global_z"])
+                and len(r.families) == len(o["families"])
+                and all(f.leader == g[0] and np.array_equal(f.members, g[1]) for f, g in zip(r.families, o["families"])))
+        line["cpu_baseline"] = {"value": n / tc, "unit": "rows/s", "cores": cores, "kind": "port",
+                                "sample": f"the whole workload: report() restated in C++ (nearest-centroid pass "
+                                          f"OpenMP {cores} threads, the rest one thread), {tc:.2f} s",
+                                "identical_to_device": bool(same)}
+    a.close()
+    print(json.dumps(line), flush=True)
+
+
 def run_c4(args):
     """Batched uneven instances (configuration 4): (a) PQ training, 4,000,000 x 128
     Gaussian-mixture rows split into 16 sub-spaces of d=8, k=256 each; (b) 48 IVF
@@ -656,7 +721,7 @@ def main():
     ap.add_argument("--rows", type=int, default=N_ROWS, help="rows per pass (profiling captures use fewer)")
     ap.add_argument("--centroids", default="trained", choices=["trained", "sampled"],
                     help="trained by the engine (default) or a fixed sample of rows (profiling captures)")
-    ap.add_argument("--workload", default="c2", choices=["c2", "c1", "c3", "c4a", "c4b", "c5"],
+    ap.add_argument("--workload", default="c2", choices=["c2", "c1", "c3", "c4a", "c4b", "c5", "report"],
                     help="c2: the headline assign benchmark; the others: the remaining configurations")
     ap.add_argument("--proposer-steps", type=int, default=8000, help="c5: Adam steps of the network")
     ap.add_argument("--proposer-configs", default="32:0:0.999,32:0:0.9999,16:0:0.99,8:0:0",
@@ -674,6 +739,8 @@ def main():
         return run_c4(args)
     if args.workload == "c5" and args.impl == "ours":
         return run_c5(args)
+    if args.workload == "report" and args.impl == "ours":
+        return run_report(args)
     args.precisions = args.precisions.split(",")
     if args.impl == "reference":
         run_reference(args)

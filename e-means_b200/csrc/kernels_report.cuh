@@ -381,128 +381,213 @@ __global__ void k_rep_z(const uint32_t* __restrict__ labels, const float* __rest
 constexpr int kPairT = 32;         // rows and columns per tile
 constexpr int kPairThreads = 256;  // 16 dimension lanes x 16 groups of 8 x 8 pairs
 constexpr int kPairDC = 64;        // dimensions per staged chunk
-constexpr int kPairLd = kPairDC + 1;
+constexpr int kPairLd = kPairDC + 4;  // row pitch of a staged chunk (16-byte rows for cp.async)
 constexpr int kPairRed = 17;       // padded lane stride of the reduction buffer
+constexpr int kPairStage = 2 * kPairT * kPairLd;  // floats of one stage (row tile chunk + column tile chunk)
 
 constexpr size_t pair_smem_bytes() {
-    return sizeof(float) * (2 * kPairT * kPairLd + kPairT * kPairT * kPairRed + 2 * kPairT * 16);
+    return sizeof(float) * (2 * kPairStage + kPairT * kPairT * kPairRed + 2 * kPairT * 16) +
+           kPairT * (sizeof(unsigned long long) + sizeof(uint32_t));
 }
 
-// For every row i of this CTA's 32 and every column j, s = sqdist(c_i, c_j)
-// with the reference's rounding: lane l of 16 accumulates (c_i[t] - c_j[t])^2
-// over t = l, l + 16, ... below d16 = d - d % 16 (separate subtract, multiply
-// and add), the lanes are summed in order, then the tail (t >= d16, summed in
-// order) is added. NEAREST (ADJ = false): the first j != i with size > 0 and
-// the least s < inf (ties: lowest j), or (i, inf); ADJ: bit j of row i is set
-// when both are live, j != i and sqrt(s) <= radius.
+__device__ __forceinline__ void pair_cp16(float* smem, const float* gmem) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void pair_cp4(float* smem, const float* gmem) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+
+// Exact squared distances of centroid pairs in the reference's sqdist rounding
+// (src/report.rs:104-114): lane l of 16 accumulates (c_i[t] - c_j[t])^2 over
+// t = l, l + 16, ... below d16 = d - d % 16 (separate subtract, multiply and
+// add), the lanes are summed in order, then the tail (t >= d16, summed in
+// order) is added. The result is the same for (i, j) and (j, i) (x - y and
+// y - x square alike), so only tiles J >= I are computed; CTA b takes row tiles
+// b and T-1-b, which balances the triangle. Dimension chunks of both tiles are
+// double-buffered by cp.async.
+//   NEAREST (ADJ = false): near_key[i] = min over live j != i with s < inf of
+//   (bits of s, j), by 64-bit atomicMin (first j of the least s, as the
+//   reference's strict < scan); the host initialises it to all ones.
+//   ADJ: bit j of row i of the adjacency is set when both are live, j != i and
+//   sqrt(s) <= radius; every word of every row is written.
 template <bool ADJ>
 __global__ void __launch_bounds__(kPairThreads) k_rep_pairs(const float* __restrict__ c, uint32_t k, uint32_t d,
                                                             const uint32_t* __restrict__ start,
-                                                            uint32_t* __restrict__ near_j, float* __restrict__ near_s,
+                                                            unsigned long long* __restrict__ near_key,
                                                             const RepScalars* __restrict__ sc,
                                                             uint32_t* __restrict__ adj, uint32_t words) {
-    extern __shared__ float pair_sm[];
-    float* xs = pair_sm;
-    float* ys = xs + kPairT * kPairLd;
-    float* red = ys + kPairT * kPairLd;
-    float* xt = red + kPairT * kPairT * kPairRed;
-    float* yt = xt + kPairT * 16;
+    extern __shared__ __align__(16) float pair_sm[];
+    float* stage = pair_sm;                      // 2 stages x (row chunk, column chunk)
+    float* red = stage + 2 * kPairStage;         // [32 x 32 pairs][16 lanes]
+    float* xt = red + kPairT * kPairT * kPairRed;  // row tile tails [32][16]
+    float* yt = xt + kPairT * 16;                  // column tile tails
+    unsigned long long* colkey = reinterpret_cast<unsigned long long*>(yt + kPairT * 16);
+    uint32_t* colbits = reinterpret_cast<uint32_t*>(colkey + kPairT);
     const int tid = threadIdx.x, l = tid & 15, g = tid >> 4, gi = g >> 2, gj = g & 3;
-    const uint32_t i0 = blockIdx.x * kPairT;
-    const uint32_t d16 = d / 16 * 16, dt = d - d16;
     const int row = tid >> 3, sub = tid & 7;  // reduction: row, and columns sub*4 .. sub*4+3
-    const uint32_t i = i0 + row;
-    const bool live_i = i < k && start[i + 1] > start[i];
+    const uint32_t T = (k + kPairT - 1) / kPairT;
+    const uint32_t d16 = d / 16 * 16, dt = d - d16;
+    const uint32_t nchunk = (d16 + kPairDC - 1) / kPairDC;
+    const bool vec = (d & 3) == 0;
     const float radius = ADJ ? sc->radius : 0.0f;
-    unsigned long long best = ~0ull;
-    // tails of this CTA's rows
-    for (int e = tid; e < kPairT * 16; e += kPairThreads) {
-        const int r = e >> 4, t = e & 15;
-        xt[e] = (i0 + r < k && t < (int)dt) ? c[(size_t)(i0 + r) * d + d16 + t] : 0.0f;
-    }
-    const uint32_t ntiles = (k + kPairT - 1) / kPairT;
-    for (uint32_t jt = 0; jt < ntiles; jt++) {
-        const uint32_t j0 = jt * kPairT;
-        float acc[8][8];
-#pragma unroll
-        for (int a = 0; a < 8; a++)
-#pragma unroll
-            for (int b = 0; b < 8; b++) acc[a][b] = 0.0f;
-        for (uint32_t dc0 = 0; dc0 < d16; dc0 += kPairDC) {
-            __syncthreads();
-            for (int e = tid; e < kPairT * kPairDC; e += kPairThreads) {
-                const int r = e / kPairDC, t = e % kPairDC;
-                const uint32_t dim = dc0 + t;
-                xs[r * kPairLd + t] = (i0 + r < k && dim < d16) ? c[(size_t)(i0 + r) * d + dim] : 0.0f;
-                ys[r * kPairLd + t] = (j0 + r < k && dim < d16) ? c[(size_t)(j0 + r) * d + dim] : 0.0f;
-            }
-            __syncthreads();
-            const int nq = (int)min((uint32_t)(kPairDC / 16), (d16 - dc0) / 16);
-            for (int q = 0; q < nq; q++) {
-                float xv[8], yv[8];
-#pragma unroll
-                for (int a = 0; a < 8; a++) xv[a] = xs[(gi * 8 + a) * kPairLd + q * 16 + l];
-#pragma unroll
-                for (int b = 0; b < 8; b++) yv[b] = ys[(gj * 8 + b) * kPairLd + q * 16 + l];
-#pragma unroll
-                for (int a = 0; a < 8; a++)
-#pragma unroll
-                    for (int b = 0; b < 8; b++) {
-                        const float u = __fsub_rn(xv[a], yv[b]);
-                        acc[a][b] = __fadd_rn(acc[a][b], __fmul_rn(u, u));
-                    }
+    const uint32_t b = blockIdx.x, I0 = b, I1 = T - 1 - b;
+    const uint32_t n0 = (T - I0) * nchunk, n1 = I1 > I0 ? (T - I1) * nchunk : 0;
+    // item it -> (row tile, column tile, first dimension), in processing order
+    auto coords = [&](uint32_t it, uint32_t& I, uint32_t& J, uint32_t& dc0) {
+        const uint32_t base = it < n0 ? 0 : n0;
+        I = it < n0 ? I0 : I1;
+        const uint32_t r = it - base;
+        J = I + r / nchunk;
+        dc0 = (r % nchunk) * kPairDC;
+    };
+    auto issue = [&](uint32_t it) {
+        if (it < n0 + n1) {
+            uint32_t I, J, dc0;
+            coords(it, I, J, dc0);
+            float* xs = stage + (it & 1) * kPairStage;
+            float* ys = xs + kPairT * kPairLd;
+            if (vec) {
+                for (int e = tid; e < 2 * kPairT * (kPairDC / 4); e += kPairThreads) {
+                    const int side = e / (kPairT * (kPairDC / 4)), f = e % (kPairT * (kPairDC / 4));
+                    const int r = f / (kPairDC / 4), q = f % (kPairDC / 4);
+                    const uint32_t ci = (side ? J : I) * kPairT + r, dim = dc0 + 4 * q;
+                    if (ci < k && dim < d16) pair_cp16((side ? ys : xs) + r * kPairLd + 4 * q, c + (size_t)ci * d + dim);
+                }
+            } else {
+                for (int e = tid; e < 2 * kPairT * kPairDC; e += kPairThreads) {
+                    const int side = e / (kPairT * kPairDC), f = e % (kPairT * kPairDC);
+                    const int r = f / kPairDC, t = f % kPairDC;
+                    const uint32_t ci = (side ? J : I) * kPairT + r, dim = dc0 + t;
+                    if (ci < k && dim < d16) pair_cp4((side ? ys : xs) + r * kPairLd + t, c + (size_t)ci * d + dim);
+                }
             }
         }
-        __syncthreads();
-#pragma unroll
-        for (int a = 0; a < 8; a++)
-#pragma unroll
-            for (int b = 0; b < 8; b++) red[((gi * 8 + a) * kPairT + gj * 8 + b) * kPairRed + l] = acc[a][b];
+        asm volatile("cp.async.commit_group;\n" ::: "memory");
+    };
+    if (tid < kPairT) {
+        colkey[tid] = ~0ull;
+        colbits[tid] = 0u;
+    }
+    uint32_t it = 0;
+    issue(0);
+    for (int sd = 0; sd < 2; sd++) {
+        const uint32_t I = sd ? I1 : I0;
+        if (sd == 1 && I1 <= I0) break;
+        const uint32_t i0 = I * kPairT, i = i0 + row;
+        const bool live_i = i < k && start[i + 1] > start[i];
+        unsigned long long best = ~0ull;
+        __syncthreads();  // the previous row tile's tails are no longer read
         for (int e = tid; e < kPairT * 16; e += kPairThreads) {
             const int r = e >> 4, t = e & 15;
-            yt[e] = (j0 + r < k && t < (int)dt) ? c[(size_t)(j0 + r) * d + d16 + t] : 0.0f;
+            xt[e] = (i0 + r < k && t < (int)dt) ? c[(size_t)(i0 + r) * d + d16 + t] : 0.0f;
         }
-        __syncthreads();
-        uint32_t bits = 0;
+        for (uint32_t J = I; J < T; J++) {
+            const uint32_t j0 = J * kPairT;
+            float acc[8][8];
 #pragma unroll
-        for (int cc = 0; cc < 4; cc++) {
-            const int col = sub * 4 + cc;
-            const float* rp = red + (row * kPairT + col) * kPairRed;
-            float s = rp[0];
+            for (int a = 0; a < 8; a++)
 #pragma unroll
-            for (int q = 1; q < 16; q++) s = __fadd_rn(s, rp[q]);
-            float tail = 0.0f;
-            for (uint32_t t = 0; t < dt; t++) {
-                const float u = __fsub_rn(xt[row * 16 + t], yt[col * 16 + t]);
-                tail = __fadd_rn(tail, __fmul_rn(u, u));
+                for (int bb = 0; bb < 8; bb++) acc[a][bb] = 0.0f;
+            for (uint32_t ch = 0; ch < nchunk; ch++, it++) {
+                issue(it + 1);
+                asm volatile("cp.async.wait_group 1;\n" ::: "memory");
+                __syncthreads();
+                const float* xs = stage + (it & 1) * kPairStage;
+                const float* ys = xs + kPairT * kPairLd;
+                const int nq = (int)min((uint32_t)(kPairDC / 16), (d16 - ch * kPairDC) / 16);
+                for (int q = 0; q < nq; q++) {
+                    float xv[8], yv[8];
+#pragma unroll
+                    for (int a = 0; a < 8; a++) xv[a] = xs[(gi * 8 + a) * kPairLd + q * 16 + l];
+#pragma unroll
+                    for (int bb = 0; bb < 8; bb++) yv[bb] = ys[(gj * 8 + bb) * kPairLd + q * 16 + l];
+#pragma unroll
+                    for (int a = 0; a < 8; a++)
+#pragma unroll
+                        for (int bb = 0; bb < 8; bb++) {
+                            const float u = __fsub_rn(xv[a], yv[bb]);
+                            acc[a][bb] = __fadd_rn(acc[a][bb], __fmul_rn(u, u));
+                        }
+                }
+                __syncthreads();  // this stage is refilled by the issue two items on
             }
-            s = __fadd_rn(s, tail);
-            const uint32_t j = j0 + col;
-            const bool cand = j < k && j != i && start[j + 1] > start[j];
+            __syncthreads();  // the previous tile's reduction reads are done
+#pragma unroll
+            for (int a = 0; a < 8; a++)
+#pragma unroll
+                for (int bb = 0; bb < 8; bb++) red[((gi * 8 + a) * kPairT + gj * 8 + bb) * kPairRed + l] = acc[a][bb];
+            for (int e = tid; e < kPairT * 16; e += kPairThreads) {
+                const int r = e >> 4, t = e & 15;
+                yt[e] = (j0 + r < k && t < (int)dt) ? c[(size_t)(j0 + r) * d + d16 + t] : 0.0f;
+            }
+            __syncthreads();
+            const bool offdiag = J != I;
+            uint32_t bits = 0;
+#pragma unroll
+            for (int cc = 0; cc < 4; cc++) {
+                const int col = sub * 4 + cc;
+                const float* rp = red + (row * kPairT + col) * kPairRed;
+                float s = rp[0];
+#pragma unroll
+                for (int q = 1; q < 16; q++) s = __fadd_rn(s, rp[q]);
+                float tail = 0.0f;
+                for (uint32_t t = 0; t < dt; t++) {
+                    const float u = __fsub_rn(xt[row * 16 + t], yt[col * 16 + t]);
+                    tail = __fadd_rn(tail, __fmul_rn(u, u));
+                }
+                s = __fadd_rn(s, tail);
+                const uint32_t j = j0 + col;
+                const bool live_j = j < k && start[j + 1] > start[j];
+                if (ADJ) {
+                    const bool hit = live_i && live_j && j != i && __fsqrt_rn(s) <= radius;
+                    if (hit) bits |= 1u << col;
+                    if (hit && offdiag) atomicOr(&colbits[col], 1u << row);
+                } else if (s < INFINITY && i < k && j < k && j != i) {
+                    if (live_j) {
+                        const unsigned long long key = ((unsigned long long)__float_as_uint(s) << 32) | j;
+                        best = key < best ? key : best;
+                    }
+                    if (live_i && offdiag)
+                        atomicMin(&colkey[col], ((unsigned long long)__float_as_uint(s) << 32) | i);
+                }
+            }
             if (ADJ) {
-                if (cand && live_i && __fsqrt_rn(s) <= radius) bits |= 1u << col;
-            } else if (cand && s < INFINITY) {
-                const unsigned long long key = ((unsigned long long)__float_as_uint(s) << 32) | j;
-                best = key < best ? key : best;
+#pragma unroll
+                for (int o = 1; o < 8; o <<= 1) bits |= __shfl_xor_sync(0xffffffffu, bits, o);
+                if (sub == 0 && i < k) adj[(size_t)i * words + J] = bits;
+            }
+            __syncthreads();
+            if (offdiag && tid < kPairT && j0 + tid < k) {  // the column tile's rows, over this row tile
+                if (ADJ) adj[(size_t)(j0 + tid) * words + I] = colbits[tid];
+                else if (colkey[tid] != ~0ull) atomicMin(&near_key[j0 + tid], colkey[tid]);
+            }
+            if (tid < kPairT) {
+                colkey[tid] = ~0ull;
+                colbits[tid] = 0u;
             }
         }
-        if (ADJ) {
+        if (!ADJ) {
 #pragma unroll
-            for (int o = 1; o < 8; o <<= 1) bits |= __shfl_xor_sync(0xffffffffu, bits, o);
-            if (sub == 0 && i < k) adj[(size_t)i * words + jt] = bits;
+            for (int o = 1; o < 8; o <<= 1) {
+                const unsigned long long v = __shfl_xor_sync(0xffffffffu, best, o);
+                best = v < best ? v : best;
+            }
+            if (sub == 0 && i < k && best != ~0ull) atomicMin(&near_key[i], best);
         }
     }
-    if (!ADJ) {
-#pragma unroll
-        for (int o = 1; o < 8; o <<= 1) {
-            const unsigned long long v = __shfl_xor_sync(0xffffffffu, best, o);
-            best = v < best ? v : best;
-        }
-        if (sub == 0 && i < k) {
-            near_j[i] = best == ~0ull ? i : (uint32_t)best;
-            near_s[i] = best == ~0ull ? INFINITY : __uint_as_float((uint32_t)(best >> 32));
-        }
-    }
+    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+}
+
+// near_key -> (nearest centroid, squared distance), or (i, inf) without one.
+__global__ void k_rep_near_finish(const unsigned long long* __restrict__ near_key, uint32_t k,
+                                  uint32_t* __restrict__ near_j, float* __restrict__ near_s) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= k) return;
+    const unsigned long long key = near_key[i];
+    near_j[i] = key == ~0ull ? i : (uint32_t)key;
+    near_s[i] = key == ~0ull ? INFINITY : __uint_as_float((uint32_t)(key >> 32));
 }
 
 // ---- families ----------------------------------------------------------------
