@@ -23,7 +23,7 @@ LIB_PATH = os.path.join(_HERE, "libemb200.so")
 
 EMB200_F32, EMB200_I8, EMB200_U8 = 0, 1, 2
 PREC_FP32, PREC_BF16, PREC_BF16X1 = 0, 1, 2
-CENTROIDS_F32, CENTROIDS_I8 = 0, 8
+CENTROIDS_F32, CENTROIDS_I8, CENTROIDS_I16 = 0, 8, 16
 MATCH = {"avx512": 0, "avx2": 1, "portable": 2}
 _DTYPES = {np.dtype(np.float32): EMB200_F32, np.dtype(np.int8): EMB200_I8, np.dtype(np.uint8): EMB200_U8}
 PRECISIONS = {"fp32": PREC_FP32, "bf16": PREC_BF16, "bf16x1": PREC_BF16X1}
@@ -239,8 +239,8 @@ class B200Assigner:
     beside CpuAssigner (src/cpu.rs) and CpuI8Assigner (src/cpu_i8.rs).
 
     precision: "fp32" (SIMT), "bf16" (tcgen05, three-term split), "bf16x1".
-    centroid_bits: 0 (CpuAssigner semantics for every row type) or 8
-    (CpuI8Assigner(I8) semantics for i8 rows). match: which CpuAssigner SIMD
+    centroid_bits: 0 (CpuAssigner semantics for every row type), 8 or 16
+    (CpuI8Assigner(I8) / CpuI8Assigner(I16) semantics for i8 rows). match: which CpuAssigner SIMD
     kernel's rounding the labels and distances reproduce.
     """
 

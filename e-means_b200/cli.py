@@ -156,7 +156,8 @@ def cmd_int8(args, emb):
               f"{100.0 * q.clipped_fraction(x, assigner=exact):.4f}% of values clipped")
         f32_on_codes = train_with(codes, precision="fp32")
         row("  f32 search (exact on the codes)", lambda cfg: q.decode(f32_on_codes(cfg), assigner=exact))
-        print(f"{'  int16-centroid search':<46} {'(I16 centroid mode not built)':>31}")
+        i16 = train_with(codes, precision="fp32", centroid_bits=16)
+        row("  int16-centroid search (dp2a)", lambda cfg: q.decode(i16(cfg), assigner=exact))
         i8 = train_with(codes, precision="fp32", centroid_bits=8)
         row("  int8-centroid search (kind::i8, as faiss)", lambda cfg: q.decode(i8(cfg), assigner=exact))
     exact.close()

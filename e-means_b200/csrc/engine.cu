@@ -106,7 +106,9 @@ struct emb200_handle {
     CUtensorMap map_hi{}, map_lo{};  // TMA descriptors of c_hi / c_lo (128B swizzle, 64 x 128 boxes)
     bool maps_ok = false;
     DevBuf<int8_t> c8;   // I8 centroids (CpuI8Assigner)
-    DevBuf<long long> off8;  // I8 offsets: sum c8^2 (+ bias)
+    DevBuf<int16_t> c16; // I16 centroids: round(c * 2^ishift)
+    int ishift = 0;      // I16 scale exponent (src/cpu_i8.rs:97)
+    DevBuf<long long> off8;  // integer offsets: sum c8^2 or sum c16^2 (+ bias in score units)
     bool bias_set = false;
     double bias_absmax = 0.0;  // largest |bias| added since set_centroids (inf: unknown, device-computed)
     CUtensorMap map_c8{};      // TMA descriptor of c8 (128B swizzle, 128 x 256 boxes)
@@ -213,7 +215,8 @@ void bound_coefficients(int precision, int dtype, size_t d, bool packed, float* 
 }
 
 bool use_i8_mode(const emb200_handle* h, int dtype) {
-    return dtype == EMB200_I8 && h->opts.centroid_bits == EMB200_CENTROIDS_I8;
+    return dtype == EMB200_I8 &&
+           (h->opts.centroid_bits == EMB200_CENTROIDS_I8 || h->opts.centroid_bits == EMB200_CENTROIDS_I16);
 }
 
 
@@ -301,6 +304,17 @@ int prepare_centroids(emb200_handle* h) {
             h->map_c8_ok = true;
         }
     }
+    if (h->opts.centroid_bits == EMB200_CENTROIDS_I16) {
+        // The largest s <= 7 with d 128 (128 2^s) < 2^31 (src/cpu_i8.rs:96-98).
+        int s = 7;
+        while (s > 0 && ((uint64_t)h->d << (14 + s)) >= ((uint64_t)1 << 31)) s--;
+        h->ishift = s;
+        const size_t kp16 = (h->d + 31) / 32 * 32;
+        if (h->c16.ensure((size_t)k * kp16) || h->off8.ensure(k)) return fail(h, EMB200_ENOMEM, "i16 centroid allocation failed");
+        k_prep_i16<<<(unsigned)((k + 7) / 8), 256, 0, st>>>(h->c.p, k, d, (int)kp16, (float)(1u << s), h->c16.p,
+                                                            h->off8.p);
+        CKL();
+    }
     h->bias_set = false;
     h->bias_absmax = 0.0;
     return EMB200_OK;
@@ -312,8 +326,9 @@ int apply_bias(emb200_handle* h, const float* bias_dev) {
     const int k = (int)h->k;
     k_add_bias<<<(unsigned)((k + 255) / 256), 256, 0, st>>>(h->norms.p, bias_dev, k, h->bounds.p);
     CKL();
-    if (h->opts.centroid_bits == EMB200_CENTROIDS_I8) {
-        k_bias_i8<<<(unsigned)((k + 255) / 256), 256, 0, st>>>(h->off8.p, bias_dev, k);
+    if (h->opts.centroid_bits == EMB200_CENTROIDS_I8 || h->opts.centroid_bits == EMB200_CENTROIDS_I16) {
+        const double unit = h->opts.centroid_bits == EMB200_CENTROIDS_I16 ? std::ldexp(1.0, 2 * h->ishift) : 1.0;
+        k_bias_i8<<<(unsigned)((k + 255) / 256), 256, 0, st>>>(h->off8.p, bias_dev, k, unit);
         CKL();
     }
     h->bias_set = true;
@@ -328,7 +343,9 @@ int launch_i8_assign(emb200_handle* h, const int8_t* x, const uint32_t* gather, 
                      float* dist, cudaStream_t st, bool graph = false) {
     const int k = (int)h->k, d = (int)h->d;
     const size_t kp8 = (h->d + 127) / 128 * 128;
-    const bool tc = h->map_c8_ok && h->d <= 512 && h->bias_absmax <= 8.0e6;
+    const bool wide = h->opts.centroid_bits == EMB200_CENTROIDS_I16;
+    const bool tc = !wide && h->map_c8_ok && h->d <= 512 && h->bias_absmax <= 8.0e6;
+    const double inv_unit = wide ? std::ldexp(1.0, -2 * h->ishift) : 1.0;
     int nsplit = 1;
     const int target = tc ? h->sm_count : 2 * h->sm_count;
     const int row_tiles = (int)((m + 127) / 128);
@@ -377,14 +394,21 @@ int launch_i8_assign(emb200_handle* h, const int8_t* x, const uint32_t* gather, 
         CKL();
     } else {
         const int xvec = (d % 16 == 0 && ((uintptr_t)x & 15) == 0) ? 1 : 0;
-        k_assign_i8<<<dim3((unsigned)row_tiles, (unsigned)nsplit), 256, 0, st>>>(
-            x, gather, (int)m, d, h->c8.p, (int)kp8, h->off8.p, k, (long long*)h->part_s.p, h->part_i.p, xvec);
+        if (wide) {
+            k_assign_i8<true><<<dim3((unsigned)row_tiles, (unsigned)nsplit), 256, 0, st>>>(
+                x, gather, (int)m, d, h->c16.p, (int)((h->d + 31) / 32 * 32), h->off8.p, k, 2ll << h->ishift,
+                (long long*)h->part_s.p, h->part_i.p, xvec);
+        } else {
+            k_assign_i8<false><<<dim3((unsigned)row_tiles, (unsigned)nsplit), 256, 0, st>>>(
+                x, gather, (int)m, d, h->c8.p, (int)kp8, h->off8.p, k, 2ll, (long long*)h->part_s.p, h->part_i.p,
+                xvec);
+        }
         CKL();
     }
     if (!graph) CK(cudaEventRecord(h->evk1, st));
     h->stats.fast_kernel = tc ? 3 : 2;
     k_finish_i8<<<(unsigned)((m + 7) / 8), 256, 0, st>>>(x, gather, (int)m, d, (const long long*)h->part_s.p,
-                                                         h->part_i.p, nsplit, labels, dist);
+                                                         h->part_i.p, nsplit, labels, dist, inv_unit);
     CKL();
     if (tc && !graph) {  // the bounded waits gave up: redo the call with the exact dp4a kernel
         uint32_t err = 0;
@@ -400,11 +424,12 @@ int launch_i8_assign(emb200_handle* h, const int8_t* x, const uint32_t* gather, 
             const int ns = std::max(1, std::min((k + kI8BN - 1) / kI8BN, (2 * h->sm_count + row_tiles - 1) / row_tiles));
             if (h->part_s.ensure((size_t)ns * m * 2) || h->part_i.ensure((size_t)ns * m))
                 return fail(h, EMB200_ENOMEM, "scratch allocation failed for %zu rows", m);
-            k_assign_i8<<<dim3((unsigned)row_tiles, (unsigned)ns), 256, 0, st>>>(
-                x, gather, (int)m, d, h->c8.p, (int)kp8, h->off8.p, k, (long long*)h->part_s.p, h->part_i.p, xvec);
+            k_assign_i8<false><<<dim3((unsigned)row_tiles, (unsigned)ns), 256, 0, st>>>(
+                x, gather, (int)m, d, h->c8.p, (int)kp8, h->off8.p, k, 2ll, (long long*)h->part_s.p, h->part_i.p,
+                xvec);
             CKL();
             k_finish_i8<<<(unsigned)((m + 7) / 8), 256, 0, st>>>(x, gather, (int)m, d, (const long long*)h->part_s.p,
-                                                                 h->part_i.p, ns, labels, dist);
+                                                                 h->part_i.p, ns, labels, dist, 1.0);
             CKL();
         }
     }
@@ -775,7 +800,7 @@ int emb200_destroy(emb200_handle* h) {
     cudaSetDevice(h->device);
     if (h->stream) cudaStreamSynchronize(h->stream);
     h->c.release(); h->norms.release(); h->bias.release(); h->bounds.release();
-    h->c_hi.release(); h->c_lo.release(); h->c8.release(); h->off8.release();
+    h->c_hi.release(); h->c_lo.release(); h->c8.release(); h->c16.release(); h->off8.release();
     h->rows.release(); h->res_labels.release(); h->res_dist.release();
     h->stage.release(); h->st_labels.release(); h->st_dist.release();
     h->part_s.release(); h->part_i.release(); h->redo_rows.release(); h->counters.release();
@@ -810,7 +835,7 @@ const char* emb200_last_error(const emb200_handle* h) {
 int emb200_set_opts(emb200_handle* h, const emb200_opts* opts) {
     if (!h || !opts) return EMB200_EINVAL;
     if (opts->precision < 0 || opts->precision > 2 || opts->match_kernel < 0 || opts->match_kernel > 2 ||
-        (opts->centroid_bits != 0 && opts->centroid_bits != 8))
+        (opts->centroid_bits != 0 && opts->centroid_bits != 8 && opts->centroid_bits != 16))
         return fail(h, EMB200_EINVAL, "invalid options");
     bool rebuild = h->opts.centroid_bits != opts->centroid_bits || h->opts.precision != opts->precision;
     h->opts = *opts;
@@ -831,8 +856,11 @@ int emb200_name(emb200_handle* h, char* buf, size_t len) {
     const char* prec = h->opts.precision == EMB200_PREC_FP32 ? "FP32 SIMT"
                        : h->opts.precision == EMB200_PREC_BF16 ? "BF16x3 tcgen05" : "BF16 tcgen05";
     const char* match = h->opts.match_kernel == 0 ? "AVX-512" : h->opts.match_kernel == 1 ? "AVX2" : "portable";
-    snprintf(buf, len, "B200 fused assign (%s search, exact re-score in %s rounding%s), %s", prec, match,
-             h->opts.centroid_bits == 8 ? ", int8 centroids for i8 rows" : "", prop.name);
+    char ib[64] = "";
+    if (h->opts.centroid_bits == 8) snprintf(ib, sizeof ib, ", int8 centroids for i8 rows");
+    if (h->opts.centroid_bits == 16) snprintf(ib, sizeof ib, ", int16 centroids (1/%u unit) for i8 rows", 1u << h->ishift);
+    snprintf(buf, len, "B200 fused assign (%s search, exact re-score in %s rounding%s), %s", prec, match, ib,
+             prop.name);
     return EMB200_OK;
 }
 

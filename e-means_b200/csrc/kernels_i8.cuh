@@ -29,11 +29,34 @@ __global__ void k_prep_i8(const float* __restrict__ c, int k, int d, int kpad, i
     if (lane == 0) off[warp] = s;
 }
 
-// set_bias for I8 (src/cpu_i8.rs:112-117): off += (bias as f64).round() as i64 (saturating).
-__global__ void k_bias_i8(long long* __restrict__ off, const float* __restrict__ bias, int k) {
+// set_centroids for I16 (src/cpu_i8.rs:95-107): c16 = clamp(round half away(c *
+// 2^shift), -32768, 32767) (NaN -> 0), off_j = sum c16^2. Rows padded with zeros
+// to kpad elements (whole 32-element K steps of k_assign_i8<true>).
+__global__ void k_prep_i16(const float* __restrict__ c, int k, int d, int kpad, float scale,
+                           int16_t* __restrict__ c16, long long* __restrict__ off) {
+    int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    int lane = threadIdx.x & 31;
+    if (warp >= k) return;
+    long long s = 0;
+    for (int t = lane; t < kpad; t += 32) {
+        int v = 0;
+        if (t < d) {
+            float f = __fmul_rn(c[(size_t)warp * d + t], scale);
+            if (f == f) v = (int)fminf(fmaxf(roundf(f), -32768.0f), 32767.0f);
+        }
+        c16[(size_t)warp * kpad + t] = (int16_t)v;
+        s += (long long)v * v;
+    }
+    for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0) off[warp] = s;
+}
+
+// set_bias in integer mode (src/cpu_i8.rs:112-117): off += (bias as f64 * unit).round()
+// as i64 (saturating), unit = 2^(2 shift) score units per squared distance (1 for I8).
+__global__ void k_bias_i8(long long* __restrict__ off, const float* __restrict__ bias, int k, double unit) {
     int j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= k) return;
-    double v = round((double)bias[j]);
+    double v = round(__dmul_rn((double)bias[j], unit));
     long long iv;
     if (v != v) iv = 0;
     else if (v >= 9.2233720368547758e18) iv = 0x7fffffffffffffffll;
@@ -73,14 +96,38 @@ EMB_DEV void i8_load(int (&r)[4], const int8_t* __restrict__ base, const uint32_
     }
 }
 
+// 32 i16 centroid elements of row (row0 + t/2) from element kb0 + 16 (t&1): eight
+// words of two elements each (rows are padded to whole 32-element steps).
+EMB_DEV void i16_load(int (&r)[8], const int16_t* __restrict__ base, int row0, int nrows, int kpad, int kb0) {
+    int t = threadIdx.x;
+    int row = row0 + (t >> 1);
+    if (row >= nrows) {
+#pragma unroll
+        for (int w = 0; w < 8; w++) r[w] = 0;
+        return;
+    }
+    const int4* p = reinterpret_cast<const int4*>(base + (size_t)row * kpad + kb0 + (t & 1) * 16);
+    int4 v0 = p[0], v1 = p[1];
+    r[0] = v0.x; r[1] = v0.y; r[2] = v0.z; r[3] = v0.w;
+    r[4] = v1.x; r[5] = v1.y; r[6] = v1.z; r[7] = v1.w;
+}
+
 // Grid (ceil(m/128), nsplit). Partial top-1 per (split, row): exact int64 score
 // and index; lowest index wins ties within and across threads.
+// WIDE = false: I8 centroids, score off_j - 2 (x . c8) by dp4a.
+// WIDE = true : I16 centroids, score off_j - mult (x . c16) by dp2a (two 16-bit
+//               centroid elements times two 8-bit row elements per instruction);
+//               the shift keeps x . c16 inside an int32 (src/cpu_i8.rs:96-97).
+template <bool WIDE>
 __global__ void __launch_bounds__(256, 1)
 k_assign_i8(const int8_t* __restrict__ x, const uint32_t* __restrict__ gather, int m, int d,
-            const int8_t* __restrict__ c8, int kpad, const long long* __restrict__ off, int k,
+            const void* __restrict__ cq, int kpad, const long long* __restrict__ off, int k, long long mult,
             long long* __restrict__ part_s, uint32_t* __restrict__ part_i, int xvec) {
+    constexpr int BW = WIDE ? 2 * kI8BKW : kI8BKW;  // centroid words per 32-element step
     __shared__ __align__(16) int As[2][kI8BKW][kI8BM];
-    __shared__ __align__(16) int Bs[2][kI8BKW][kI8BN];
+    __shared__ __align__(16) int Bs[2][BW][kI8BN];
+    const int8_t* c8 = static_cast<const int8_t*>(cq);
+    const int16_t* c16 = static_cast<const int16_t*>(cq);
     const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
     const int row0 = blockIdx.x * kI8BM;
     const int nsplit = gridDim.y;
@@ -100,46 +147,58 @@ k_assign_i8(const int8_t* __restrict__ x, const uint32_t* __restrict__ gather, i
         for (int i = 0; i < 8; i++)
 #pragma unroll
             for (int j = 0; j < 8; j++) acc[i][j] = 0;
-        int ra[4], rb[4];
-        i8_load(ra, x, gather, row0, m, d, d, 0, xvec);
-        i8_load(rb, c8, nullptr, col0, k, kpad, kpad, 0, true);
-        __syncthreads();
-        {
-            int r = tid >> 1, w0 = (tid & 1) * 4;
+        int ra[4], rb[WIDE ? 8 : 4];
+        auto load_b = [&](int kb0) {
+            if constexpr (WIDE) i16_load(rb, c16, col0, k, kpad, kb0);
+            else i8_load(rb, c8, nullptr, col0, k, kpad, kpad, kb0, true);
+        };
+        auto store = [&](int buf) {
+            const int r = tid >> 1, w0 = (tid & 1) * 4;
 #pragma unroll
-            for (int w = 0; w < 4; w++) {
-                As[0][w0 + w][r] = ra[w];
-                Bs[0][w0 + w][r] = rb[w];
-            }
-        }
+            for (int w = 0; w < 4; w++) As[buf][w0 + w][r] = ra[w];
+#pragma unroll
+            for (int w = 0; w < (WIDE ? 8 : 4); w++) Bs[buf][(tid & 1) * (WIDE ? 8 : 4) + w][r] = rb[w];
+        };
+        i8_load(ra, x, gather, row0, m, d, d, 0, xvec);
+        load_b(0);
+        __syncthreads();
+        store(0);
         __syncthreads();
         for (int kt = 0; kt < nk; kt++) {
             const int buf = kt & 1;
             if (kt + 1 < nk) {
                 i8_load(ra, x, gather, row0, m, d, d, (kt + 1) * 32, xvec);
-                i8_load(rb, c8, nullptr, col0, k, kpad, kpad, (kt + 1) * 32, true);
+                load_b((kt + 1) * 32);
             }
 #pragma unroll
             for (int w = 0; w < kI8BKW; w++) {
                 int4 a0 = *reinterpret_cast<const int4*>(&As[buf][w][ty * 4]);
                 int4 a1 = *reinterpret_cast<const int4*>(&As[buf][w][64 + ty * 4]);
-                int4 b0 = *reinterpret_cast<const int4*>(&Bs[buf][w][tx * 4]);
-                int4 b1 = *reinterpret_cast<const int4*>(&Bs[buf][w][64 + tx * 4]);
                 int a[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
-                int b[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
+                if constexpr (WIDE) {
+                    // word 2w: elements 4w, 4w+1; word 2w+1: elements 4w+2, 4w+3
+                    int4 l0 = *reinterpret_cast<const int4*>(&Bs[buf][2 * w][tx * 4]);
+                    int4 l1 = *reinterpret_cast<const int4*>(&Bs[buf][2 * w][64 + tx * 4]);
+                    int4 h0 = *reinterpret_cast<const int4*>(&Bs[buf][2 * w + 1][tx * 4]);
+                    int4 h1 = *reinterpret_cast<const int4*>(&Bs[buf][2 * w + 1][64 + tx * 4]);
+                    int bl[8] = {l0.x, l0.y, l0.z, l0.w, l1.x, l1.y, l1.z, l1.w};
+                    int bh[8] = {h0.x, h0.y, h0.z, h0.w, h1.x, h1.y, h1.z, h1.w};
 #pragma unroll
-                for (int i = 0; i < 8; i++)
+                    for (int i = 0; i < 8; i++)
 #pragma unroll
-                    for (int j = 0; j < 8; j++) acc[i][j] = __dp4a(a[i], b[j], acc[i][j]);
-            }
-            if (kt + 1 < nk) {
-                int r = tid >> 1, w0 = (tid & 1) * 4;
+                        for (int j = 0; j < 8; j++)
+                            acc[i][j] = __dp2a_hi(bh[j], a[i], __dp2a_lo(bl[j], a[i], acc[i][j]));
+                } else {
+                    int4 b0 = *reinterpret_cast<const int4*>(&Bs[buf][w][tx * 4]);
+                    int4 b1 = *reinterpret_cast<const int4*>(&Bs[buf][w][64 + tx * 4]);
+                    int b[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
 #pragma unroll
-                for (int w = 0; w < 4; w++) {
-                    As[buf ^ 1][w0 + w][r] = ra[w];
-                    Bs[buf ^ 1][w0 + w][r] = rb[w];
+                    for (int i = 0; i < 8; i++)
+#pragma unroll
+                        for (int j = 0; j < 8; j++) acc[i][j] = __dp4a(a[i], b[j], acc[i][j]);
                 }
             }
+            if (kt + 1 < nk) store(buf ^ 1);
             __syncthreads();
         }
 #pragma unroll
@@ -149,7 +208,7 @@ k_assign_i8(const int8_t* __restrict__ x, const uint32_t* __restrict__ gather, i
                 long long o = off[col];
 #pragma unroll
                 for (int i = 0; i < 8; i++) {
-                    long long s = o - 2ll * (long long)acc[i][j];
+                    long long s = o - mult * (long long)acc[i][j];
                     if (s < best[i]) {
                         best[i] = s;
                         bidx[i] = (uint32_t)col;
@@ -183,11 +242,12 @@ k_assign_i8(const int8_t* __restrict__ x, const uint32_t* __restrict__ gather, i
     }
 }
 
-// Merge the split partials, dist = max(|x|^2 + best, 0) computed in f64 and
-// rounded to f32 (src/cpu_i8.rs:183-186). One warp per row.
+// Merge the split partials, dist = max(|x|^2 + best * inv_unit, 0) computed in
+// f64 and rounded to f32 (src/cpu_i8.rs:183-186; inv_unit = 2^(-2 shift), 1 for
+// I8). One warp per row.
 __global__ void k_finish_i8(const int8_t* __restrict__ x, const uint32_t* __restrict__ gather, int m, int d,
                             const long long* __restrict__ part_s, const uint32_t* __restrict__ part_i, int nsplit,
-                            uint32_t* __restrict__ labels, float* __restrict__ dist) {
+                            uint32_t* __restrict__ labels, float* __restrict__ dist, double inv_unit) {
     const int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (row >= m) return;
@@ -208,7 +268,7 @@ __global__ void k_finish_i8(const int8_t* __restrict__ x, const uint32_t* __rest
         }
     }
     labels[row] = l;
-    dist[row] = (float)fmax((double)nrm + (double)b, 0.0);
+    dist[row] = (float)fmax(__dadd_rn((double)nrm, __dmul_rn((double)b, inv_unit)), 0.0);
 }
 
 }  // namespace emb

@@ -52,6 +52,8 @@ typedef struct emb200_handle emb200_handle;
 /* Centroid representation for i8 rows (src/cpu_i8.rs:21-25). */
 #define EMB200_CENTROIDS_F32 0 /* CpuAssigner semantics: rows widened to f32 */
 #define EMB200_CENTROIDS_I8 8  /* CpuI8Assigner(CentroidBits::I8): centroids rounded to i8, exact integer ranking */
+#define EMB200_CENTROIDS_I16 16 /* CpuI8Assigner(CentroidBits::I16): centroids rounded to 1/2^s of a unit
+                                   (s <= 7 from d, src/cpu_i8.rs:95-107), exact integer ranking */
 
 /* Which CpuAssigner kernel's f32 rounding the exact re-score reproduces
  * (src/cpu.rs:13-33: AVX-512 on CPUs that have it, else AVX2+FMA, else portable). */

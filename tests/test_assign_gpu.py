@@ -182,6 +182,35 @@ def test_i8_mode_integer_exact(orc, assigners, shape):
         assert np.array_equal(lab, rl) and same_f32(dist, rd)
 
 
+@pytest.mark.parametrize("shape", SHAPES_I8 + [(300, 200, 2048), (50, 40, 40000 // 2)])
+def test_i16_mode_integer_exact(orc, assigners, shape):
+    # CpuI8Assigner(I16) (src/cpu_i8.rs:95-107): centroids in 1/2^s units, s from d
+    # (d = 2048 and 20000 take smaller shifts); labels and dists bit for bit.
+    n, k, d = shape
+    x, ci = lcg_i8(n * d, 1).reshape(n, d), lcg_i8(k * d, 2).reshape(k, d)
+    a = assigners("fp32", 16)
+    for c in (ci.astype(np.float32), ci.astype(np.float32) * np.float32(0.37) + np.float32(0.5)):
+        a.set_centroids(c)
+        lab, dist = a.assign(x)
+        assert a.stats()["fast_kernel"] == 2
+        rl, rd = orc.i8_assign(x, c, bits=16)
+        assert np.array_equal(lab, rl) and same_f32(dist, rd), shape
+
+
+def test_i16_mode_with_bias(orc, assigners):
+    rng = np.random.default_rng(6)
+    x = rng.integers(-128, 128, (600, 96), dtype=np.int8)
+    c = (rng.standard_normal((333, 96)) * 50).astype(np.float32)
+    bias = rng.uniform(0, 5000, 333).astype(np.float32)
+    a = assigners("fp32", 16)
+    a.set_centroids(c)
+    a.set_bias(bias)
+    lab, dist = a.assign(x)
+    rl, rd = orc.i8_assign(x, c, bits=16, bias=bias)
+    assert np.array_equal(lab, rl) and same_f32(dist, rd)
+    assert "int16 centroids (1/128 unit)" in a.name()
+
+
 def test_i8_mode_with_bias(orc, assigners):
     rng = np.random.default_rng(5)
     x = rng.integers(-128, 128, (600, 96), dtype=np.int8)

@@ -88,6 +88,9 @@ def test_int8_rows_both_semantics(emb, orc):
     # CpuI8Assigner(I8): integer search (src/cpu_i8.rs), f32 sums and EMA.
     out, ref, _ = run_both(emb, orc, codes, 200, "fp32", centroid_bits=8, assigner="i8", nepochs=3.0)
     check_same(out, ref)
+    # CpuI8Assigner(I16): centroids in 1/128 units, exact integer search.
+    out, ref, _ = run_both(emb, orc, codes, 200, "fp32", centroid_bits=16, assigner="i16", nepochs=3.0)
+    check_same(out, ref)
     # CpuAssigner on i8 rows: rows widened to f32.
     out, ref, _ = run_both(emb, orc, codes, 200, "bf16", nepochs=3.0)
     check_same(out, ref)
