@@ -447,9 +447,11 @@ def run_report(args):
             "config": {"workload": f"report of {n} x {d} embedding rows, k={K} trained centroids",
                        "live_clusters": live, "families": len(r.families)},
             "clocks": clock.summary(),
-            "pair_pass": {"element_ops": pairs, "note": "k^2 d (c_i - c_j)^2 terms per pass, SIMT f32 in the "
-                                                        "reference's sqdist rounding (no tensor cores: the order of "
-                                                        "roundings is the result)"},
+            "pair_pass": {"element_ops": pairs, "note": "k^2 d (c_i - c_j)^2 terms per pass as the reference "
+                                                        "computes them; the device computes each unordered pair once "
+                                                        "(the rounding is symmetric), SIMT f32 in the reference's "
+                                                        "sqdist rounding (no tensor cores: the order of roundings is "
+                                                        "the result)"},
             "e2e": {"value": n / te, "unit": "rows/s", "h2d_bytes_per_step": n * 8 + K * d * 4,
                     "d2h_bytes_per_step": n * 8 + K * 48 + live * 4}}
     if not args.no_cpu:

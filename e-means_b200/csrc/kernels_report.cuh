@@ -379,15 +379,13 @@ __global__ void k_rep_z(const uint32_t* __restrict__ labels, const float* __rest
 // ---- exact pair pass ---------------------------------------------------------
 
 constexpr int kPairT = 32;         // rows and columns per tile
-constexpr int kPairThreads = 256;  // 16 dimension lanes x 16 groups of 8 x 8 pairs
+constexpr int kPairThreads = 256;  // each thread: rows {r, r+16} x columns {c, c+16} of the tile
 constexpr int kPairDC = 64;        // dimensions per staged chunk
 constexpr int kPairLd = kPairDC + 4;  // row pitch of a staged chunk (16-byte rows for cp.async)
-constexpr int kPairRed = 17;       // padded lane stride of the reduction buffer
 constexpr int kPairStage = 2 * kPairT * kPairLd;  // floats of one stage (row tile chunk + column tile chunk)
 
 constexpr size_t pair_smem_bytes() {
-    return sizeof(float) * (2 * kPairStage + kPairT * kPairT * kPairRed + 2 * kPairT * 16) +
-           kPairT * (sizeof(unsigned long long) + sizeof(uint32_t));
+    return sizeof(float) * (2 * kPairStage + 2 * kPairT * 16) + kPairT * (sizeof(unsigned long long) + sizeof(uint32_t));
 }
 
 __device__ __forceinline__ void pair_cp16(float* smem, const float* gmem) {
@@ -403,30 +401,29 @@ __device__ __forceinline__ void pair_cp4(float* smem, const float* gmem) {
 // (src/report.rs:104-114): lane l of 16 accumulates (c_i[t] - c_j[t])^2 over
 // t = l, l + 16, ... below d16 = d - d % 16 (separate subtract, multiply and
 // add), the lanes are summed in order, then the tail (t >= d16, summed in
-// order) is added. The result is the same for (i, j) and (j, i) (x - y and
-// y - x square alike), so only tiles J >= I are computed; CTA b takes row tiles
-// b and T-1-b, which balances the triangle. Dimension chunks of both tiles are
-// double-buffered by cp.async.
+// order) is added. A thread keeps all 16 lane accumulators of its 4 pairs, so
+// the ordered lane sum stays in registers. The result is the same for (i, j)
+// and (j, i) (x - y and y - x square alike), so only tiles J >= I are
+// computed; CTA b takes row tiles b and T-1-b, which balances the triangle.
+// Dimension chunks of both tiles are double-buffered by cp.async.
 //   NEAREST (ADJ = false): near_key[i] = min over live j != i with s < inf of
 //   (bits of s, j), by 64-bit atomicMin (first j of the least s, as the
 //   reference's strict < scan); the host initialises it to all ones.
 //   ADJ: bit j of row i of the adjacency is set when both are live, j != i and
 //   sqrt(s) <= radius; every word of every row is written.
 template <bool ADJ>
-__global__ void __launch_bounds__(kPairThreads) k_rep_pairs(const float* __restrict__ c, uint32_t k, uint32_t d,
-                                                            const uint32_t* __restrict__ start,
-                                                            unsigned long long* __restrict__ near_key,
-                                                            const RepScalars* __restrict__ sc,
-                                                            uint32_t* __restrict__ adj, uint32_t words) {
+__global__ void __launch_bounds__(kPairThreads, 2) k_rep_pairs(const float* __restrict__ c, uint32_t k, uint32_t d,
+                                                               const uint32_t* __restrict__ start,
+                                                               unsigned long long* __restrict__ near_key,
+                                                               const RepScalars* __restrict__ sc,
+                                                               uint32_t* __restrict__ adj, uint32_t words) {
     extern __shared__ __align__(16) float pair_sm[];
-    float* stage = pair_sm;                      // 2 stages x (row chunk, column chunk)
-    float* red = stage + 2 * kPairStage;         // [32 x 32 pairs][16 lanes]
-    float* xt = red + kPairT * kPairT * kPairRed;  // row tile tails [32][16]
-    float* yt = xt + kPairT * 16;                  // column tile tails
+    float* stage = pair_sm;                  // 2 stages x (row chunk, column chunk)
+    float* xt = stage + 2 * kPairStage;      // row tile tails [32][16]
+    float* yt = xt + kPairT * 16;            // column tile tails
     unsigned long long* colkey = reinterpret_cast<unsigned long long*>(yt + kPairT * 16);
     uint32_t* colbits = reinterpret_cast<uint32_t*>(colkey + kPairT);
-    const int tid = threadIdx.x, l = tid & 15, g = tid >> 4, gi = g >> 2, gj = g & 3;
-    const int row = tid >> 3, sub = tid & 7;  // reduction: row, and columns sub*4 .. sub*4+3
+    const int tid = threadIdx.x, tr = tid >> 4, tc = tid & 15;  // rows tr, tr+16; columns tc, tc+16
     const uint32_t T = (k + kPairT - 1) / kPairT;
     const uint32_t d16 = d / 16 * 16, dt = d - d16;
     const uint32_t nchunk = (d16 + kPairDC - 1) / kPairDC;
@@ -434,7 +431,6 @@ __global__ void __launch_bounds__(kPairThreads) k_rep_pairs(const float* __restr
     const float radius = ADJ ? sc->radius : 0.0f;
     const uint32_t b = blockIdx.x, I0 = b, I1 = T - 1 - b;
     const uint32_t n0 = (T - I0) * nchunk, n1 = I1 > I0 ? (T - I1) * nchunk : 0;
-    // item it -> (row tile, column tile, first dimension), in processing order
     auto coords = [&](uint32_t it, uint32_t& I, uint32_t& J, uint32_t& dc0) {
         const uint32_t base = it < n0 ? 0 : n0;
         I = it < n0 ? I0 : I1;
@@ -475,9 +471,11 @@ __global__ void __launch_bounds__(kPairThreads) k_rep_pairs(const float* __restr
     for (int sd = 0; sd < 2; sd++) {
         const uint32_t I = sd ? I1 : I0;
         if (sd == 1 && I1 <= I0) break;
-        const uint32_t i0 = I * kPairT, i = i0 + row;
-        const bool live_i = i < k && start[i + 1] > start[i];
-        unsigned long long best = ~0ull;
+        const uint32_t i0 = I * kPairT;
+        const uint32_t ia = i0 + tr, ib = i0 + tr + 16;
+        const bool live_a = ia < k && start[ia + 1] > start[ia];
+        const bool live_b = ib < k && start[ib + 1] > start[ib];
+        unsigned long long best_a = ~0ull, best_b = ~0ull;
         __syncthreads();  // the previous row tile's tails are no longer read
         for (int e = tid; e < kPairT * 16; e += kPairThreads) {
             const int r = e >> 4, t = e & 15;
@@ -485,11 +483,13 @@ __global__ void __launch_bounds__(kPairThreads) k_rep_pairs(const float* __restr
         }
         for (uint32_t J = I; J < T; J++) {
             const uint32_t j0 = J * kPairT;
-            float acc[8][8];
+            float acc[2][2][16];
 #pragma unroll
-            for (int a = 0; a < 8; a++)
+            for (int a = 0; a < 2; a++)
 #pragma unroll
-                for (int bb = 0; bb < 8; bb++) acc[a][bb] = 0.0f;
+                for (int bb = 0; bb < 2; bb++)
+#pragma unroll
+                    for (int l = 0; l < 16; l++) acc[a][bb][l] = 0.0f;
             for (uint32_t ch = 0; ch < nchunk; ch++, it++) {
                 issue(it + 1);
                 asm volatile("cp.async.wait_group 1;\n" ::: "memory");
@@ -498,65 +498,79 @@ __global__ void __launch_bounds__(kPairThreads) k_rep_pairs(const float* __restr
                 const float* ys = xs + kPairT * kPairLd;
                 const int nq = (int)min((uint32_t)(kPairDC / 16), (d16 - ch * kPairDC) / 16);
                 for (int q = 0; q < nq; q++) {
-                    float xv[8], yv[8];
 #pragma unroll
-                    for (int a = 0; a < 8; a++) xv[a] = xs[(gi * 8 + a) * kPairLd + q * 16 + l];
+                    for (int g4 = 0; g4 < 4; g4++) {
+                        const int off = q * 16 + g4 * 4;
+                        const float4 x0 = *reinterpret_cast<const float4*>(xs + tr * kPairLd + off);
+                        const float4 x1 = *reinterpret_cast<const float4*>(xs + (tr + 16) * kPairLd + off);
+                        const float4 y0 = *reinterpret_cast<const float4*>(ys + tc * kPairLd + off);
+                        const float4 y1 = *reinterpret_cast<const float4*>(ys + (tc + 16) * kPairLd + off);
+                        const float xv[2][4] = {{x0.x, x0.y, x0.z, x0.w}, {x1.x, x1.y, x1.z, x1.w}};
+                        const float yv[2][4] = {{y0.x, y0.y, y0.z, y0.w}, {y1.x, y1.y, y1.z, y1.w}};
 #pragma unroll
-                    for (int bb = 0; bb < 8; bb++) yv[bb] = ys[(gj * 8 + bb) * kPairLd + q * 16 + l];
+                        for (int a = 0; a < 2; a++)
 #pragma unroll
-                    for (int a = 0; a < 8; a++)
+                            for (int bb = 0; bb < 2; bb++)
 #pragma unroll
-                        for (int bb = 0; bb < 8; bb++) {
-                            const float u = __fsub_rn(xv[a], yv[bb]);
-                            acc[a][bb] = __fadd_rn(acc[a][bb], __fmul_rn(u, u));
-                        }
+                                for (int i = 0; i < 4; i++) {
+                                    const float u = __fsub_rn(xv[a][i], yv[bb][i]);
+                                    acc[a][bb][g4 * 4 + i] = __fadd_rn(acc[a][bb][g4 * 4 + i], __fmul_rn(u, u));
+                                }
+                    }
                 }
                 __syncthreads();  // this stage is refilled by the issue two items on
             }
-            __syncthreads();  // the previous tile's reduction reads are done
-#pragma unroll
-            for (int a = 0; a < 8; a++)
-#pragma unroll
-                for (int bb = 0; bb < 8; bb++) red[((gi * 8 + a) * kPairT + gj * 8 + bb) * kPairRed + l] = acc[a][bb];
             for (int e = tid; e < kPairT * 16; e += kPairThreads) {
                 const int r = e >> 4, t = e & 15;
                 yt[e] = (j0 + r < k && t < (int)dt) ? c[(size_t)(j0 + r) * d + d16 + t] : 0.0f;
             }
             __syncthreads();
             const bool offdiag = J != I;
-            uint32_t bits = 0;
+            uint32_t bits_a = 0, bits_b = 0;
 #pragma unroll
-            for (int cc = 0; cc < 4; cc++) {
-                const int col = sub * 4 + cc;
-                const float* rp = red + (row * kPairT + col) * kPairRed;
-                float s = rp[0];
+            for (int a = 0; a < 2; a++) {
+                const int row = tr + 16 * a;
+                const uint32_t i = i0 + row;
+                const bool live_i = a ? live_b : live_a;
 #pragma unroll
-                for (int q = 1; q < 16; q++) s = __fadd_rn(s, rp[q]);
-                float tail = 0.0f;
-                for (uint32_t t = 0; t < dt; t++) {
-                    const float u = __fsub_rn(xt[row * 16 + t], yt[col * 16 + t]);
-                    tail = __fadd_rn(tail, __fmul_rn(u, u));
-                }
-                s = __fadd_rn(s, tail);
-                const uint32_t j = j0 + col;
-                const bool live_j = j < k && start[j + 1] > start[j];
-                if (ADJ) {
-                    const bool hit = live_i && live_j && j != i && __fsqrt_rn(s) <= radius;
-                    if (hit) bits |= 1u << col;
-                    if (hit && offdiag) atomicOr(&colbits[col], 1u << row);
-                } else if (s < INFINITY && i < k && j < k && j != i) {
-                    if (live_j) {
-                        const unsigned long long key = ((unsigned long long)__float_as_uint(s) << 32) | j;
-                        best = key < best ? key : best;
+                for (int bb = 0; bb < 2; bb++) {
+                    const int col = tc + 16 * bb;
+                    float s = acc[a][bb][0];
+#pragma unroll
+                    for (int l = 1; l < 16; l++) s = __fadd_rn(s, acc[a][bb][l]);
+                    float tail = 0.0f;
+                    for (uint32_t t = 0; t < dt; t++) {
+                        const float u = __fsub_rn(xt[row * 16 + t], yt[col * 16 + t]);
+                        tail = __fadd_rn(tail, __fmul_rn(u, u));
                     }
-                    if (live_i && offdiag)
-                        atomicMin(&colkey[col], ((unsigned long long)__float_as_uint(s) << 32) | i);
+                    s = __fadd_rn(s, tail);
+                    const uint32_t j = j0 + col;
+                    const bool live_j = j < k && start[j + 1] > start[j];
+                    if (ADJ) {
+                        const bool hit = live_i && live_j && j != i && __fsqrt_rn(s) <= radius;
+                        if (hit) (a ? bits_b : bits_a) |= 1u << col;
+                        if (hit && offdiag) atomicOr(&colbits[col], 1u << row);
+                    } else if (s < INFINITY && i < k && j < k && j != i) {
+                        if (live_j) {
+                            const unsigned long long key = ((unsigned long long)__float_as_uint(s) << 32) | j;
+                            unsigned long long& best = a ? best_b : best_a;
+                            best = key < best ? key : best;
+                        }
+                        if (live_i && offdiag)
+                            atomicMin(&colkey[col], ((unsigned long long)__float_as_uint(s) << 32) | i);
+                    }
                 }
             }
-            if (ADJ) {
+            if (ADJ) {  // the 16 lanes of a half-warp hold one row pair: OR their bits
 #pragma unroll
-                for (int o = 1; o < 8; o <<= 1) bits |= __shfl_xor_sync(0xffffffffu, bits, o);
-                if (sub == 0 && i < k) adj[(size_t)i * words + J] = bits;
+                for (int o = 1; o < 16; o <<= 1) {
+                    bits_a |= __shfl_xor_sync(0xffffffffu, bits_a, o);
+                    bits_b |= __shfl_xor_sync(0xffffffffu, bits_b, o);
+                }
+                if (tc == 0) {
+                    if (ia < k) adj[(size_t)ia * words + J] = bits_a;
+                    if (ib < k) adj[(size_t)ib * words + J] = bits_b;
+                }
             }
             __syncthreads();
             if (offdiag && tid < kPairT && j0 + tid < k) {  // the column tile's rows, over this row tile
@@ -570,11 +584,16 @@ __global__ void __launch_bounds__(kPairThreads) k_rep_pairs(const float* __restr
         }
         if (!ADJ) {
 #pragma unroll
-            for (int o = 1; o < 8; o <<= 1) {
-                const unsigned long long v = __shfl_xor_sync(0xffffffffu, best, o);
-                best = v < best ? v : best;
+            for (int o = 1; o < 16; o <<= 1) {
+                const unsigned long long va = __shfl_xor_sync(0xffffffffu, best_a, o);
+                const unsigned long long vb = __shfl_xor_sync(0xffffffffu, best_b, o);
+                best_a = va < best_a ? va : best_a;
+                best_b = vb < best_b ? vb : best_b;
             }
-            if (sub == 0 && i < k && best != ~0ull) atomicMin(&near_key[i], best);
+            if (tc == 0) {
+                if (ia < k && best_a != ~0ull) atomicMin(&near_key[ia], best_a);
+                if (ib < k && best_b != ~0ull) atomicMin(&near_key[ib], best_b);
+            }
         }
     }
     asm volatile("cp.async.wait_group 0;\n" ::: "memory");
