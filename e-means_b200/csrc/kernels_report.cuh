@@ -620,17 +620,31 @@ __global__ void k_rep_order_keys(const uint32_t* __restrict__ start, uint32_t k,
 
 // Greedy families (src/report.rs:198-216) in one CTA: the first unassigned
 // cluster in size order leads a new family of every unassigned live cluster
-// within the radius (the adjacency row) and itself.
+// within the radius (the adjacency row) and itself. The assigned bitset lives in
+// shared memory; with TABLES, so do the size order and the cluster sizes, which
+// leaves one global read (the leader's adjacency row) on each leader's path.
+// Dynamic shared memory: words x 4 bytes, plus 2 x k x 4 bytes with TABLES.
+template <bool TABLES>
 __global__ void __launch_bounds__(1024) k_rep_families(const unsigned long long* __restrict__ order, uint32_t live,
-                                                       const uint32_t* __restrict__ adj, uint32_t words,
+                                                       uint32_t k, const uint32_t* __restrict__ adj, uint32_t words,
                                                        const uint32_t* __restrict__ start,
-                                                       uint32_t* __restrict__ assigned, uint32_t* __restrict__ fam_of,
-                                                       uint32_t* __restrict__ fam_lead,
+                                                       uint32_t* __restrict__ fam_of, uint32_t* __restrict__ fam_lead,
                                                        unsigned long long* __restrict__ fam_size,
                                                        uint32_t* __restrict__ nfam) {
+    extern __shared__ __align__(16) uint32_t fam_sm[];
+    uint32_t* assigned = fam_sm;                       // [words]
+    uint32_t* ord = fam_sm + words;                    // TABLES: [live] cluster ids in size order
+    uint32_t* size = ord + (TABLES ? k : 0);           // TABLES: [k] cluster sizes
     __shared__ uint32_t s_q;
     __shared__ unsigned long long s_part[32];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    for (uint32_t w = tid; w < words; w += 1024) assigned[w] = 0u;
+    if (TABLES) {
+        for (uint32_t q = tid; q < live; q += 1024) ord[q] = (uint32_t)order[q];
+        for (uint32_t j = tid; j < k; j += 1024) size[j] = start[j + 1] - start[j];
+    }
+    auto order_at = [&](uint32_t q) { return TABLES ? ord[q] : (uint32_t)order[q]; };
+    auto size_of = [&](uint32_t j) { return TABLES ? size[j] : start[j + 1] - start[j]; };
     uint32_t p = 0, F = 0;
     for (;;) {
         if (tid == 0) s_q = 0xffffffffu;
@@ -638,7 +652,7 @@ __global__ void __launch_bounds__(1024) k_rep_families(const unsigned long long*
         for (uint32_t b0 = p; b0 < live; b0 += 1024) {
             const uint32_t q = b0 + tid;
             if (q < live) {
-                const uint32_t j = (uint32_t)order[q];
+                const uint32_t j = order_at(q);
                 if (!((assigned[j >> 5] >> (j & 31)) & 1u)) atomicMin(&s_q, q);
             }
             __syncthreads();
@@ -648,7 +662,7 @@ __global__ void __launch_bounds__(1024) k_rep_families(const unsigned long long*
         }
         const uint32_t q = s_q;
         if (q == 0xffffffffu) break;
-        const uint32_t lead = (uint32_t)order[q];
+        const uint32_t lead = order_at(q);
         p = q + 1;
         const uint32_t* arow = adj + (size_t)lead * words;
         unsigned long long sz = 0;
@@ -662,7 +676,7 @@ __global__ void __launch_bounds__(1024) k_rep_families(const unsigned long long*
                     m &= m - 1;
                     const uint32_t j = w * 32 + b;
                     fam_of[j] = F;
-                    sz += start[j + 1] - start[j];
+                    sz += size_of(j);
                 }
             }
         }

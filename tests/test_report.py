@@ -95,7 +95,7 @@ def _synthetic(n, k, d, seed, empty=0.1, dup=0.0):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("n,k,d", [(0, 5, 3), (1, 1, 1), (7, 3, 16), (500, 40, 15), (3000, 64, 37),
-                                   (20000, 200, 128), (50000, 1000, 8), (4000, 33, 200)])
+                                   (20000, 200, 128), (50000, 1000, 8), (4000, 33, 200), (60000, 30000, 8)])
 def test_report_matches_oracle(emb, orc, n, k, d):
     labels, sq, c = _synthetic(n, k, d, seed=n + k + d, dup=0.05)
     r = emb.report(labels, sq, c, d)
