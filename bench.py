@@ -345,7 +345,7 @@ def run_c3(args):
     from oracle import oracle as orc
 
     emb = load_package()
-    n = args.rows if args.rows != N_ROWS else 2_000_000
+    n = args.rows if args.rows != 1_000_000 else 2_000_000  # --rows: fewer rows for profiling captures
     x = emb.datasets.embeddings(n, 512, latent=64, seed=0)
     a = emb.B200Assigner(0, precision="fp32", centroid_bits=8)
     # f32 rows resident, then Int8Quantizer::fit and encode on the device (faiss calibration)

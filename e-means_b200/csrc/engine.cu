@@ -184,6 +184,24 @@ int fail(emb200_handle* h, int code, const char* fmt, ...) {
                                            __FILE__, __LINE__);                                       \
     } while (0)
 
+// cudaFuncSetAttribute(MaxDynamicSharedMemorySize) once per kernel and device:
+// the attribute belongs to the device context, so a flag per call site and
+// device (bit `device` of `done`) covers handles on several GPUs in one process.
+int smem_attr_once(emb200_handle* h, std::atomic<uint64_t>& done, const void* fn, int bytes) {
+    const uint64_t bit = 1ull << (h->device & 63);
+    if (done.load() & bit) return EMB200_OK;
+    CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+    done.fetch_or(bit);
+    return EMB200_OK;
+}
+
+#define SMEM_ATTR_ONCE(fn, bytes)                                               \
+    do {                                                                        \
+        static std::atomic<uint64_t> done_{0};                                  \
+        int rc_ = smem_attr_once(h, done_, (const void*)(fn), (int)(bytes));    \
+        if (rc_) return rc_;                                                    \
+    } while (0)
+
 size_t elt_size(int dtype) { return dtype == EMB200_F32 ? 4 : 1; }
 
 // Error-bound coefficients of the certification, E = ka |x| cmax + kb nmax
@@ -385,11 +403,7 @@ int launch_i8_assign(emb200_handle* h, const int8_t* x, const uint32_t* gather, 
         p.err = (int*)(h->counters.p + 2);
         const TcSmem L = tc_i8_smem_layout(p.kpad);
         const size_t smem = std::max<size_t>(L.total + 1024, 120 * 1024);
-        static bool attr = false;
-        if (!attr) {
-            CK(cudaFuncSetAttribute(k_assign_tc_i8, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmemLimit));
-            attr = true;
-        }
+        SMEM_ATTR_ONCE(k_assign_tc_i8, kTcSmemLimit);
         k_assign_tc_i8<<<dim3((unsigned)row_tiles, (unsigned)nsplit), kTcThreads, smem, st>>>(x, h->map_c8, p);
         CKL();
     } else {
@@ -481,11 +495,7 @@ int launch_tc(emb200_handle* h, const T* x, const uint32_t* gather, const uint32
     TcSmem L = tc_smem_layout(p.kpad, p.nterms);
     // At least 120 KB so that two CTAs never share an SM: each holds all 512 TMEM columns.
     size_t smem = std::max<size_t>(L.total + 1024, 120 * 1024);
-    static bool attr_set = false;  // one flag per <T, COLLECT> instantiation
-    if (!attr_set) {
-        CK(cudaFuncSetAttribute(k_assign_tc<T, COLLECT>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
-        attr_set = true;
-    }
+    SMEM_ATTR_ONCE((k_assign_tc<T, COLLECT>), 227 * 1024);  // one flag per <T, COLLECT> instantiation
     int nsplit = nsplit_override > 0 ? nsplit_override : tc_nsplit(h, m);
     dim3 grid((unsigned)((m + kTcBM - 1) / kTcBM), (unsigned)nsplit);
     k_assign_tc<T, COLLECT><<<grid, kTcThreads, smem, st>>>(x, h->map_hi, h->map_lo, p);
