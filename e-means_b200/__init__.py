@@ -69,7 +69,8 @@ PROPOSER_MODES = {"mlp": 0, "centroids": 1}
 
 
 class _ReportConfig(ctypes.Structure):
-    _fields_ = [("family_radius", ctypes.c_float), ("reserved", ctypes.c_uint32), ("min_local_size", ctypes.c_uint64)]
+    _fields_ = [("family_radius", ctypes.c_float), ("family_pass", ctypes.c_uint32),
+                ("min_local_size", ctypes.c_uint64)]
 
 
 class _ReportSummary(ctypes.Structure):
@@ -609,9 +610,10 @@ class ReportConfig:
 
     family_radius: float = 1.25
     min_local_size: int = 30
+    family_pass: int = 0  # engine option: 0 auto, 1 parallel rounds, 2 sequential greedy (same result)
 
     def _c(self):
-        return _ReportConfig(self.family_radius, 0, self.min_local_size)
+        return _ReportConfig(self.family_radius, self.family_pass, self.min_local_size)
 
 
 @dataclass

@@ -696,6 +696,152 @@ __global__ void __launch_bounds__(1024) k_rep_families(const unsigned long long*
     if (tid == 0) *nfam = F;
 }
 
+// ---- families as the lexicographically first maximal independent set --------
+//
+// The greedy pass above makes cluster v a leader exactly when no cluster before
+// it in size order that is adjacent to it is a leader; every other live cluster
+// joins the earliest adjacent leader (the first leader to reach it). The same
+// result, computed in parallel rounds over compact lists of earlier neighbours
+// (by size-order position): an undecided position becomes FOLLOWER as soon as an
+// earlier neighbour is a LEADER, and LEADER once all earlier neighbours are
+// decided followers. Each round decides at least the earliest undecided position.
+
+constexpr uint8_t kFamUndecided = 0, kFamLeader = 1, kFamFollower = 2;
+
+// pos[cluster] = its position in size order (live clusters only).
+__global__ void k_rep_pos(const unsigned long long* __restrict__ order, uint32_t live, uint32_t* __restrict__ pos) {
+    const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q < live) pos[(uint32_t)order[q]] = q;
+}
+
+// One warp per live position q: the earlier neighbours of cluster order[q] in its
+// adjacency row. FILL = false counts them into ecount[q]; FILL = true writes their
+// positions from eoff[q] on.
+template <bool FILL>
+__global__ void k_rep_nbrs(const unsigned long long* __restrict__ order, uint32_t live,
+                           const uint32_t* __restrict__ adj, uint32_t words, const uint32_t* __restrict__ pos,
+                           uint32_t* __restrict__ ecount, const uint32_t* __restrict__ eoff,
+                           uint32_t* __restrict__ nbr) {
+    const uint32_t q = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (q >= live) return;
+    const uint32_t v = (uint32_t)order[q];
+    const uint32_t* row = adj + (size_t)v * words;
+    uint32_t base = FILL ? eoff[q] : 0u, total = 0;
+    for (uint32_t w0 = 0; w0 < words; w0 += 32) {
+        const uint32_t w = w0 + lane;
+        uint32_t m = w < words ? row[w] : 0u;
+        uint32_t cnt = 0, keep = 0;
+        for (uint32_t mm = m; mm;) {
+            const int b = __ffs(mm) - 1;
+            mm &= mm - 1;
+            if (pos[w * 32 + b] < q) {
+                cnt++;
+                keep |= 1u << b;
+            }
+        }
+        if (FILL) {
+            uint32_t pre = cnt;  // inclusive prefix of the counts over lanes
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t y = __shfl_up_sync(0xffffffffu, pre, o);
+                if (lane >= o) pre += y;
+            }
+            uint32_t at = base + pre - cnt;
+            for (uint32_t mm = keep; mm;) {
+                const int b = __ffs(mm) - 1;
+                mm &= mm - 1;
+                nbr[at++] = pos[w * 32 + b];
+            }
+            base += __shfl_sync(0xffffffffu, pre, 31);
+        } else {
+            total += cnt;
+        }
+    }
+    if (!FILL) {
+#pragma unroll
+        for (int o = 16; o; o >>= 1) total += __shfl_xor_sync(0xffffffffu, total, o);
+        if (lane == 0) ecount[q] = total;
+    }
+}
+
+// One CTA: the rounds above on a status byte per position in shared memory
+// (dynamic: live bytes), then each position's family: its own (leader) or that
+// of its earliest leader neighbour. Families are numbered by their leaders'
+// positions, which is the greedy pass's order of formation. fam_size must be
+// zero on entry.
+__global__ void __launch_bounds__(1024) k_rep_lfmis(const unsigned long long* __restrict__ order, uint32_t live,
+                                                    const uint32_t* __restrict__ eoff,
+                                                    const uint32_t* __restrict__ nbr,
+                                                    const uint32_t* __restrict__ start,
+                                                    uint32_t* __restrict__ fidx, uint32_t* __restrict__ fam_of,
+                                                    uint32_t* __restrict__ fam_lead,
+                                                    unsigned long long* __restrict__ fam_size,
+                                                    uint32_t* __restrict__ nfam) {
+    extern __shared__ uint8_t status[];
+    __shared__ uint32_t ws[32];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    for (uint32_t q = tid; q < live; q += 1024) status[q] = kFamUndecided;
+    __syncthreads();
+    for (uint32_t round = 0; round <= live; round++) {
+        int open = 0;
+        for (uint32_t q = tid; q < live; q += 1024) {
+            if (status[q] != kFamUndecided) continue;
+            bool leader_seen = false, all_decided = true;
+            for (uint32_t e = eoff[q]; e < eoff[q + 1]; e++) {
+                const uint8_t st = status[nbr[e]];
+                if (st == kFamLeader) {
+                    leader_seen = true;
+                    break;
+                }
+                if (st == kFamUndecided) all_decided = false;
+            }
+            if (leader_seen) status[q] = kFamFollower;
+            else if (all_decided) status[q] = kFamLeader;
+            else open = 1;
+        }
+        if (!__syncthreads_or(open)) break;
+    }
+    // (every round decides the earliest undecided position, so none is left here)
+    for (uint32_t q = tid; q < live; q += 1024)
+        if (status[q] == kFamUndecided) status[q] = kFamLeader;
+    __syncthreads();
+    // family number of each leader: leaders before it in position order
+    uint32_t carry = 0;
+    for (uint32_t b0 = 0; b0 < live; b0 += 1024) {
+        const uint32_t q = b0 + tid;
+        const uint32_t isl = q < live && status[q] == kFamLeader ? 1u : 0u;
+        const unsigned bal = __ballot_sync(0xffffffffu, isl);
+        if (lane == 0) ws[warp] = __popc(bal);
+        __syncthreads();
+        uint32_t before = carry;
+        for (int w = 0; w < warp; w++) before += ws[w];
+        before += __popc(bal & ((1u << lane) - 1u));
+        if (isl) fidx[q] = before;
+        uint32_t tot = 0;
+        for (int w = 0; w < 32; w++) tot += ws[w];
+        carry += tot;
+        __syncthreads();
+    }
+    if (tid == 0) *nfam = carry;
+    __syncthreads();
+    for (uint32_t q = tid; q < live; q += 1024) {
+        uint32_t lq = q;
+        if (status[q] != kFamLeader) {
+            lq = 0xffffffffu;
+            for (uint32_t e = eoff[q]; e < eoff[q + 1]; e++) {
+                const uint32_t u = nbr[e];
+                if (status[u] == kFamLeader && u < lq) lq = u;
+            }
+        }
+        const uint32_t f = fidx[lq];
+        const uint32_t v = (uint32_t)order[q];
+        fam_of[v] = f;
+        atomicAdd(&fam_size[f], (unsigned long long)(start[v + 1] - start[v]));
+        if (lq == q) fam_lead[f] = v;
+    }
+}
+
 // Families renumbered by size, largest first (formation order among equals).
 __global__ void k_rep_family_keys(const unsigned long long* __restrict__ fam_size, uint32_t F,
                                   unsigned long long* __restrict__ keys) {

@@ -307,10 +307,13 @@ int emb200_quantizer_decode(emb200_handle* h, const float* codes, size_t n, size
  * are taken in index order when families form, and families of equal size
  * keep the order in which they formed. k <= 131072. */
 
-/* ReportConfig, src/report.rs:21-34 (default {1.25, 30}). */
+/* ReportConfig, src/report.rs:21-34 (default {1.25, 0, 30}). family_pass picks
+ * how families are formed, with the same result either way: 0 = parallel rounds
+ * unless their neighbour lists would be too large, 1 = parallel rounds, 2 = the
+ * sequential greedy pass. */
 typedef struct emb200_report_config {
     float family_radius;
-    uint32_t reserved;
+    uint32_t family_pass;
     uint64_t min_local_size;
 } emb200_report_config;
 

@@ -98,8 +98,10 @@ def _synthetic(n, k, d, seed, empty=0.1, dup=0.0):
                                    (20000, 200, 128), (50000, 1000, 8), (4000, 33, 200), (60000, 30000, 8)])
 def test_report_matches_oracle(emb, orc, n, k, d):
     labels, sq, c = _synthetic(n, k, d, seed=n + k + d, dup=0.05)
-    r = emb.report(labels, sq, c, d)
-    _assert_same(r, _oracle_report(emb, orc, labels, sq, c))
+    o = _oracle_report(emb, orc, labels, sq, c)
+    for family_pass in (1, 2):  # parallel rounds, sequential greedy
+        r = emb.report(labels, sq, c, d, emb.ReportConfig(family_pass=family_pass))
+        _assert_same(r, o)
 
 
 @pytest.mark.gpu
@@ -118,6 +120,8 @@ def test_report_edge_values(emb, orc):
     sq[:3] = [-1.0, np.nan, 0.0]
     sq[40:43] = [-0.0, np.inf, 1e-30]
     for cfg in (emb.ReportConfig(), emb.ReportConfig(family_radius=3.0, min_local_size=1),
+                emb.ReportConfig(family_radius=3.0, min_local_size=1, family_pass=2),
+                emb.ReportConfig(family_radius=100.0, family_pass=1),
                 emb.ReportConfig(family_radius=0.0, min_local_size=1000)):
         r = emb.report(labels, sq, c, d, cfg)
         _assert_same(r, _oracle_report(emb, orc, labels, sq, c, cfg))
