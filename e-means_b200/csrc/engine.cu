@@ -736,16 +736,20 @@ int assign_host(emb200_handle* h, int dtype, const void* x, size_t m, uint32_t* 
     CK(cudaEventRecord(h->ev0, st));
     const size_t esz = elt_size(dtype);
     const size_t row_bytes = h->d * esz;
-    // 64 MB per chunk. Smaller chunks shorten the last search, which no copy
-    // overlaps, but each chunk's search reads its counters on the host: at 16 MB
-    // the 1M x 128 call went from 10.6 to 13.4 ms.
+    // 64 MB chunks. The copies bound the call (the last chunk's search is the part no
+    // copy overlaps), but each chunk's search reads its counters on the host, so more
+    // chunks cost more than they hide: on 1M x 128 rows, 16 MB chunks took 13.4 ms
+    // and 64 MB chunks halving over the last two took 11.0 ms, against 10.6 ms here.
     const size_t chunk = std::max<size_t>(1, std::min(m, ((size_t)64 << 20) / row_bytes));
-    const size_t nch = (m + chunk - 1) / chunk;
+    std::vector<size_t> starts;
+    for (size_t r0 = 0; r0 < m; r0 += chunk) starts.push_back(r0);
+    starts.push_back(m);
+    const size_t nch = starts.size() - 1;
     if (h->stage.ensure(2 * chunk * row_bytes) || h->st_labels.ensure(chunk) || h->st_dist.ensure(chunk))
         return fail(h, EMB200_ENOMEM, "staging allocation failed");
     auto stage_of = [&](size_t i) { return h->stage.p + (i & 1) * chunk * row_bytes; };
     auto copy_in = [&](size_t i) -> int {
-        const size_t r0 = i * chunk, mc = std::min(chunk, m - r0);
+        const size_t r0 = starts[i], mc = starts[i + 1] - r0;
         CK(cudaStreamWaitEvent(h->copy_stream, h->ev_done[i & 1], 0));  // buffer no longer read
         CK(cudaMemcpyAsync(stage_of(i), (const uint8_t*)x + r0 * row_bytes, mc * row_bytes, cudaMemcpyHostToDevice,
                            h->copy_stream));
@@ -757,7 +761,7 @@ int assign_host(emb200_handle* h, int dtype, const void* x, size_t m, uint32_t* 
         if (rc) return rc;
     }
     for (size_t i = 0; i < nch; i++) {
-        const size_t r0 = i * chunk, mc = std::min(chunk, m - r0);
+        const size_t r0 = starts[i], mc = starts[i + 1] - r0;
         // Chunk i + 1 goes into the buffer of chunk i - 1 once that search is done.
         if (i + 1 < nch) {
             rc = copy_in(i + 1);
