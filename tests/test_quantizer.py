@@ -129,3 +129,31 @@ def test_large_unit_norm_rows(emb, orc, qa):
         assert np.array_equal(q.shift, shift) and q.scale == np.float32(scale)
         codes = q.encode(x, assigner=qa)
         assert np.array_equal(codes, orc.quantizer_encode(x, shift, scale))
+
+
+def test_quantizer_errors(emb, qa):
+    lib = emb.lib()
+    scale = ctypes.c_float()
+    shift = np.zeros(4, np.float32)
+    cal = emb.Calibration.faiss()._c()
+    x = np.ones((3, 4), np.float32)
+    # an empty sample (src/quantize.rs:47 asserts n > 0), a null sample
+    assert lib.emb200_quantizer_fit(qa._h, x.ctypes.data_as(ctypes.c_void_p), 0, 4, ctypes.byref(cal),
+                                    shift.ctypes.data_as(ctypes.c_void_p), ctypes.byref(scale)) == -1
+    assert lib.emb200_quantizer_fit(qa._h, None, 3, 4, ctypes.byref(cal), shift.ctypes.data_as(ctypes.c_void_p),
+                                    ctypes.byref(scale)) == -1
+    # device rows must be 16-byte aligned
+    import torch
+
+    xd = torch.ones(64, dtype=torch.float32, device="cuda")
+    assert lib.emb200_quantizer_fit_device(qa._h, ctypes.c_void_p(xd.data_ptr() + 4), 3, 4, ctypes.byref(cal),
+                                           shift.ctypes.data_as(ctypes.c_void_p), ctypes.byref(scale)) == -1
+    assert "aligned" in lib.emb200_last_error(qa._h).decode()
+    # the resident rows must be f32
+    a = emb.B200Assigner(0)
+    a.load_rows(np.zeros((8, 4), np.int8))
+    with pytest.raises(emb.EngineError):
+        emb.Int8Quantizer.fit_resident(a, emb.Calibration.faiss())
+    with pytest.raises(emb.EngineError):
+        emb.Int8Quantizer(4, shift, 1.0).quantize_resident(a)
+    a.close()

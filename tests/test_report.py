@@ -147,3 +147,25 @@ def test_report_after_training_and_resident(emb, orc):
     assert sum(f.size for f in r.families) == 200_000
     assert np.isclose(sum(f.share for f in r.families), 1.0)
     a.close()
+
+
+@pytest.mark.gpu
+def test_report_argument_errors(emb):
+    c = np.zeros((3, 2), np.float32)
+    ones = np.ones(4, np.float32)
+    with pytest.raises(emb.EngineError, match="family_pass"):
+        emb.report(np.zeros(4, np.uint32), ones, c, 2, emb.ReportConfig(family_pass=3))
+    with pytest.raises(emb.EngineError, match="k <="):
+        emb.report(np.zeros(4, np.uint32), ones, np.zeros((131073, 1), np.float32), 1)
+    a = emb.B200Assigner(0)
+    a.load_rows(np.zeros((4, 2), np.float32))
+    a.set_centroids(c)
+    with pytest.raises(emb.EngineError, match="assign_resident"):  # nothing assigned yet
+        emb.report_resident(a)
+    a.assign_resident()
+    r = emb.report_resident(a)
+    assert r.clusters["size"].sum() == 4
+    a.set_centroids(c * 2)  # new centroids: the resident results are stale
+    with pytest.raises(emb.EngineError, match="assign_resident"):
+        emb.report_resident(a)
+    a.close()
