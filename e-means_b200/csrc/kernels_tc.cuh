@@ -181,7 +181,7 @@ EMB_DEV void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: 
 
 struct TcSmem {
     // Offsets (bytes) inside the dynamic shared memory block (1024-aligned base).
-    uint32_t a_hi, a_lo, b0, stage_bytes, term_bytes, norms, merge, bars, total;
+    uint32_t a_hi, a_lo, b0, stage_bytes, term_bytes, norms, merge, bars, pub, total;
     int stages;
 };
 
@@ -196,14 +196,16 @@ __host__ __device__ inline TcSmem tc_smem_layout(int kpad, int nterms) {
     s.b0 = a_total;
     s.term_bytes = b_term;
     s.stage_bytes = b_term * bterms;
-    const uint32_t fixed = kTcNormSlots * kTcBN * 4 + 3 * kTcBM * 16 + 256 + 1024;  // norms, merge, barriers, align
+    // norms, merge, barriers, published top-2 keys, alignment
+    const uint32_t fixed = kTcNormSlots * kTcBN * 4 + 3 * kTcBM * 16 + 256 + 4 * kTcBM * 8 + 1024;
     int st = 0;
     while (st < kTcMaxStages && a_total + (st + 1) * s.stage_bytes + fixed <= (uint32_t)kTcSmemLimit) st++;
     s.stages = st;
     s.norms = s.b0 + st * s.stage_bytes;                 // [8][256] f32
     s.merge = s.norms + kTcNormSlots * kTcBN * 4;        // [3][128] x (s1, i1, s2, i2)
     s.bars = s.merge + 3 * kTcBM * 16;
-    s.total = s.bars + 256;
+    s.pub = s.bars + 256;                                // [4 column quarters][128 rows] float2 (s1, s2)
+    s.total = s.pub + 4 * kTcBM * 8;
     return s;
 }
 
@@ -336,6 +338,34 @@ EMB_DEV void tc_top2_32(const float (&s)[32], float& k1, float& k2) {
     k2 = hi[0];
 }
 
+// Whether a chunk of 32 scores can hold one of a row's final two smallest keys:
+// only a key below an upper bound T of the row's final second key can. A key
+// differs from its score by less than 2^-18 relative (the 5 column bits), so a
+// chunk whose smallest score, lowered by 2^-17 relative, is still >= T cannot;
+// NaN scores never rule a chunk out.
+EMB_DEV bool tc_chunk_may_enter(const float (&s)[32], float T) {
+    const float m = tc_min32(s);
+    return !(fmaf(-fabsf(m), 0x1p-17f, m) >= T);
+}
+
+// An upper bound of a row's final second-smallest key from the running top-2
+// pairs (s1 <= s2) that the four column-quarter warps of the row publish: the
+// second smallest of their union, or at least the smaller of the second
+// smallest s1 and the smallest s2. Values only decrease, so stale reads of
+// another warp's pair are still bounds.
+EMB_DEV float tc_row_bound(const float2* pub, int r) {
+    float2 v[4];
+#pragma unroll
+    for (int c = 0; c < 4; c++)
+        asm volatile("ld.volatile.shared.v2.f32 {%0, %1}, [%2];"
+                     : "=f"(v[c].x), "=f"(v[c].y)
+                     : "r"(smem_u32(pub + c * kTcBM + r)));
+    const float lo01 = fminf(v[0].x, v[1].x), hi01 = fmaxf(v[0].x, v[1].x);
+    const float lo23 = fminf(v[2].x, v[3].x), hi23 = fmaxf(v[2].x, v[3].x);
+    const float second_s1 = min3f(fmaxf(lo01, lo23), hi01, hi23);
+    return fminf(second_s1, fminf(fminf(v[0].y, v[1].y), fminf(v[2].y, v[3].y)));
+}
+
 // Merge a chunk's top-2 (keys k1 <= k2 at columns cb + key&31) into a running top-2.
 EMB_DEV void top2_merge_keys(Top2& t, float k1, float k2, int cb) {
     const uint32_t j1 = (uint32_t)cb + (__float_as_uint(k1) & 31u), j2 = (uint32_t)cb + (__float_as_uint(k2) & 31u);
@@ -430,6 +460,10 @@ k_assign_tc(const T* __restrict__ x, const __grid_constant__ CUtensorMap map_hi,
         for (int u = 0; u < issued; u++) issue(u);
     }
     tc_load_rows(smem, L, x, p, row0, m, threadIdx.x, blockDim.x);
+    {  // published top-2 pairs of the single-term epilogue start at +inf
+        float2* pub = (float2*)(smem + L.pub);
+        for (int i = threadIdx.x; i < 4 * kTcBM; i += blockDim.x) pub[i] = make_float2(INFINITY, INFINITY);
+    }
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     tc_fence_before();
     __syncthreads();
@@ -543,9 +577,22 @@ k_assign_tc(const T* __restrict__ x, const __grid_constant__ CUtensorMap map_hi,
                 tc_scores32(v, nrm + ch * 32, s);
                 const int cb = cq0 + ch * 32;
                 if (!COLLECT) {
-                    float k1, k2;
-                    tc_top2_32(s, k1, k2);
-                    top2_merge_keys(top, k1, k2, cb);
+                    // Single-term search (epilogue-bound): the keyed tournament only for
+                    // chunks that can hold one of the row's final two keys, judged
+                    // against the top-2 pairs that the row's four column-quarter warps
+                    // publish in shared memory (the branch stays uniform across the
+                    // warp). The three-term search is tensor-bound and takes every chunk.
+                    float2* pub = (float2*)(smem + L.pub);
+                    if (p.nterms > 1 ||
+                        __any_sync(__activemask(), tc_chunk_may_enter(s, tc_row_bound(pub, r)))) {
+                        float k1, k2;
+                        tc_top2_32(s, k1, k2);
+                        top2_merge_keys(top, k1, k2, cb);
+                        if (p.nterms == 1)
+                            asm volatile("st.volatile.shared.v2.f32 [%0], {%1, %2};" ::"r"(smem_u32(pub + cq * kTcBM + r)),
+                                         "f"(top.s1), "f"(top.s2)
+                                         : "memory");
+                    }
                 } else if (tc_min32(s) <= theta) {
 #pragma unroll
                     for (int j = 0; j < 32; j++) {
