@@ -106,7 +106,12 @@ EMB_DEV const uint32_t* warp_sort_segment(uint32_t* seg, uint32_t c, uint32_t* s
 // Per touched cluster l (one warp each): put its batch rows back in row order and
 // sum them sequentially per dimension in f32, the order of src/lib.rs:431-441.
 // Also the last pass's per-cluster sums (src/lib.rs:446-454) and labels.
-template <typename T>
+// MAXG > 0 (d <= 32 MAXG): lane t keeps the sums of dimensions t, t + 32, ... in
+// registers, the warp fetches 32 row offsets at a time (one per lane) and passes
+// them by shuffle, so the loads of several rows and dimension groups are in flight
+// together while each dimension's adds keep the row order. MAXG = 0: one
+// dimension group at a time.
+template <typename T, int MAXG>
 __global__ void k_segment_sums(const T* __restrict__ x, const uint32_t* __restrict__ rows, int d, int k,
                                const uint32_t* __restrict__ counts, const uint32_t* __restrict__ offsets,
                                uint32_t* __restrict__ list, uint32_t* __restrict__ scratch, float* __restrict__ sums,
@@ -122,20 +127,55 @@ __global__ void k_segment_sums(const T* __restrict__ x, const uint32_t* __restri
     // Segment l sorts in scratch[2 offsets[l] ...): next_pow2(c) <= 2c entries,
     // disjoint from every other segment's region.
     const uint32_t* seg = warp_sort_segment(list + offsets[l], c, scratch + 2 * (size_t)offsets[l], lane);
-    for (int t0 = 0; t0 < d; t0 += 32) {
-        const int t = t0 + lane;
-        float acc = 0.0f;
-        double acc64 = 0.0;
-        if (t < d) {
-            for (uint32_t j = 0; j < c; j++) {
-                const float v = to_f32(x[(size_t)rows[seg[j]] * d + t]);
-                acc = __fadd_rn(acc, v);
-                if (pass_sums64) acc64 += (double)v;
+    auto store = [&](int t, float acc, double acc64) {
+        sums[(size_t)l * d + t] = acc;
+        if (is_last) {
+            if (pass_sums64) pass_sums64[(size_t)l * d + t] += acc64;
+            else pass_sums[(size_t)l * d + t] = __fadd_rn(pass_sums[(size_t)l * d + t], acc);
+        }
+    };
+    if constexpr (MAXG > 0) {
+        float acc[MAXG];
+        double acc64[MAXG];
+#pragma unroll
+        for (int g = 0; g < MAXG; g++) {
+            acc[g] = 0.0f;
+            acc64[g] = 0.0;
+        }
+        for (uint32_t j0 = 0; j0 < c; j0 += 32) {
+            const uint32_t n = min(32u, c - j0);
+            const uint32_t myrow = (uint32_t)lane < n ? rows[seg[j0 + lane]] : 0u;
+#pragma unroll 4
+            for (uint32_t jj = 0; jj < n; jj++) {
+                const T* xr = x + (size_t)__shfl_sync(0xffffffffu, myrow, (int)jj) * d;
+#pragma unroll
+                for (int g = 0; g < MAXG; g++) {
+                    const int t = g * 32 + lane;
+                    if (t < d) {
+                        const float v = to_f32(xr[t]);
+                        acc[g] = __fadd_rn(acc[g], v);
+                        if (pass_sums64) acc64[g] += (double)v;
+                    }
+                }
             }
-            sums[(size_t)l * d + t] = acc;
-            if (is_last) {
-                if (pass_sums64) pass_sums64[(size_t)l * d + t] += acc64;
-                else pass_sums[(size_t)l * d + t] = __fadd_rn(pass_sums[(size_t)l * d + t], acc);
+        }
+#pragma unroll
+        for (int g = 0; g < MAXG; g++) {
+            const int t = g * 32 + lane;
+            if (t < d) store(t, acc[g], acc64[g]);
+        }
+    } else {
+        for (int t0 = 0; t0 < d; t0 += 32) {
+            const int t = t0 + lane;
+            float acc = 0.0f;
+            double acc64 = 0.0;
+            if (t < d) {
+                for (uint32_t j = 0; j < c; j++) {
+                    const float v = to_f32(x[(size_t)rows[seg[j]] * d + t]);
+                    acc = __fadd_rn(acc, v);
+                    if (pass_sums64) acc64 += (double)v;
+                }
+                store(t, acc, acc64);
             }
         }
     }
