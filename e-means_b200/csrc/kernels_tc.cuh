@@ -366,6 +366,43 @@ EMB_DEV float tc_row_bound(const float2* pub, int r) {
     return fminf(second_s1, fminf(fminf(v[0].y, v[1].y), fminf(v[2].y, v[3].y)));
 }
 
+// Two smallest keys of the 16 scores s[h*16 .. h*16+15] (columns h*16 + j in the
+// key bits), as tc_top2_32 for half a chunk.
+EMB_DEV void tc_top2_16(const float (&s)[32], int h, float& k1, float& k2) {
+    float lo[8], hi[8];
+#pragma unroll
+    for (int p = 0; p < 8; p++) {
+        const int j0 = h * 16 + 2 * p;
+        float a = __uint_as_float((__float_as_uint(s[j0]) & ~31u) | (uint32_t)j0);
+        float b = __uint_as_float((__float_as_uint(s[j0 + 1]) & ~31u) | (uint32_t)(j0 + 1));
+        lo[p] = fminf(a, b);
+        hi[p] = fmaxf(a, b);
+    }
+#pragma unroll
+    for (int w = 4; w >= 1; w >>= 1) {
+#pragma unroll
+        for (int p = 0; p < w; p++) {
+            float a1 = lo[p], a2 = hi[p], b1 = lo[p + w], b2 = hi[p + w];
+            lo[p] = fminf(a1, b1);
+            hi[p] = min3f(fmaxf(a1, b1), a2, b2);
+        }
+    }
+    k1 = lo[0];
+    k2 = hi[0];
+}
+
+// Smallest of the 16 scores s[h*16 .. h*16+15] (NaN-ignoring).
+EMB_DEV float tc_min16(const float (&s)[32], int h) {
+    const int o = h * 16;
+    const float a = min3f(s[o], s[o + 1], s[o + 2]), b = min3f(s[o + 3], s[o + 4], s[o + 5]);
+    const float c = min3f(s[o + 6], s[o + 7], s[o + 8]), d = min3f(s[o + 9], s[o + 10], s[o + 11]);
+    const float e = min3f(s[o + 12], s[o + 13], s[o + 14]);
+    return fminf(min3f(a, b, c), min3f(d, e, s[o + 15]));
+}
+
+// Whether a key of scores whose smallest is m can be below T (see tc_chunk_may_enter).
+EMB_DEV bool tc_min_may_enter(float m, float T) { return !(fmaf(-fabsf(m), 0x1p-17f, m) >= T); }
+
 // Merge a chunk's top-2 (keys k1 <= k2 at columns cb + key&31) into a running top-2.
 EMB_DEV void top2_merge_keys(Top2& t, float k1, float k2, int cb) {
     const uint32_t j1 = (uint32_t)cb + (__float_as_uint(k1) & 31u), j2 = (uint32_t)cb + (__float_as_uint(k2) & 31u);
@@ -583,12 +620,25 @@ k_assign_tc(const T* __restrict__ x, const __grid_constant__ CUtensorMap map_hi,
                     // publish in shared memory (the branch stays uniform across the
                     // warp). The three-term search is tensor-bound and takes every chunk.
                     float2* pub = (float2*)(smem + L.pub);
-                    if (p.nterms > 1 ||
-                        __any_sync(__activemask(), tc_chunk_may_enter(s, tc_row_bound(pub, r)))) {
+                    if (p.nterms > 1) {
                         float k1, k2;
                         tc_top2_32(s, k1, k2);
                         top2_merge_keys(top, k1, k2, cb);
-                        if (p.nterms == 1)
+                    } else {
+                        // Judged per 16-column half: a half needs its tournament less
+                        // often than the whole chunk, and costs less than half of it.
+                        const float bound = tc_row_bound(pub, r);
+                        bool changed = false;
+#pragma unroll
+                        for (int hh = 0; hh < 2; hh++) {
+                            if (__any_sync(__activemask(), tc_min_may_enter(tc_min16(s, hh), bound))) {
+                                float k1, k2;
+                                tc_top2_16(s, hh, k1, k2);
+                                top2_merge_keys(top, k1, k2, cb);
+                                changed = true;
+                            }
+                        }
+                        if (changed)
                             asm volatile("st.volatile.shared.v2.f32 [%0], {%1, %2};" ::"r"(smem_u32(pub + cq * kTcBM + r)),
                                          "f"(top.s1), "f"(top.s2)
                                          : "memory");
