@@ -338,16 +338,6 @@ EMB_DEV void tc_top2_32(const float (&s)[32], float& k1, float& k2) {
     k2 = hi[0];
 }
 
-// Whether a chunk of 32 scores can hold one of a row's final two smallest keys:
-// only a key below an upper bound T of the row's final second key can. A key
-// differs from its score by less than 2^-18 relative (the 5 column bits), so a
-// chunk whose smallest score, lowered by 2^-17 relative, is still >= T cannot;
-// NaN scores never rule a chunk out.
-EMB_DEV bool tc_chunk_may_enter(const float (&s)[32], float T) {
-    const float m = tc_min32(s);
-    return !(fmaf(-fabsf(m), 0x1p-17f, m) >= T);
-}
-
 // An upper bound of a row's final second-smallest key from the running top-2
 // pairs (s1 <= s2) that the four column-quarter warps of the row publish: the
 // second smallest of their union, or at least the smaller of the second
@@ -400,7 +390,11 @@ EMB_DEV float tc_min16(const float (&s)[32], int h) {
     return fminf(min3f(a, b, c), min3f(d, e, s[o + 15]));
 }
 
-// Whether a key of scores whose smallest is m can be below T (see tc_chunk_may_enter).
+// Whether scores whose smallest is m can hold one of a row's final two smallest
+// keys: only a key below an upper bound T of the row's final second key can. A
+// key differs from its score by less than 2^-18 relative (the 5 column bits), so
+// scores whose smallest, lowered by 2^-17 relative, is still >= T cannot; NaN
+// scores never rule a chunk out.
 EMB_DEV bool tc_min_may_enter(float m, float T) { return !(fmaf(-fabsf(m), 0x1p-17f, m) >= T); }
 
 // Merge a chunk's top-2 (keys k1 <= k2 at columns cb + key&31) into a running top-2.
