@@ -626,7 +626,15 @@ int settle_rows(emb200_handle* h, const T* x, const uint32_t* gather, size_t m, 
     bound_coefficients(fast_prec, dtype, h->d, tc, &ka, &kb);
     bound_coefficients(EMB200_PREC_BF16, dtype, h->d, false, &ka2, &kb2);
     const int match = h->opts.match_kernel;
-    if (match == kMatchAvx512) {
+    bool vec4 = false;
+    if constexpr (std::is_same<T, float>::value)
+        vec4 = d % 16 == 0 && ((uintptr_t)x & 15) == 0 && ((uintptr_t)h->c.p & 15) == 0;
+    if (match == kMatchAvx512 && vec4) {
+        k_certify16v<<<(unsigned)((m + 63) / 64), 256, 0, st>>>(
+            (const float*)x, gather, (int)m, d, h->c.p, h->norms.p, k, h->part_s.p, h->part_i.p, nsplit, h->bounds.p,
+            ka, kb, labels, dist, h->redo_rows.p, ctr, ctr + 1, tc ? (const int*)(ctr + 2) : nullptr, h->redo_theta.p,
+            ka2, kb2, row_bounds);
+    } else if (match == kMatchAvx512) {
         k_certify16<T><<<(unsigned)((m + 15) / 16), 256, 0, st>>>(
             x, gather, (int)m, d, h->c.p, h->norms.p, k, h->part_s.p, h->part_i.p, nsplit, h->bounds.p, ka, kb, labels,
             dist, h->redo_rows.p, ctr, ctr + 1, tc ? (const int*)(ctr + 2) : nullptr, h->redo_theta.p, ka2, kb2,

@@ -219,6 +219,72 @@ __global__ void k_certify(const T* __restrict__ x, const uint32_t* __restrict__ 
     }
 }
 
+// The decision of k_certify16 for one row, given the exact re-scores' dot
+// products a1, a2 (candidates j1, j2) and |x|^2: true when the row is certified
+// (its label and distance written), else false with the refine pass's threshold
+// in *theta_out.
+EMB_DEV bool certify16_decide(int row, const Top2& t, uint32_t j1, uint32_t j2, float a1, float a2, float xn, int k,
+                              const float* __restrict__ norms, const Bounds* __restrict__ bounds, float ka, float kb,
+                              uint32_t* __restrict__ labels, float* __restrict__ dist,
+                              const int* __restrict__ fast_err, float ka2, float kb2,
+                              const float2* __restrict__ row_bounds, float* theta_out) {
+    bool ok = t.i1 < (uint32_t)k && (k < 2 || t.i2 < (uint32_t)k);
+    const float s1 = score_ref(norms[j1], a1);
+    float sb = s1;
+    uint32_t jb = j1;
+    if (t.i2 < (uint32_t)k) {
+        const float s2 = score_ref(norms[j2], a2);
+        if (lex_less(s2, j2, sb, jb)) {
+            sb = s2;
+            jb = j2;
+        }
+    }
+    if (ok && k > 2) {
+        const float xnorm = __fmul_ru(__fsqrt_ru(fmaxf(xn, 0.0f)), 1.0000005f);
+        const float E = __fadd_ru(__fmul_ru(__fmul_ru(ka, xnorm), row_bounds ? row_bounds[row].x : bounds->cmax),
+                                  __fmul_ru(kb, row_bounds ? row_bounds[row].y : bounds->nmax));
+        const float thr = __fsub_rd(t.s2, E);
+        ok = isfinite(E) && sb < thr;
+    }
+    if (ok && !(sb < __int_as_float(0x7f800000))) ok = false;
+    if (fast_err && *fast_err) ok = false;
+    if (ok) {
+        labels[row] = jb;
+        dist[row] = fmaxf(__fadd_rn(sb, xn), 0.0f);
+        return true;
+    }
+    float theta = __int_as_float(0x7fc00000);
+    if (t.i1 < (uint32_t)k && sb < __int_as_float(0x7f800000) && sb > -__int_as_float(0x7f800000)) {
+        const float xnorm = __fmul_ru(__fsqrt_ru(fmaxf(xn, 0.0f)), 1.0000005f);
+        const float E2 = __fadd_ru(__fmul_ru(__fmul_ru(ka2, xnorm), bounds->cmax), __fmul_ru(kb2, bounds->nmax));
+        const float th = __fadd_ru(sb, E2);
+        if (isfinite(th)) theta = th;
+    }
+    *theta_out = theta;
+    return false;
+}
+
+// Warp-wide tally of the certify decisions (all 32 lanes call it): one atomic
+// for the warp's certified rows, one reservation of refine-list slots for its
+// uncertified rows. The list's order is immaterial (each row settles alone).
+EMB_DEV void certify_tally(bool ok, bool redo, int row, float theta, uint32_t* __restrict__ cert_count,
+                           uint32_t* __restrict__ redo_count, uint32_t* __restrict__ redo_rows,
+                           float* __restrict__ redo_theta) {
+    const int lane = threadIdx.x & 31;
+    const unsigned okb = __ballot_sync(kFull, ok);
+    if (lane == 0 && okb) atomicAdd(cert_count, (unsigned)__popc(okb));
+    const unsigned rb = __ballot_sync(kFull, redo);
+    if (!rb) return;
+    uint32_t base = 0;
+    if (lane == 0) base = atomicAdd(redo_count, (unsigned)__popc(rb));
+    base = __shfl_sync(kFull, base, 0);
+    if (redo) {
+        const uint32_t slot = base + (uint32_t)__popc(rb & ((1u << lane) - 1u));
+        redo_rows[slot] = (uint32_t)row;
+        redo_theta[slot] = theta;
+    }
+}
+
 // k_certify specialised to the AVX-512 rounding (the default): one half-warp
 // per row, so a warp certifies two rows, and one pass over the row computes its
 // sqnorm lanes and both candidates' 16 FMA lanes. Same decisions and outputs as
@@ -276,43 +342,86 @@ __global__ void k_certify16(const T* __restrict__ x, const uint32_t* __restrict_
         tail = __fadd_rn(tail, __fmul_rn(v, v));
     }
     xn = __fadd_rn(xn, tail);
-    if (!live || l != 0) return;
-    bool ok = t.i1 < (uint32_t)k && (k < 2 || t.i2 < (uint32_t)k);
-    const float s1 = score_ref(norms[j1], a1);
-    float sb = s1;
-    uint32_t jb = j1;
-    if (t.i2 < (uint32_t)k) {
-        const float s2 = score_ref(norms[j2], a2);
-        if (lex_less(s2, j2, sb, jb)) {
-            sb = s2;
-            jb = j2;
+    bool ok = false, redo = false;
+    float theta = 0.0f;
+    if (live && l == 0) {
+        ok = certify16_decide(row, t, j1, j2, a1, a2, xn, k, norms, bounds, ka, kb, labels, dist, fast_err, ka2, kb2,
+                              row_bounds, &theta);
+        redo = !ok;
+    }
+    certify_tally(ok, redo, row, theta, cert_count, redo_count, redo_rows, redo_theta);
+}
+
+// k_certify16 with four threads per row (eight rows per warp), for f32 rows with
+// d % 16 == 0: thread q keeps AVX-512 lanes 4q .. 4q+3 and loads them as float4.
+// The lane sums combine in the reference's tree order (lane l with l^8, l^4,
+// l^2, l^1: threads q^2 and q^1, then in registers), and |x|^2 adds the 16 lane
+// partials in lane order, so every value equals k_certify16's.
+__global__ void k_certify16v(const float* __restrict__ x, const uint32_t* __restrict__ gather, int m, int d,
+                             const float* __restrict__ c, const float* __restrict__ norms, int k,
+                             const float* __restrict__ part_s, const uint32_t* __restrict__ part_i, int nsplit,
+                             const Bounds* __restrict__ bounds, float ka, float kb, uint32_t* __restrict__ labels,
+                             float* __restrict__ dist, uint32_t* __restrict__ redo_rows,
+                             uint32_t* __restrict__ redo_count, uint32_t* __restrict__ cert_count,
+                             const int* __restrict__ fast_err, float* __restrict__ redo_theta, float ka2, float kb2,
+                             const float2* __restrict__ row_bounds = nullptr) {
+    const int lane = threadIdx.x & 31, q = lane & 3;
+    const int row = (int)(((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 2);
+    const bool live = row < m;
+    const int r = live ? row : m - 1;  // dead quarter-warps mirror a live row and write nothing
+    const size_t src = gather ? gather[r] : (size_t)r;
+    const float* xr = x + src * (size_t)d;
+    Top2 t;
+    t.init();
+    for (int s = 0; s < nsplit; s++) {
+        const size_t o = ((size_t)s * m + r) * 2;
+        t.push(part_s[o], part_i[o]);
+        t.push(part_s[o + 1], part_i[o + 1]);
+    }
+    const uint32_t j1 = t.i1 < (uint32_t)k ? t.i1 : 0u;
+    const uint32_t j2 = t.i2 < (uint32_t)k ? t.i2 : j1;
+    const float* c1 = c + (size_t)j1 * d;
+    const float* c2 = c + (size_t)j2 * d;
+    float sq[4] = {0.0f, 0.0f, 0.0f, 0.0f}, p1[4] = {0.0f, 0.0f, 0.0f, 0.0f}, p2[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+    for (int i = 4 * q; i < d; i += 16) {
+        const float4 xv = *reinterpret_cast<const float4*>(xr + i);
+        const float4 u = *reinterpret_cast<const float4*>(c1 + i);
+        const float4 w = *reinterpret_cast<const float4*>(c2 + i);
+        const float xs[4] = {xv.x, xv.y, xv.z, xv.w}, us[4] = {u.x, u.y, u.z, u.w}, ws[4] = {w.x, w.y, w.z, w.w};
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            sq[j] = __fadd_rn(sq[j], __fmul_rn(xs[j], xs[j]));
+            p1[j] = __fmaf_rn(xs[j], us[j], p1[j]);
+            p2[j] = __fmaf_rn(xs[j], ws[j], p2[j]);
         }
     }
-    if (ok && k > 2) {
-        const float xnorm = __fmul_ru(__fsqrt_ru(fmaxf(xn, 0.0f)), 1.0000005f);
-        const float E = __fadd_ru(__fmul_ru(__fmul_ru(ka, xnorm), row_bounds ? row_bounds[row].x : bounds->cmax),
-                                  __fmul_ru(kb, row_bounds ? row_bounds[row].y : bounds->nmax));
-        const float thr = __fsub_rd(t.s2, E);
-        ok = isfinite(E) && sb < thr;
+#pragma unroll
+    for (int j = 0; j < 4; j++) {  // lane l with l^8, then l^4
+        p1[j] = __fadd_rn(p1[j], __shfl_xor_sync(kFull, p1[j], 2));
+        p2[j] = __fadd_rn(p2[j], __shfl_xor_sync(kFull, p2[j], 2));
     }
-    if (ok && !(sb < __int_as_float(0x7f800000))) ok = false;
-    if (fast_err && *fast_err) ok = false;
-    if (ok) {
-        labels[row] = jb;
-        dist[row] = fmaxf(__fadd_rn(sb, xn), 0.0f);
-        atomicAdd(cert_count, 1u);
-    } else {
-        float theta = __int_as_float(0x7fc00000);
-        if (t.i1 < (uint32_t)k && sb < __int_as_float(0x7f800000) && sb > -__int_as_float(0x7f800000)) {
-            const float xnorm = __fmul_ru(__fsqrt_ru(fmaxf(xn, 0.0f)), 1.0000005f);
-            const float E2 = __fadd_ru(__fmul_ru(__fmul_ru(ka2, xnorm), bounds->cmax), __fmul_ru(kb2, bounds->nmax));
-            const float th = __fadd_ru(sb, E2);
-            if (isfinite(th)) theta = th;
-        }
-        const uint32_t slot = atomicAdd(redo_count, 1u);
-        redo_rows[slot] = (uint32_t)row;
-        redo_theta[slot] = theta;
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+        p1[j] = __fadd_rn(p1[j], __shfl_xor_sync(kFull, p1[j], 1));
+        p2[j] = __fadd_rn(p2[j], __shfl_xor_sync(kFull, p2[j], 1));
     }
+    // l^2 and l^1 within the thread
+    const float a1 = __fadd_rn(__fadd_rn(p1[0], p1[2]), __fadd_rn(p1[1], p1[3]));
+    const float a2 = __fadd_rn(__fadd_rn(p2[0], p2[2]), __fadd_rn(p2[1], p2[3]));
+    float xn = -0.0f;
+    const int base = lane & ~3;
+#pragma unroll
+    for (int qq = 0; qq < 4; qq++)
+#pragma unroll
+        for (int j = 0; j < 4; j++) xn = __fadd_rn(xn, __shfl_sync(kFull, sq[j], base + qq));
+    bool ok = false, redo = false;
+    float theta = 0.0f;
+    if (live && q == 0) {
+        ok = certify16_decide(row, t, j1, j2, a1, a2, xn, k, norms, bounds, ka, kb, labels, dist, fast_err, ka2, kb2,
+                              row_bounds, &theta);
+        redo = !ok;
+    }
+    certify_tally(ok, redo, row, theta, cert_count, redo_count, redo_rows, redo_theta);
 }
 
 // Exact re-score of the refine pass's candidates (one warp per refined row):
