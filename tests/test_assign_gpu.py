@@ -236,6 +236,25 @@ def test_resident_assign_matches_host_path(emb, assigners, precision):
     assert np.array_equal(l1, l2) and same_f32(d1, d2)
 
 
+@pytest.mark.parametrize("n,d,k", [(600_000, 128, 512), (70_000, 1024, 64), (131_073, 128, 300)])
+def test_host_path_many_chunks(emb, orc, assigners, n, d, k):
+    # Host rows go through two staging buffers in 64 MB chunks (600k x 128:
+    # five chunks; 70k x 1024: five; 131,073 x 128: a full chunk and one row),
+    # so each buffer is reused. Every chunk's results must equal the resident
+    # path's, and the first and last rows the oracle's.
+    x = emb.datasets.embeddings(n, d, latent=16, seed=n % 97)
+    c = x[np.random.default_rng(n).choice(n, k, replace=False)] * np.float32(0.97)
+    a = assigners("bf16x1")
+    a.set_centroids(c)
+    l1, d1 = a.assign(x)
+    a.load_rows(x)
+    l2, d2 = a.assign_resident()
+    assert np.array_equal(l1, l2) and same_f32(d1, d2)
+    idx = np.r_[0:3000, n - 20000:n]
+    rl, rd = orc.cpu_assign(x[idx], c, emulate=True)
+    assert np.array_equal(l1[idx], rl) and same_f32(d1[idx], rd)
+
+
 @pytest.mark.parametrize("precision", ["bf16", "bf16x1"])
 @pytest.mark.parametrize("d", [1, 33, 64, 96, 128])
 def test_tcgen05_path_runs_and_certifies(emb, orc, assigners, precision, d):
