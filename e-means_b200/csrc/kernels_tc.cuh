@@ -592,6 +592,9 @@ k_assign_tc(const T* __restrict__ x, const __grid_constant__ CUtensorMap map_hi,
             const int cq0 = col_first + t * col_step + cq * 64;
             const float* nrm = norms_s + (t % kTcNormSlots) * kTcBN + cq * 64;
             const uint32_t taddr = tmem_base + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * kTcBN + cq * 64);
+            // The published bound is read once per tile (the epilogue is issue-bound);
+            // within the tile the warp's own second key tightens it.
+            const float tile_bound = (!COLLECT && p.nterms == 1) ? tc_row_bound((const float2*)(smem + L.pub), r) : 0.0f;
 #pragma unroll
             for (int ch = 0; ch < 2; ch++) {
                 uint32_t v[32];
@@ -621,7 +624,9 @@ k_assign_tc(const T* __restrict__ x, const __grid_constant__ CUtensorMap map_hi,
                     } else {
                         // Judged per 16-column half: a half needs its tournament less
                         // often than the whole chunk, and costs less than half of it.
-                        const float bound = tc_row_bound(pub, r);
+                        // The warp's own running s2 is an upper bound of the row's final
+                        // s2 too (its columns are a subset of the row's).
+                        const float bound = fminf(tile_bound, top.s2);
                         bool changed = false;
 #pragma unroll
                         for (int hh = 0; hh < 2; hh++) {
