@@ -138,6 +138,53 @@ __global__ void k_add_bias(float* __restrict__ norms, const float* __restrict__ 
     atomic_max_pos(&bounds->nmax, fabsf(v));
 }
 
+// The certify decision for one row, given the exact re-scores' dot products a1,
+// a2 (candidates j1, j2) and |x|^2: true when the row is certified (its label and
+// distance written), else false with the refine pass's threshold in *theta_out.
+EMB_DEV bool certify_decide(int row, const Top2& t, uint32_t j1, uint32_t j2, float a1, float a2, float xn, int k,
+                            const float* __restrict__ norms, const Bounds* __restrict__ bounds, float ka, float kb,
+                            uint32_t* __restrict__ labels, float* __restrict__ dist,
+                            const int* __restrict__ fast_err, float ka2, float kb2,
+                            const float2* __restrict__ row_bounds, float* theta_out) {
+    bool ok = t.i1 < (uint32_t)k && (k < 2 || t.i2 < (uint32_t)k);
+    const float s1 = score_ref(norms[j1], a1);
+    float sb = s1;
+    uint32_t jb = j1;
+    if (t.i2 < (uint32_t)k) {
+        const float s2 = score_ref(norms[j2], a2);
+        if (lex_less(s2, j2, sb, jb)) {
+            sb = s2;
+            jb = j2;
+        }
+    }
+    if (ok && k > 2) {
+        const float xnorm = __fmul_ru(__fsqrt_ru(fmaxf(xn, 0.0f)), 1.0000005f);
+        const float E = __fadd_ru(__fmul_ru(__fmul_ru(ka, xnorm), row_bounds ? row_bounds[row].x : bounds->cmax),
+                                  __fmul_ru(kb, row_bounds ? row_bounds[row].y : bounds->nmax));
+        const float thr = __fsub_rd(t.s2, E);
+        ok = isfinite(E) && sb < thr;  // NaN-safe: any NaN fails
+    }
+    if (ok && !(sb < __int_as_float(0x7f800000))) ok = false;  // non-finite best: re-search
+    if (fast_err && *fast_err) ok = false;  // the fast kernel gave up: trust nothing it wrote
+    if (ok) {
+        labels[row] = jb;
+        dist[row] = fmaxf(__fadd_rn(sb, xn), 0.0f);
+        return true;
+    }
+    // Threshold for the refine pass: the reference's best j* has s_j* <= sb, so
+    // its refine-pass score is <= sb + E2. Non-finite: no candidates, so the row
+    // is searched exhaustively.
+    float theta = __int_as_float(0x7fc00000);
+    if (t.i1 < (uint32_t)k && sb < __int_as_float(0x7f800000) && sb > -__int_as_float(0x7f800000)) {
+        const float xnorm = __fmul_ru(__fsqrt_ru(fmaxf(xn, 0.0f)), 1.0000005f);
+        const float E2 = __fadd_ru(__fmul_ru(__fmul_ru(ka2, xnorm), bounds->cmax), __fmul_ru(kb2, bounds->nmax));
+        const float th = __fadd_ru(sb, E2);
+        if (isfinite(th)) theta = th;
+    }
+    *theta_out = theta;
+    return false;
+}
+
 // Certification of the fast top-2 (one warp per row).
 //   part_s/part_i: nsplit partial top-2 lists per row, [split][row][2].
 //   The approximate score of every centroid is within E of its reference
@@ -178,90 +225,15 @@ __global__ void k_certify(const T* __restrict__ x, const uint32_t* __restrict__ 
     float d1 = __shfl_sync(kFull, dg, 0);
     float d2 = __shfl_sync(kFull, dg, gsz);
     if (lane != 0) return;
-    bool ok = t.i1 < (uint32_t)k && (k < 2 || t.i2 < (uint32_t)k);
-    float s1 = score_ref(norms[j1], d1);
-    float sb = s1;
-    uint32_t jb = j1;
-    if (t.i2 < (uint32_t)k) {
-        float s2 = score_ref(norms[j2], d2);
-        if (lex_less(s2, j2, sb, jb)) {
-            sb = s2;
-            jb = j2;
-        }
-    }
-    if (ok && k > 2) {
-        float xnorm = __fmul_ru(__fsqrt_ru(fmaxf(xn, 0.0f)), 1.0000005f);
-        float E = __fadd_ru(__fmul_ru(__fmul_ru(ka, xnorm), row_bounds ? row_bounds[row].x : bounds->cmax),
-                                  __fmul_ru(kb, row_bounds ? row_bounds[row].y : bounds->nmax));
-        float thr = __fsub_rd(t.s2, E);
-        ok = isfinite(E) && sb < thr;  // NaN-safe: any NaN fails
-    }
-    if (ok && !(sb < __int_as_float(0x7f800000))) ok = false;  // non-finite best: re-search
-    if (fast_err && *fast_err) ok = false;  // the fast kernel gave up: trust nothing it wrote
-    if (ok) {
-        labels[row] = jb;
-        dist[row] = fmaxf(__fadd_rn(sb, xn), 0.0f);
+    float theta = 0.0f;
+    if (certify_decide(row, t, j1, j2, d1, d2, xn, k, norms, bounds, ka, kb, labels, dist, fast_err, ka2, kb2,
+                       row_bounds, &theta)) {
         atomicAdd(cert_count, 1u);
     } else {
-        // Threshold for the refine pass: the reference's best j* has s_j* <= sb,
-        // so its refine-pass score is <= sb + E2. Non-finite: no candidates, so
-        // the row is searched exhaustively.
-        float theta = __int_as_float(0x7fc00000);
-        if (t.i1 < (uint32_t)k && sb < __int_as_float(0x7f800000) && sb > -__int_as_float(0x7f800000)) {
-            float xnorm = __fmul_ru(__fsqrt_ru(fmaxf(xn, 0.0f)), 1.0000005f);
-            float E2 = __fadd_ru(__fmul_ru(__fmul_ru(ka2, xnorm), bounds->cmax), __fmul_ru(kb2, bounds->nmax));
-            float th = __fadd_ru(sb, E2);
-            if (isfinite(th)) theta = th;
-        }
-        uint32_t slot = atomicAdd(redo_count, 1u);
+        const uint32_t slot = atomicAdd(redo_count, 1u);
         redo_rows[slot] = (uint32_t)row;
         redo_theta[slot] = theta;
     }
-}
-
-// The decision of k_certify16 for one row, given the exact re-scores' dot
-// products a1, a2 (candidates j1, j2) and |x|^2: true when the row is certified
-// (its label and distance written), else false with the refine pass's threshold
-// in *theta_out.
-EMB_DEV bool certify16_decide(int row, const Top2& t, uint32_t j1, uint32_t j2, float a1, float a2, float xn, int k,
-                              const float* __restrict__ norms, const Bounds* __restrict__ bounds, float ka, float kb,
-                              uint32_t* __restrict__ labels, float* __restrict__ dist,
-                              const int* __restrict__ fast_err, float ka2, float kb2,
-                              const float2* __restrict__ row_bounds, float* theta_out) {
-    bool ok = t.i1 < (uint32_t)k && (k < 2 || t.i2 < (uint32_t)k);
-    const float s1 = score_ref(norms[j1], a1);
-    float sb = s1;
-    uint32_t jb = j1;
-    if (t.i2 < (uint32_t)k) {
-        const float s2 = score_ref(norms[j2], a2);
-        if (lex_less(s2, j2, sb, jb)) {
-            sb = s2;
-            jb = j2;
-        }
-    }
-    if (ok && k > 2) {
-        const float xnorm = __fmul_ru(__fsqrt_ru(fmaxf(xn, 0.0f)), 1.0000005f);
-        const float E = __fadd_ru(__fmul_ru(__fmul_ru(ka, xnorm), row_bounds ? row_bounds[row].x : bounds->cmax),
-                                  __fmul_ru(kb, row_bounds ? row_bounds[row].y : bounds->nmax));
-        const float thr = __fsub_rd(t.s2, E);
-        ok = isfinite(E) && sb < thr;
-    }
-    if (ok && !(sb < __int_as_float(0x7f800000))) ok = false;
-    if (fast_err && *fast_err) ok = false;
-    if (ok) {
-        labels[row] = jb;
-        dist[row] = fmaxf(__fadd_rn(sb, xn), 0.0f);
-        return true;
-    }
-    float theta = __int_as_float(0x7fc00000);
-    if (t.i1 < (uint32_t)k && sb < __int_as_float(0x7f800000) && sb > -__int_as_float(0x7f800000)) {
-        const float xnorm = __fmul_ru(__fsqrt_ru(fmaxf(xn, 0.0f)), 1.0000005f);
-        const float E2 = __fadd_ru(__fmul_ru(__fmul_ru(ka2, xnorm), bounds->cmax), __fmul_ru(kb2, bounds->nmax));
-        const float th = __fadd_ru(sb, E2);
-        if (isfinite(th)) theta = th;
-    }
-    *theta_out = theta;
-    return false;
 }
 
 // Warp-wide tally of the certify decisions (all 32 lanes call it): one atomic
@@ -345,7 +317,7 @@ __global__ void k_certify16(const T* __restrict__ x, const uint32_t* __restrict_
     bool ok = false, redo = false;
     float theta = 0.0f;
     if (live && l == 0) {
-        ok = certify16_decide(row, t, j1, j2, a1, a2, xn, k, norms, bounds, ka, kb, labels, dist, fast_err, ka2, kb2,
+        ok = certify_decide(row, t, j1, j2, a1, a2, xn, k, norms, bounds, ka, kb, labels, dist, fast_err, ka2, kb2,
                               row_bounds, &theta);
         redo = !ok;
     }
@@ -417,7 +389,7 @@ __global__ void k_certify16v(const float* __restrict__ x, const uint32_t* __rest
     bool ok = false, redo = false;
     float theta = 0.0f;
     if (live && q == 0) {
-        ok = certify16_decide(row, t, j1, j2, a1, a2, xn, k, norms, bounds, ka, kb, labels, dist, fast_err, ka2, kb2,
+        ok = certify_decide(row, t, j1, j2, a1, a2, xn, k, norms, bounds, ka, kb, labels, dist, fast_err, ka2, kb2,
                               row_bounds, &theta);
         redo = !ok;
     }
