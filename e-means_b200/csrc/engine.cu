@@ -32,6 +32,7 @@
 #include "kernels_report.cuh"
 
 constexpr int kRefineCap = 32;  // candidates kept per refined row
+constexpr size_t kMaxSearchRows = (size_t)1 << 26;  // rows per search pass (32-bit row indexing inside)
 
 using namespace emb;
 
@@ -549,6 +550,17 @@ int assign_rows_dev(emb200_handle* h, const T* x, const uint32_t* gather, size_t
     const int dtype = std::is_same<T, float>::value ? EMB200_F32 : (std::is_same<T, int8_t>::value ? EMB200_I8 : EMB200_U8);
     const int k = (int)h->k, d = (int)h->d;
     if (m == 0) return EMB200_OK;
+    if (m > kMaxSearchRows) {
+        // Pieces of at most 2^26 rows: the search kernels index rows (up to 32
+        // threads each) in 32 bits.
+        for (size_t r0 = 0; r0 < m; r0 += kMaxSearchRows) {
+            const size_t mc = std::min(kMaxSearchRows, m - r0);
+            const T* xs = gather ? x : x + r0 * (size_t)d;
+            int rc = assign_rows_dev(h, xs, gather ? gather + r0 : nullptr, mc, labels + r0, dist + r0, st, graph);
+            if (rc) return rc;
+        }
+        return EMB200_OK;
+    }
     if (use_i8_mode(h, dtype)) {
         h->stats.fast_kernel = 2;
         return launch_i8_assign(h, (const int8_t*)x, gather, m, labels, dist, st, graph);

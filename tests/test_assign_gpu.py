@@ -255,6 +255,24 @@ def test_host_path_many_chunks(emb, orc, assigners, n, d, k):
     assert np.array_equal(l1[idx], rl) and same_f32(d1[idx], rd)
 
 
+def test_resident_rows_past_one_search_pass(emb, orc, assigners):
+    # 2^26 + 4099 resident rows: the search runs in two passes of at most 2^26
+    # rows (its kernels index rows in 32 bits). Rows on both sides of the seam,
+    # at the ends and at random must match the oracle.
+    n = (1 << 26) + 4099
+    rng = np.random.default_rng(26)
+    x = rng.standard_normal((n, 2), dtype=np.float32)
+    c = rng.standard_normal((8, 2), dtype=np.float32)
+    a = assigners("bf16x1")
+    a.set_centroids(c)
+    a.load_rows(x)
+    lab, dist = a.assign_resident()
+    seam = 1 << 26
+    idx = np.unique(np.r_[0:2000, seam - 2000:seam + 2000, n - 2000:n, rng.integers(0, n, 20000)])
+    rl, rd = orc.cpu_assign(x[idx], c, emulate=True)
+    assert np.array_equal(lab[idx], rl) and same_f32(dist[idx], rd)
+
+
 @pytest.mark.parametrize("precision", ["bf16", "bf16x1"])
 @pytest.mark.parametrize("d", [1, 33, 64, 96, 128])
 def test_tcgen05_path_runs_and_certifies(emb, orc, assigners, precision, d):
