@@ -255,6 +255,28 @@ def test_host_path_many_chunks(emb, orc, assigners, n, d, k):
     assert np.array_equal(l1[idx], rl) and same_f32(d1[idx], rd)
 
 
+@pytest.mark.parametrize("precision", ["bf16x1", "bf16"])
+def test_device_rows_not_16_byte_aligned(emb, orc, assigners, precision):
+    # Device rows at a 4-byte offset with d % 16 == 0: the fast kernel's row loads
+    # and the certify pass take their scalar forms; the results are the oracle's.
+    import torch
+
+    n, d = 5000, 128
+    x = emb.datasets.embeddings(n, d, latent=16, seed=31)
+    c = x[np.random.default_rng(31).choice(n, 300, replace=False)] * np.float32(0.97)
+    a = assigners(precision)
+    a.set_centroids(c)
+    buf = torch.empty(n * d + 1, dtype=torch.float32, device="cuda")
+    buf[1:] = torch.from_numpy(x.ravel()).cuda()
+    lab = torch.empty(n, dtype=torch.int32, device="cuda")
+    dst = torch.empty(n, dtype=torch.float32, device="cuda")
+    torch.cuda.synchronize()
+    a.assign_device(buf.data_ptr() + 4, emb.EMB200_F32, n, lab.data_ptr(), dst.data_ptr())
+    torch.cuda.synchronize()
+    rl, rd = orc.cpu_assign(x, c, emulate=True)
+    assert np.array_equal(lab.cpu().numpy().view(np.uint32), rl) and same_f32(dst.cpu().numpy(), rd)
+
+
 def test_resident_rows_past_one_search_pass(emb, orc, assigners):
     # 2^26 + 4099 resident rows: the search runs in two passes of at most 2^26
     # rows (its kernels index rows in 32 bits). Rows on both sides of the seam,
