@@ -133,6 +133,9 @@ struct emb200_handle {
     cudaEvent_t ev_done[2] = {nullptr, nullptr};  // a staging buffer's search is complete
     DevBuf<uint32_t> st_labels;
     DevBuf<float> st_dist;
+    // largest split partials of any batch of up to part_size_m rows (no-host-read mode)
+    size_t part_size_m = 0, part_size_k = 0, part_size_rows = 0;
+    bool part_size_tc = false;
     DevBuf<float> part_s;
     DevBuf<uint32_t> part_i;
     DevBuf<uint32_t> redo_rows;
@@ -472,9 +475,13 @@ int tc_nsplit(const emb200_handle* h, size_t m) {
     const long row_tiles = (long)((m + kTcBM - 1) / kTcBM);
     const int ntiles = (int)((h->k + kTcBN - 1) / kTcBN);
     const long sms = std::max(1, h->sm_count);
+    // From one full wave of row tiles up, splits only even out the last wave:
+    // 32 give the same choices as all of them (checked up to 40,000 row tiles
+    // and 1024 centroid tiles) and keep the search short.
+    const int max_ns = row_tiles >= sms ? std::min(ntiles, 32) : ntiles;
     int best = 1;
     double best_cost = 0.0;
-    for (int ns = 1; ns <= ntiles; ns++) {
+    for (int ns = 1; ns <= max_ns; ns++) {
         const double waves = (double)((row_tiles * ns + sms - 1) / sms);
         const double cost = waves * ((double)((ntiles + ns - 1) / ns) + 0.5);
         if (ns == 1 || cost < 0.97 * best_cost) {
@@ -581,7 +588,9 @@ int assign_rows_dev(emb200_handle* h, const T* x, const uint32_t* gather, size_t
     // captured, and a smaller batch can need more split partials than a full one
     // (fewer row tiles, more splits): size them for every batch of up to m rows.
     size_t part_rows = (size_t)nsplit * m;
-    if (graph) {
+    if (graph && h->part_size_m == m && h->part_size_k == h->k && h->part_size_tc == tc) {
+        part_rows = std::max(part_rows, h->part_size_rows);  // the same batch shape as before
+    } else if (graph) {
         for (size_t rt = 1; rt * kTcBM < m + kTcBM; rt++) {
             const size_t mm = std::min(rt * kTcBM, m);
             int ns = 1;
@@ -593,6 +602,10 @@ int assign_rows_dev(emb200_handle* h, const T* x, const uint32_t* gather, size_t
             }
             part_rows = std::max(part_rows, (size_t)ns * mm);
         }
+        h->part_size_m = m;
+        h->part_size_k = h->k;
+        h->part_size_tc = tc;
+        h->part_size_rows = part_rows;
     }
     if (h->part_s.ensure(part_rows * 2) || h->part_i.ensure(part_rows * 2) || h->redo_rows.ensure(m) ||
         h->redo_theta.ensure(m) || h->counters.ensure(8))
