@@ -22,11 +22,11 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libemb200.so")
 
 EMB200_F32, EMB200_I8, EMB200_U8 = 0, 1, 2
-PREC_FP32, PREC_BF16, PREC_BF16X1 = 0, 1, 2
+PREC_FP32, PREC_BF16, PREC_BF16X1, PREC_FP8 = 0, 1, 2, 3
 CENTROIDS_F32, CENTROIDS_I8, CENTROIDS_I16 = 0, 8, 16
 MATCH = {"avx512": 0, "avx2": 1, "portable": 2}
 _DTYPES = {np.dtype(np.float32): EMB200_F32, np.dtype(np.int8): EMB200_I8, np.dtype(np.uint8): EMB200_U8}
-PRECISIONS = {"fp32": PREC_FP32, "bf16": PREC_BF16, "bf16x1": PREC_BF16X1}
+PRECISIONS = {"fp32": PREC_FP32, "bf16": PREC_BF16, "bf16x1": PREC_BF16X1, "fp8": PREC_FP8}
 
 
 class EngineError(RuntimeError):
@@ -35,7 +35,7 @@ class EngineError(RuntimeError):
 
 class _Opts(ctypes.Structure):
     _fields_ = [("precision", ctypes.c_int), ("centroid_bits", ctypes.c_int), ("match_kernel", ctypes.c_int),
-                ("train_eager", ctypes.c_int), ("reserved", ctypes.c_int * 4)]
+                ("train_eager", ctypes.c_int), ("batched_streams", ctypes.c_int), ("reserved", ctypes.c_int * 3)]
 
 
 class _Config(ctypes.Structure):
@@ -121,6 +121,11 @@ def lib():
     L.emb200_assign_device.argtypes = [P, I, P, S, P, P, P]
     L.emb200_load_rows.argtypes = [P, I, P, S, S]
     L.emb200_assign_resident.argtypes = [P, P, P]
+    L.emb200_set_abort_test.argtypes = [P, I, ctypes.c_uint64]
+    L.emb200_measure_simt_peak.argtypes = [I, P, P]
+    L.emb200_batched_search_choice.argtypes = [P, P, P, P]
+    L.emb200_train_proposed.argtypes = [P, ctypes.POINTER(_Config), S, ctypes.POINTER(_ProposerConfig), ctypes.c_uint32,
+                                        ctypes.c_uint32, P, P, P, P, ctypes.POINTER(_Recipe)]
     L.emb200_resolve_recipe.argtypes = [S, S, S, ctypes.POINTER(_Config), ctypes.POINTER(_Recipe), P, S]
     L.emb200_scheduled_alpha.restype = ctypes.c_double
     L.emb200_scheduled_alpha.argtypes = [ctypes.c_double, S, S]
@@ -227,6 +232,15 @@ def scheduled_alpha(alpha0, step, total):
     return lib().emb200_scheduled_alpha(alpha0, step, total)
 
 
+def measure_simt_peak(ordinal=0):
+    """FP32 SIMT FMA throughput of the GPU in TFLOP/s: (scalar FFMA, paired FFMA2)."""
+    a, b = ctypes.c_double(), ctypes.c_double()
+    rc = lib().emb200_measure_simt_peak(ordinal, ctypes.byref(a), ctypes.byref(b))
+    if rc != 0:
+        raise EngineError(f"emb200_measure_simt_peak failed ({rc})")
+    return a.value, b.value
+
+
 def balance_stats(labels, k):
     """balance_stats (src/lib.rs:497-504): (imbalance factor, largest/mean size, empty clusters)."""
     counts = np.bincount(np.asarray(labels, np.int64), minlength=k).astype(np.uint64)
@@ -239,15 +253,16 @@ class B200Assigner:
     """Drop-in for the `Assigner` + `AssignRows<T>` traits (src/lib.rs:75-91),
     beside CpuAssigner (src/cpu.rs) and CpuI8Assigner (src/cpu_i8.rs).
 
-    precision: "fp32" (SIMT), "bf16" (tcgen05, three-term split), "bf16x1".
+    precision: "fp32" (SIMT), "bf16" (tcgen05, three-term split), "bf16x1", "fp8" (tcgen05 e4m3).
     centroid_bits: 0 (CpuAssigner semantics for every row type), 8 or 16
     (CpuI8Assigner(I8) / CpuI8Assigner(I16) semantics for i8 rows). match: which CpuAssigner SIMD
     kernel's rounding the labels and distances reproduce.
     """
 
-    def __init__(self, ordinal=0, precision="fp32", centroid_bits=0, match="avx512", train_eager=False):
+    def __init__(self, ordinal=0, precision="fp32", centroid_bits=0, match="avx512", train_eager=False,
+                 batched_streams=False):
         self._h = ctypes.c_void_p()
-        self._opts = _Opts(PRECISIONS[precision], centroid_bits, MATCH[match], int(train_eager))
+        self._opts = _Opts(PRECISIONS[precision], centroid_bits, MATCH[match], int(train_eager), int(batched_streams))
         rc = lib().emb200_create(ordinal, ctypes.byref(self._opts), ctypes.byref(self._h))
         if rc != 0:
             raise EngineError(f"emb200_create failed ({rc}): no usable B200 (sm_100) device")
@@ -335,6 +350,13 @@ class B200Assigner:
         self._check(lib().emb200_assign_resident(self._h, _p(labels), _p(dist)))
         return labels, dist
 
+    def set_abort_test(self, stall_tile=-1, stall_ns=0):
+        """Test hook of the bounded-wait abort path: the fast tensor-core searches
+        stall one epilogue warp at centroid tile `stall_tile` on a barrier nothing
+        completes, bounded by `stall_ns`; the call then re-searches its rows
+        exactly. stall_tile < 0 turns it off."""
+        self._check(lib().emb200_set_abort_test(self._h, int(stall_tile), int(stall_ns)))
+
     def stats(self):
         s = _Stats()
         self._check(lib().emb200_get_stats(self._h, ctypes.byref(s)))
@@ -344,8 +366,13 @@ class B200Assigner:
         """train() for independent instances over row ranges of the resident rows.
 
         instances: [(row0, n, k), ...]. Returns one Output per instance (labels in
-        the instance's own row order). The instances run concurrently on their own
-        streams with graph-replayed epochs."""
+        the instance's own row order). The instances advance in lockstep, one
+        global step at a time through batched kernels (the search a persistent
+        kernel over an (instance, row tile) work queue, its tile shape chosen by
+        a measured sweep), the step captured once as a CUDA graph; or, with
+        batched_streams=True (and for the cases lockstep does not cover), each on
+        its own stream with graph-replayed epochs. Either way each instance's
+        result equals its own train() call."""
         cfg = cfg or Config()
         n_all, d = self.rows_shape
         inst = np.array([[r0, n, k] for (r0, n, k) in instances], np.uint64).reshape(-1, 3)
@@ -367,6 +394,13 @@ class B200Assigner:
         return outs
 
     # ---- learned proposer ------------------------------------------------
+    def batched_search_choice(self):
+        """(rows, centroids, split_all) of the search tile the autotuner chose for
+        the last lockstep train_batched call."""
+        r, c, sa = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        self._check(lib().emb200_batched_search_choice(self._h, ctypes.byref(r), ctypes.byref(c), ctypes.byref(sa)))
+        return r.value, c.value, bool(sa.value)
+
     def proposer_init(self, groups=256, hidden=512, top=8, mode="mlp", confidence=0.0, batch=4096, lr=2e-3,
                       group_epochs=5.0, seed=1234, mass=0.0):
         """Group the current centroids (e-means with k = groups on the centroids),
@@ -463,6 +497,30 @@ class B200Assigner:
         self._check(lib().emb200_train(self._h, ctypes.byref(c), k, _p(cent), _p(labels), _p(obj), _p(ns),
                                        ctypes.byref(r)))
         self.k, self.d = k, d
+        return Output(cent, labels, obj, int(ns[0]), rec, self.stats())
+
+    def train_resident_proposed(self, k, cfg: Optional[Config] = None, late_epochs=1, net_steps=4000, groups=256,
+                                hidden=512, top=32, confidence=0.0, mass=0.999, batch=4096, lr=2e-3,
+                                group_epochs=5.0, seed=7) -> Output:
+        """train() with the learned proposer searching the last `late_epochs`
+        epochs' batches (emb200_train_proposed): the network is fitted on the
+        labels the full search gave in the epoch before them."""
+        cfg = cfg or Config()
+        n, d = self.rows_shape
+        c = cfg._c()
+        pc = _ProposerConfig(groups, hidden, top, PROPOSER_MODES["mlp"], confidence, batch, lr, group_epochs, seed,
+                             mass)
+        rec = resolve_recipe(n, d, k, cfg)
+        cent = np.empty((k, d), np.float32)
+        labels = np.empty(n, np.uint32)
+        obj = np.empty(len(rec.epoch_rows), np.float64)
+        ns = np.zeros(1, np.uint64)
+        r = _Recipe()
+        self._check(lib().emb200_train_proposed(self._h, ctypes.byref(c), k, ctypes.byref(pc), late_epochs, net_steps,
+                                                _p(cent), _p(labels), _p(obj), _p(ns), ctypes.byref(r)))
+        self.k, self.d = k, d
+        self.proposer_top = top
+        self._proposer_groups_n = groups
         return Output(cent, labels, obj, int(ns[0]), rec, self.stats())
 
 

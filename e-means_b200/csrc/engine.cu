@@ -30,6 +30,8 @@
 #include "kernels_proposer.cuh"
 #include "kernels_quant.cuh"
 #include "kernels_report.cuh"
+#include "kernels_peak.cuh"
+#include "kernels_batched.cuh"
 
 constexpr int kRefineCap = 32;  // candidates kept per refined row
 constexpr size_t kMaxSearchRows = (size_t)1 << 26;  // rows per search pass (32-bit row indexing inside)
@@ -66,7 +68,7 @@ struct DevBuf {
 
 // Device state of a training run (filled by emb200_train).
 struct TrainState {
-    DevBuf<float> usage, sums, pass_sums, batch_dist, alphas;
+    DevBuf<float> usage, sums, pass_sums, batch_dist, alphas, xbatch;
     DevBuf<int> ctl;  // [0] step, [1] epoch, [2] last pass
     DevBuf<double> pass_sums64, keys, scalars, obj, gstream;
     DevBuf<uint32_t> counts, offsets, slot, list, scratch, batch_labels, labels_all, order, didx, unused;
@@ -78,10 +80,30 @@ struct TrainState {
         order_host = nullptr;
         order_host_n = 0;
         usage.release(); sums.release(); pass_sums.release(); batch_dist.release(); alphas.release(); ctl.release();
+        xbatch.release();
         pass_sums64.release(); keys.release(); scalars.release(); obj.release(); gstream.release();
         counts.release(); offsets.release(); slot.release(); list.release(); scratch.release();
         batch_labels.release(); labels_all.release(); order.release(); didx.release(); unused.release();
         pass_counts.release();
+    }
+};
+
+// Device state of a batched lockstep run (emb200_train_batched).
+struct BatchState {
+    DevBuf<uint8_t> inst, steps, ctl;
+    DevBuf<uint32_t> orders, counts, offsets, slot, list, scratch, blabels, labels_all, didx, unused, part_i, items,
+        redo, init, init_off;
+    DevBuf<float> alphas, c, norms, usage, sums, bdist, pass_sums, part_s;
+    DevBuf<Bounds> bounds;
+    DevBuf<unsigned long long> pass_counts, cursor, nsplits;
+    DevBuf<double> pass_sums64, obj, gstream, keys;
+    void release() {
+        inst.release(); steps.release(); ctl.release(); orders.release(); counts.release(); offsets.release();
+        slot.release(); list.release(); scratch.release(); blabels.release(); labels_all.release(); didx.release();
+        unused.release(); part_i.release(); items.release(); redo.release(); init.release(); init_off.release();
+        alphas.release(); c.release(); norms.release(); usage.release(); sums.release(); bdist.release();
+        pass_sums.release(); part_s.release(); bounds.release(); pass_counts.release(); cursor.release();
+        nsplits.release(); pass_sums64.release(); obj.release(); gstream.release(); keys.release();
     }
 };
 
@@ -115,6 +137,12 @@ struct emb200_handle {
     CUtensorMap map_c8{};      // TMA descriptor of c8 (128B swizzle, 128 x 256 boxes)
     bool map_c8_ok = false;
     DevBuf<int> pkeys;         // per-centroid integer keys of the kind::i8 epilogue
+    // FP8 (e4m3) search operands: codes [k][kp8], column factors and scoring norms
+    // (padded to whole tiles), TMA descriptor of the codes
+    DevBuf<uint8_t> c_f8;
+    DevBuf<float> wf8, nf8;
+    CUtensorMap map_f8{};
+    bool f8_ok = false;
 
     // resident rows
     DevBuf<uint8_t> rows;
@@ -146,6 +174,8 @@ struct emb200_handle {
 
     // training state
     TrainState train;
+    BatchState bat;       // batched lockstep training (emb200_train_batched)
+    int bat_variant = -1; // search variant of the last lockstep run (autotuner's choice)
 
     // learned proposer (emb200_proposer_*), and a counter of centroid changes it tracks
     Proposer* prop = nullptr;
@@ -159,6 +189,10 @@ struct emb200_handle {
 
     // report() state (emb200_report*)
     ReportState* rep = nullptr;
+
+    // abort-path test (emb200_set_abort_test): stall of the fast tensor-core kernels
+    int stall_tile = 0;
+    uint64_t stall_ns = 0;
 };
 
 namespace {
@@ -218,6 +252,14 @@ void bound_coefficients(int precision, int dtype, size_t d, bool packed, float* 
     double a;
     if (precision == EMB200_PREC_FP32) {
         a = 2.0 * (gamma((double)d + 2, u) + g_ref) + 4.02 * u;
+    } else if (precision == EMB200_PREC_FP8) {
+        // e4m3 rounding of both operands: relative u8 = 2^-4 for elements in the
+        // binades below the scaled maximum (224, 448], and for the small ones a
+        // floor of 2^-10 / scale <= 2^-10 max / 224 per element, at most
+        // sqrt(d) 2^-10 / 224 |x||c| over a dot product, for each operand.
+        const double u8 = std::ldexp(1.0, -4);
+        const double rep = 2.0 * u8 + u8 * u8 + 2.0 * (1.0 + u8) * std::sqrt((double)d) * std::ldexp(1.0, -10) / 224.0;
+        a = 2.0 * (rep + 1.02 * gamma((double)d + 2, 2 * u) + g_ref) + 4.02 * u;
     } else if (precision == EMB200_PREC_BF16) {
         double terms = dtype == EMB200_F32 ? 3.0 : 2.0;
         double rep = dtype == EMB200_F32 ? 3.2 * ub * ub : 1.1 * ub * ub;  // dropped split terms
@@ -305,6 +347,31 @@ int prepare_centroids(emb200_handle* h) {
     k_prep_centroids<<<(unsigned)((k + 7) / 8), 256, 0, st>>>(h->c.p, k, d, h->norms.p, h->bounds.p, hi, lo,
                                                               (int)h->kpad);
     CKL();
+    h->f8_ok = false;
+    if (h->opts.precision == EMB200_PREC_FP8 && h->d <= 256) {
+        // e4m3 codes in rows of one or two 128-byte swizzle atoms; scoring norms are
+        // the reference norms, -3e38 for a centroid outside the FP8 range (so it can
+        // only be a row's first candidate, which the certification re-scores
+        // exactly), 3e38 for the padding.
+        const size_t kp8 = (h->d + 127) / 128 * 128;
+        if (h->c_f8.ensure((size_t)k * kp8) || h->wf8.ensure(kp) || h->nf8.ensure(kp))
+            return fail(h, EMB200_ENOMEM, "FP8 centroid allocation failed");
+        CK(cudaMemcpyAsync(h->nf8.p, h->norms.p, kp * sizeof(float), cudaMemcpyDeviceToDevice, st));
+        k_prep_fp8<<<(unsigned)((kp * 32 + 255) / 256), 256, 0, st>>>(h->c.p, k, d, (int)kp8, (int)kp, h->c_f8.p,
+                                                                      h->wf8.p, h->nf8.p);
+        CKL();
+        EncodeTiledFn fn = encode_tiled_fn();
+        if (!fn) return fail(h, EMB200_ECUDA, "cuTensorMapEncodeTiled unavailable");
+        cuuint64_t dims[2] = {(cuuint64_t)kp8, (cuuint64_t)h->k};
+        cuuint64_t strides[1] = {(cuuint64_t)kp8};
+        cuuint32_t box[2] = {128, (cuuint32_t)kTcBN};
+        cuuint32_t estr[2] = {1, 1};
+        CUresult r = fn(&h->map_f8, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, h->c_f8.p, dims, strides, box, estr,
+                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+        if (r != CUDA_SUCCESS) return fail(h, EMB200_ECUDA, "cuTensorMapEncodeTiled (fp8) failed (%d)", (int)r);
+        h->f8_ok = true;
+    }
     if (h->opts.centroid_bits == EMB200_CENTROIDS_I8) {
         // Rows of c8 padded to whole 128-byte swizzle atoms (the kind::i8 K atom).
         const size_t kp8 = (h->d + 127) / 128 * 128;
@@ -348,6 +415,10 @@ int apply_bias(emb200_handle* h, const float* bias_dev) {
     const int k = (int)h->k;
     k_add_bias<<<(unsigned)((k + 255) / 256), 256, 0, st>>>(h->norms.p, bias_dev, k, h->bounds.p);
     CKL();
+    if (h->f8_ok) {
+        k_add_bias_f8<<<(unsigned)((k + 255) / 256), 256, 0, st>>>(h->nf8.p, bias_dev, k);
+        CKL();
+    }
     if (h->opts.centroid_bits == EMB200_CENTROIDS_I8 || h->opts.centroid_bits == EMB200_CENTROIDS_I16) {
         const double unit = h->opts.centroid_bits == EMB200_CENTROIDS_I16 ? std::ldexp(1.0, 2 * h->ishift) : 1.0;
         k_bias_i8<<<(unsigned)((k + 255) / 256), 256, 0, st>>>(h->off8.p, bias_dev, k, unit);
@@ -405,6 +476,8 @@ int launch_i8_assign(emb200_handle* h, const int8_t* x, const uint32_t* gather, 
         p.part_s = (long long*)h->part_s.p;
         p.part_i = h->part_i.p;
         p.err = (int*)(h->counters.p + 2);
+        p.stall_tile = h->stall_tile;
+        p.stall_ns = h->stall_ns;
         const TcSmem L = tc_i8_smem_layout(p.kpad);
         const size_t smem = std::max<size_t>(L.total + 1024, 120 * 1024);
         SMEM_ATTR_ONCE(k_assign_tc_i8, kTcSmemLimit);
@@ -455,15 +528,18 @@ int launch_i8_assign(emb200_handle* h, const int8_t* x, const uint32_t* gather, 
 }
 
 // Product terms of the tensor-core search: three for f32 rows (their BF16 split
-// has a low part), two for integer rows (exact in BF16), one for BF16X1.
+// has a low part), two for integer rows (exact in BF16), one for BF16X1 and FP8.
 int tc_terms(int precision, int dtype) {
-    if (precision == EMB200_PREC_BF16X1) return 1;
+    if (precision == EMB200_PREC_BF16X1 || precision == EMB200_PREC_FP8) return 1;
     return dtype == EMB200_F32 ? 3 : 2;
 }
 
-bool tc_supported(const emb200_handle* h, int nterms) {
-    if (!h->maps_ok) return false;
-    TcSmem L = tc_smem_layout((int)h->kpad, nterms);
+// K width of the operands in elements: one 128-byte atom per 64 BF16 or 128 e4m3.
+int tc_kpad(const emb200_handle* h, bool fp8) { return fp8 ? (int)((h->d + 127) / 128 * 128) : (int)h->kpad; }
+
+bool tc_supported(const emb200_handle* h, int nterms, bool fp8 = false) {
+    if (fp8 ? !h->f8_ok : !h->maps_ok) return false;
+    const TcLayout L = tc_layout(tc_kpad(h, fp8), nterms, fp8);
     return L.stages >= 2 && L.total + 1024 <= (uint32_t)kTcSmemLimit;
 }
 
@@ -471,40 +547,59 @@ bool tc_supported(const emb200_handle* h, int nterms) {
 // times the tiles a CTA takes (plus half a tile of per-CTA setup), a larger
 // split only when it saves 3%. 394 row tiles on 148 SMs: 3 splits, 8 waves of 22
 // tiles, against 3 waves of 64 unsplit.
+//
+// Splits with the same tiles per CTA form runs of consecutive counts, and within
+// a run the waves never decrease with the count, so only the first count of each
+// run can be chosen: visiting those (O(sqrt(tiles)) of them) picks the same split
+// as trying every count from 1 to the number of tiles.
 int tc_nsplit(const emb200_handle* h, size_t m) {
     const long row_tiles = (long)((m + kTcBM - 1) / kTcBM);
     const int ntiles = (int)((h->k + kTcBN - 1) / kTcBN);
     const long sms = std::max(1, h->sm_count);
-    // From one full wave of row tiles up, splits only even out the last wave:
-    // 32 give the same choices as all of them (checked up to 40,000 row tiles
-    // and 1024 centroid tiles) and keep the search short.
-    const int max_ns = row_tiles >= sms ? std::min(ntiles, 32) : ntiles;
     int best = 1;
     double best_cost = 0.0;
-    for (int ns = 1; ns <= max_ns; ns++) {
+    for (int ns = 1; ns <= ntiles;) {
+        const int per_cta = (ntiles + ns - 1) / ns;
         const double waves = (double)((row_tiles * ns + sms - 1) / sms);
-        const double cost = waves * ((double)((ntiles + ns - 1) / ns) + 0.5);
+        const double cost = waves * ((double)per_cta + 0.5);
         if (ns == 1 || cost < 0.97 * best_cost) {
             best = ns;
             best_cost = cost;
         }
+        if (per_cta == 1) break;
+        ns = (ntiles + per_cta - 2) / (per_cta - 1);  // first count with fewer tiles per CTA
     }
     return best;
+}
+
+template <typename T, bool COLLECT, bool FP8>
+int launch_tc_kernel(emb200_handle* h, const T* x, const TcParams& p, int nsplit, cudaStream_t st) {
+    const TcLayout L = tc_layout(p.kpad, p.nterms, FP8);
+    // At least 120 KB so that two CTAs never share an SM: each holds all 512 TMEM columns.
+    const size_t smem = std::max<size_t>(L.total + 1024, 120 * 1024);
+    SMEM_ATTR_ONCE((k_assign_tc<T, COLLECT, FP8>), 227 * 1024);  // one flag per instantiation
+    // Persistent: one CTA per SM, or one per work item when there are fewer.
+    const size_t items = (p.m + (size_t)kTcBM - 1) / kTcBM * (size_t)nsplit;
+    const unsigned grid = (unsigned)std::max<size_t>(1, std::min(items, (size_t)h->sm_count));
+    k_assign_tc<T, COLLECT, FP8><<<grid, kTcPThreads, smem, st>>>(x, FP8 ? h->map_f8 : h->map_hi, h->map_lo, p);
+    CKL();
+    return EMB200_OK;
 }
 
 template <typename T, bool COLLECT>
 int launch_tc(emb200_handle* h, const T* x, const uint32_t* gather, const uint32_t* gather2, size_t m, int nterms,
               const float* theta, uint32_t* cand, uint32_t* cand_count, int cap, int* err, cudaStream_t st,
-              const uint32_t* m_dev = nullptr, int nsplit_override = 0) {
+              const uint32_t* m_dev = nullptr, int nsplit_override = 0, bool fp8 = false) {
     TcParams p{};
     p.m = (int)m;
     p.d = (int)h->d;
     p.k = (int)h->k;
-    p.kpad = (int)h->kpad;
+    p.kpad = tc_kpad(h, fp8);
     p.nterms = nterms;
     p.gather = gather;
     p.gather2 = gather2;
-    p.norms = h->norms.p;
+    p.norms = fp8 ? h->nf8.p : h->norms.p;
+    p.wf8 = fp8 ? h->wf8.p : nullptr;
     p.part_s = h->part_s.p;
     p.part_i = h->part_i.p;
     p.err = err;
@@ -514,15 +609,16 @@ int launch_tc(emb200_handle* h, const T* x, const uint32_t* gather, const uint32
     p.cand_count = cand_count;
     p.cand_cap = cap;
     p.m_dev = m_dev;
-    TcSmem L = tc_smem_layout(p.kpad, p.nterms);
-    // At least 120 KB so that two CTAs never share an SM: each holds all 512 TMEM columns.
-    size_t smem = std::max<size_t>(L.total + 1024, 120 * 1024);
-    SMEM_ATTR_ONCE((k_assign_tc<T, COLLECT>), 227 * 1024);  // one flag per <T, COLLECT> instantiation
-    int nsplit = nsplit_override > 0 ? nsplit_override : tc_nsplit(h, m);
-    dim3 grid((unsigned)((m + kTcBM - 1) / kTcBM), (unsigned)nsplit);
-    k_assign_tc<T, COLLECT><<<grid, kTcThreads, smem, st>>>(x, h->map_hi, h->map_lo, p);
-    CKL();
-    return EMB200_OK;
+    if (!COLLECT) {  // the abort-path test stalls the fast search only
+        p.stall_tile = h->stall_tile;
+        p.stall_ns = h->stall_ns;
+    }
+    const int nsplit = nsplit_override > 0 ? nsplit_override : tc_nsplit(h, m);
+    p.nsplit = nsplit;
+    if constexpr (!COLLECT && std::is_same<T, float>::value) {
+        if (fp8) return launch_tc_kernel<T, false, true>(h, x, p, nsplit, st);
+    }
+    return launch_tc_kernel<T, COLLECT, false>(h, x, p, nsplit, st);
 }
 
 // Fold the device counters of one pipeline run into the handle's stats.
@@ -572,11 +668,14 @@ int assign_rows_dev(emb200_handle* h, const T* x, const uint32_t* gather, size_t
         h->stats.fast_kernel = 2;
         return launch_i8_assign(h, (const int8_t*)x, gather, m, labels, dist, st, graph);
     }
-    const int prec = h->opts.precision;
+    int prec = h->opts.precision;
+    // FP8 operands for f32 rows when prepared (d <= 256); otherwise the single-term BF16 search.
+    const bool fp8 = prec == EMB200_PREC_FP8 && dtype == EMB200_F32 && tc_supported(h, 1, true);
+    if (prec == EMB200_PREC_FP8 && !fp8) prec = EMB200_PREC_BF16X1;
     const int row_tiles = (int)((m + kSimtBM - 1) / kSimtBM);
     const int ntiles = (k + kSimtBN - 1) / kSimtBN;
     const int fast_terms = tc_terms(prec, dtype);
-    const bool tc = prec != EMB200_PREC_FP32 && tc_supported(h, fast_terms);
+    const bool tc = prec != EMB200_PREC_FP32 && (fp8 || tc_supported(h, fast_terms));
     int nsplit = 1;
     if (tc) {
         nsplit = tc_nsplit(h, m);
@@ -588,8 +687,9 @@ int assign_rows_dev(emb200_handle* h, const T* x, const uint32_t* gather, size_t
     // captured, and a smaller batch can need more split partials than a full one
     // (fewer row tiles, more splits): size them for every batch of up to m rows.
     size_t part_rows = (size_t)nsplit * m;
-    if (graph && h->part_size_m == m && h->part_size_k == h->k && h->part_size_tc == tc) {
-        part_rows = std::max(part_rows, h->part_size_rows);  // the same batch shape as before
+    if (graph && m <= h->part_size_m && h->part_size_k == h->k && h->part_size_tc == tc) {
+        // Sized before for every batch of up to part_size_m rows, which covers this one.
+        part_rows = std::max(part_rows, h->part_size_rows);
     } else if (graph) {
         for (size_t rt = 1; rt * kTcBM < m + kTcBM; rt++) {
             const size_t mm = std::min(rt * kTcBM, m);
@@ -612,11 +712,11 @@ int assign_rows_dev(emb200_handle* h, const T* x, const uint32_t* gather, size_t
         return fail(h, EMB200_ENOMEM, "scratch allocation failed for %zu rows", m);
     uint32_t* ctr = h->counters.p;
     CK(cudaMemsetAsync(ctr, 0, 8 * sizeof(uint32_t), st));
-    h->stats.fast_kernel = tc ? 1 : 0;
+    h->stats.fast_kernel = fp8 ? 4 : tc ? 1 : 0;
     if (!graph) CK(cudaEventRecord(h->evk0, st));
     if (tc) {
         int rc = launch_tc<T, false>(h, x, gather, nullptr, m, fast_terms, nullptr, nullptr, nullptr, 0,
-                                     (int*)(ctr + 2), st);
+                                     (int*)(ctr + 2), st, nullptr, 0, fp8);
         if (rc) return rc;
     } else {
         dim3 grid(row_tiles, nsplit);
@@ -872,6 +972,7 @@ int emb200_destroy(emb200_handle* h) {
     h->rkeys.release();
     h->qshift.release(); h->qsel.release(); h->qclip.release(); h->qx.release(); h->qcodes.release();
     h->train.release();
+    h->bat.release();
     proposer_release(h);
     report_release(h);
     if (h->ev0) cudaEventDestroy(h->ev0);
@@ -898,7 +999,7 @@ const char* emb200_last_error(const emb200_handle* h) {
 
 int emb200_set_opts(emb200_handle* h, const emb200_opts* opts) {
     if (!h || !opts) return EMB200_EINVAL;
-    if (opts->precision < 0 || opts->precision > 2 || opts->match_kernel < 0 || opts->match_kernel > 2 ||
+    if (opts->precision < 0 || opts->precision > 3 || opts->match_kernel < 0 || opts->match_kernel > 2 ||
         (opts->centroid_bits != 0 && opts->centroid_bits != 8 && opts->centroid_bits != 16))
         return fail(h, EMB200_EINVAL, "invalid options");
     bool rebuild = h->opts.centroid_bits != opts->centroid_bits || h->opts.precision != opts->precision;
@@ -917,8 +1018,10 @@ int emb200_name(emb200_handle* h, char* buf, size_t len) {
     if (!h || !buf || len == 0) return EMB200_EINVAL;
     cudaDeviceProp prop;
     cudaGetDeviceProperties(&prop, h->device);
-    const char* prec = h->opts.precision == EMB200_PREC_FP32 ? "FP32 SIMT"
-                       : h->opts.precision == EMB200_PREC_BF16 ? "BF16x3 tcgen05" : "BF16 tcgen05";
+    const char* prec = h->opts.precision == EMB200_PREC_FP32   ? "FP32 SIMT"
+                       : h->opts.precision == EMB200_PREC_BF16 ? "BF16x3 tcgen05"
+                       : h->opts.precision == EMB200_PREC_FP8  ? "FP8 e4m3 tcgen05"
+                                                               : "BF16 tcgen05";
     const char* match = h->opts.match_kernel == 0 ? "AVX-512" : h->opts.match_kernel == 1 ? "AVX2" : "portable";
     char ib[64] = "";
     if (h->opts.centroid_bits == 8) snprintf(ib, sizeof ib, ", int8 centroids for i8 rows");
@@ -1044,6 +1147,56 @@ int emb200_resolve_recipe(size_t n, size_t d, size_t k, const emb200_config* cfg
 
 double emb200_scheduled_alpha(double alpha0, size_t step, size_t total) { return scheduled_alpha(alpha0, step, total); }
 
+int emb200_measure_simt_peak(int ordinal, double* tflops, double* tflops_paired) {
+    if (!tflops || !tflops_paired) return EMB200_EINVAL;
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || ordinal < 0 || ordinal >= n) return EMB200_EDEVICE;
+    if (cudaSetDevice(ordinal) != cudaSuccess) return EMB200_ECUDA;
+    int sms = 0;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ordinal) != cudaSuccess) return EMB200_ECUDA;
+    const int blocks = sms * 8, threads = 256, iters = 1 << 14;  // 64 warps per SM
+    float* out = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    int rc = EMB200_OK;
+    if (cudaMalloc(&out, (size_t)blocks * threads * sizeof(float)) != cudaSuccess) return EMB200_ENOMEM;
+    if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) rc = EMB200_ECUDA;
+    const double flops = 2.0 * 8.0 * (double)iters * blocks * threads;
+    for (int paired = 0; paired < 2 && rc == EMB200_OK; paired++) {
+        float best = 1e30f;
+        for (int rep = 0; rep < 6; rep++) {  // the first launches warm up; the best of the rest
+            cudaEventRecord(e0);
+            if (paired) k_simt_peak<true><<<blocks, threads>>>(out, iters, 0.999999f, 1e-7f);
+            else k_simt_peak<false><<<blocks, threads>>>(out, iters, 0.999999f, 1e-7f);
+            cudaEventRecord(e1);
+            if (cudaEventSynchronize(e1) != cudaSuccess) {
+                rc = EMB200_ECUDA;
+                break;
+            }
+            float ms = 0.0f;
+            cudaEventElapsedTime(&ms, e0, e1);
+            if (rep >= 2) best = std::min(best, ms);
+        }
+        (paired ? *tflops_paired : *tflops) = flops / (best * 1e-3) / 1e12;
+    }
+    if (cudaGetLastError() != cudaSuccess) rc = EMB200_ECUDA;
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    cudaFree(out);
+    return rc;
+}
+
+int emb200_set_abort_test(emb200_handle* h, int stall_tile, uint64_t stall_ns) {
+    if (!h) return EMB200_EINVAL;
+    if (stall_tile < 0 || stall_ns == 0) {
+        h->stall_tile = 0;
+        h->stall_ns = 0;
+        return EMB200_OK;
+    }
+    h->stall_tile = stall_tile;
+    h->stall_ns = stall_ns;
+    return EMB200_OK;
+}
+
 }  // extern "C"
 
 // ---------------------------------------------------------------------------
@@ -1075,21 +1228,15 @@ constexpr size_t kNoAllocScratchBytes = 256 + 256 + kNoAllocMaxK * 4 + kNoAllocP
 
 __device__ __align__(256) uint8_t g_noalloc_scratch[kNoAllocScratchBytes];
 
-// Device address of g_noalloc_scratch per device ordinal, taken once with that
-// device current (host code must not use the symbol itself as an address).
-std::mutex g_noalloc_mu;
-void* g_noalloc_ptr[64] = {};
-
+// Device address of g_noalloc_scratch in the current device's context. Host code
+// must not use the symbol itself as an address. The lookup is repeated on every
+// call (a host-side query, no allocation): a cached address would go stale when
+// the caller resets the device or switches to another context on the same
+// device, where the module's array can sit elsewhere.
 int noalloc_scratch(void** out) {
-    int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return EMB200_EDEVICE;
-    std::lock_guard<std::mutex> lock(g_noalloc_mu);
-    if (!g_noalloc_ptr[dev]) {
-        void* p = nullptr;
-        if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return EMB200_ECUDA;
-        g_noalloc_ptr[dev] = p;
-    }
-    *out = g_noalloc_ptr[dev];
+    void* p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return EMB200_ECUDA;
+    *out = p;
     return EMB200_OK;
 }
 
@@ -1099,7 +1246,8 @@ extern "C" int emb200_assign_f32_noalloc(const float* x_dev, size_t m, size_t d,
                                          size_t k, uint32_t* labels_dev, float* dist_dev, int match_kernel,
                                          void* stream) {
     if (m > kNoAllocMaxRows || k > kNoAllocMaxK) return EMB200_ELIMIT;
-    if (d == 0 || k == 0 || d > 0x7FFFFFFF) return EMB200_EINVAL;
+    // d rounded up to 64 (the padded width the centroid preparation takes) must fit in an int.
+    if (d == 0 || k == 0 || d > (size_t)0x7FFFFFFF - 63) return EMB200_EINVAL;
     if (match_kernel < 0 || match_kernel > 2) return EMB200_EINVAL;
     if (m == 0) return EMB200_OK;
     if (!x_dev || !centroids_dev || !labels_dev || !dist_dev) return EMB200_EINVAL;
@@ -1142,6 +1290,7 @@ extern "C" int emb200_assign_f32_noalloc(const float* x_dev, size_t m, size_t d,
     return cudaGetLastError() == cudaSuccess ? EMB200_OK : EMB200_ECUDA;
 }
 
+#include "engine_batched.inc"
 #include "engine_train.inc"
 #include "engine_proposer.inc"
 #include "engine_quant.inc"

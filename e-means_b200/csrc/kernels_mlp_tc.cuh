@@ -130,7 +130,8 @@ k_mlp_tc(const __grid_constant__ CUtensorMap map_w1, const __grid_constant__ CUt
     uint64_t* empty = full + kMlpMaxStages;       // [kMlpMaxStages]
     uint64_t* acc_full = empty + kMlpMaxStages;   // MMA -> epilogue, once per layer
     uint64_t* a_ready = acc_full + 1;             // epilogue -> MMA, once per layer (16 warp arrivals)
-    uint32_t* tmem_slot = (uint32_t*)(a_ready + 1);
+    uint64_t* mma_done = a_ready + 1;             // every issued MMA completed (teardown)
+    uint32_t* tmem_slot = (uint32_t*)(mma_done + 1);
     volatile int* abort_flag = (volatile int*)(tmem_slot + 1);
     uint8_t* act = smem + L.act;
 
@@ -146,6 +147,7 @@ k_mlp_tc(const __grid_constant__ CUtensorMap map_w1, const __grid_constant__ CUt
         }
         mbar_init(acc_full, 1);
         mbar_init(a_ready, kTcEpiWarps);
+        mbar_init(mma_done, 1);
         *abort_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
@@ -220,6 +222,7 @@ k_mlp_tc(const __grid_constant__ CUtensorMap map_w1, const __grid_constant__ CUt
                     if (ok) mma_commit(acc_full);
                 }
             }
+            mma_drain(mma_done);  // no MMA may outlive the TMEM allocation (see k_assign_tc)
         }
     } else {
         const int q = warp & 3;          // TMEM lane quarter

@@ -41,6 +41,12 @@ constexpr int kTcTmemCols = 512;  // two 256-column accumulators
 // therefore refilled (for tile t+8) only after every warp is done with tile t.
 constexpr int kTcNormSlots = 8;
 constexpr int kTcSmemLimit = 227 * 1024;
+// The persistent search kernel k_assign_tc adds two row-loading warps (2, 3)
+// before its 16 epilogue warps (4..19).
+constexpr int kTcLoadWarps = 2;
+constexpr int kTcEpi0 = 2 + kTcLoadWarps;
+constexpr int kTcPThreads = 32 * (kTcEpi0 + kTcEpiWarps);
+constexpr int kTcRowScaleSlots = 4;  // FP8 per-row scales, a ring over work items
 
 struct TcParams {
     int m, d, k, kpad;   // kpad: d rounded up to 64 (one 128-byte swizzle atom per 64 BF16)
@@ -64,6 +70,16 @@ struct TcParams {
     const int2* tile_info;
     const __nv_bfloat16* rows_hi;  // grouped search: the chunk's rows split into BF16 hi / lo, [rows][kpad]
     const __nv_bfloat16* rows_lo;
+    // Test of the bounded-wait abort path: when stall_ns > 0, the first epilogue
+    // warp waits at tile stall_tile on a barrier nothing completes, with limit
+    // stall_ns, so the wait runs out and the kernel takes its abort path (results
+    // re-searched). Zero (the default of a zeroed struct): off.
+    int stall_tile;
+    uint64_t stall_ns;
+    // FP8 (e4m3) operands: rows scaled per row by a power of two and centroids per
+    // centroid; wf8[j] = -2 / (centroid j's scale), 0 past k (score = norm + acc r w).
+    const float* wf8;
+    int nsplit;  // column splits of the search (work item = row tile x split)
 };
 
 // ---- PTX wrappers -----------------------------------------------------------
@@ -106,19 +122,30 @@ EMB_DEV uint64_t global_ns() {
 constexpr uint64_t kWaitLimitNs = 4000000000ull;  // a healthy wait takes microseconds
 
 // Bounded wait: returns false (and raises the abort flag) if the phase does not
-// complete within kWaitLimitNs, or if another role already aborted.
-EMB_DEV bool mbar_wait(uint64_t* bar, uint32_t parity, volatile int* abort_flag, uint32_t hint_ns = 0) {
+// complete within limit_ns, or if another role already aborted.
+EMB_DEV bool mbar_wait(uint64_t* bar, uint32_t parity, volatile int* abort_flag, uint32_t hint_ns = 0,
+                       uint64_t limit_ns = kWaitLimitNs) {
     if (mbar_try(bar, parity)) return true;
     const uint64_t t0 = global_ns();
     for (uint32_t i = 1;; i++) {
         if (hint_ns ? mbar_try_sleep(bar, parity, hint_ns) : mbar_try(bar, parity)) return true;
         if ((i & 63) == 0) {
             if (*abort_flag) return false;
-            if (global_ns() - t0 > kWaitLimitNs) {
+            if (global_ns() - t0 > limit_ns) {
                 *abort_flag = 1;
                 return false;
             }
         }
+    }
+}
+
+// Wait, bounded by kWaitLimitNs and whatever the abort flag says, for a phase
+// that is certain to complete (copies or MMAs already issued): used on the way
+// out of a kernel, so that no asynchronous operation still reads or writes
+// shared memory or TMEM when the CTA frees them.
+EMB_DEV void mbar_drain(uint64_t* bar, uint32_t parity) {
+    const uint64_t t0 = global_ns();
+    while (!mbar_try(bar, parity) && global_ns() - t0 < kWaitLimitNs) {
     }
 }
 
@@ -166,6 +193,15 @@ EMB_DEV void mma_commit(uint64_t* bar) {
                  : "memory");
 }
 
+// Called once by the MMA-issuing thread before it leaves, normally or after an
+// abort: a commit tracks every tcgen05.mma the thread issued before it, so once
+// `bar` (initialised with one arrival, used only here) completes its phase no
+// MMA is still reading shared memory or writing TMEM, and TMEM may be freed.
+EMB_DEV void mma_drain(uint64_t* bar) {
+    mma_commit(bar);
+    mbar_drain(bar, 0);
+}
+
 #define EMB_TMEM_LD32(taddr, r)                                                                                  \
     asm volatile(                                                                                                \
         "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"        \
@@ -185,27 +221,42 @@ struct TcSmem {
     int stages;
 };
 
-__host__ __device__ inline TcSmem tc_smem_layout(int kpad, int nterms) {
-    TcSmem s;
-    const uint32_t a_bytes = (uint32_t)kTcBM * kpad * 2;
-    const uint32_t b_term = (uint32_t)kTcBN * 128;  // one K atom (64 BF16) of 256 centroids
-    const int bterms = nterms == 1 ? 1 : 2;
-    s.a_hi = 0;
-    s.a_lo = a_bytes;
-    const uint32_t a_total = nterms == 3 ? 2 * a_bytes : a_bytes;
-    s.b0 = a_total;
-    s.term_bytes = b_term;
-    s.stage_bytes = b_term * bterms;
-    // norms, merge, barriers, published top-2 keys, alignment
-    const uint32_t fixed = kTcNormSlots * kTcBN * 4 + 3 * kTcBM * 16 + 256 + 4 * kTcBM * 8 + 1024;
+// Shared memory of the persistent search kernel k_assign_tc (offsets in bytes from
+// a 1024-aligned base). kpad is d rounded up to one 128-byte swizzle atom per row:
+// 64 BF16 or 128 e4m3 elements.
+struct TcLayout {
+    uint32_t a_buf;        // bytes of one row-tile buffer (hi, then lo for three terms)
+    uint32_t a_lo;         // offset of the lo part inside a buffer
+    uint32_t b0, stage_bytes, term_bytes;
+    uint32_t norms, nrm_slot_bytes;  // ring of per-tile norms (FP8: norms, then column factors)
+    uint32_t rscale;       // FP8: ring of per-row scales [kTcRowScaleSlots][128]
+    uint32_t merge, bars, pub, total;
+    int stages, nbuf;
+};
+
+__host__ __device__ inline TcLayout tc_layout(int kpad, int nterms, bool fp8) {
+    TcLayout s;
+    const uint32_t a_term = (uint32_t)kTcBM * (uint32_t)kpad * (fp8 ? 1u : 2u);
+    s.a_buf = a_term * ((!fp8 && nterms == 3) ? 2u : 1u);
+    s.a_lo = a_term;
+    s.term_bytes = (uint32_t)kTcBN * 128;  // one K atom of 256 centroids
+    s.stage_bytes = s.term_bytes * ((fp8 || nterms == 1) ? 1u : 2u);
+    s.nrm_slot_bytes = (uint32_t)kTcBN * 4 * (fp8 ? 2u : 1u);
+    const uint32_t fixed = kTcNormSlots * s.nrm_slot_bytes + kTcRowScaleSlots * kTcBM * 4 + 3 * kTcBM * 16 + 256 +
+                           4 * kTcBM * 4 + 1024;
+    // Two row-tile buffers (the next tile's rows load while the current one is
+    // searched) when they leave room for three stages, else one.
+    s.nbuf = 2 * s.a_buf + 3 * s.stage_bytes + fixed <= (uint32_t)kTcSmemLimit ? 2 : 1;
     int st = 0;
-    while (st < kTcMaxStages && a_total + (st + 1) * s.stage_bytes + fixed <= (uint32_t)kTcSmemLimit) st++;
+    while (st < kTcMaxStages && s.nbuf * s.a_buf + (st + 1) * s.stage_bytes + fixed <= (uint32_t)kTcSmemLimit) st++;
     s.stages = st;
-    s.norms = s.b0 + st * s.stage_bytes;                 // [8][256] f32
-    s.merge = s.norms + kTcNormSlots * kTcBN * 4;        // [3][128] x (s1, i1, s2, i2)
+    s.b0 = s.nbuf * s.a_buf;
+    s.norms = s.b0 + st * s.stage_bytes;
+    s.rscale = s.norms + kTcNormSlots * s.nrm_slot_bytes;
+    s.merge = s.rscale + kTcRowScaleSlots * kTcBM * 4;
     s.bars = s.merge + 3 * kTcBM * 16;
-    s.pub = s.bars + 256;                                // [4 column quarters][128 rows] float2 (s1, s2)
-    s.total = s.pub + 4 * kTcBM * 8;
+    s.pub = s.bars + 256;                  // [4 column quarters][128 rows] published best key
+    s.total = s.pub + 4 * kTcBM * 4;
     return s;
 }
 
@@ -217,12 +268,20 @@ EMB_DEV uint32_t sw128_offset(int r, int kc, int rows) {
     return (uint32_t)(atom * rows * 128 + r * 128 + ((c ^ (r & 7)) << 4));
 }
 
+// Source row of kernel row g: through the optional first-level map, then the gather.
+EMB_DEV size_t tc_src_row(const TcParams& p, int g) {
+    size_t src = p.gather2 ? (size_t)p.gather2[g] : (size_t)g;
+    if (p.gather) src = p.gather[src];
+    return src;
+}
+
+// Row tile -> BF16 hi (and lo for three terms) in the K-major 128B-swizzled layout,
+// by threads tid = 0 .. nthr-1: 128 rows x (kpad / 8) chunks of 8 elements. Each
+// thread issues the loads of up to four chunks before converting any of them, so
+// that the gathered rows' latencies overlap.
 template <typename T>
-EMB_DEV void tc_load_rows(uint8_t* smem, const TcSmem& L, const T* __restrict__ x, const TcParams& p, int row0,
-                          int m, int tid, int nthr) {
-    // 128 rows x (kpad / 8) chunks of 8 elements. Each thread issues the loads of
-    // up to four chunks before converting any of them, so that four gathered
-    // rows' latencies overlap instead of following one another.
+EMB_DEV void tc_load_rows(uint8_t* a_hi, uint8_t* a_lo, const T* __restrict__ x, const TcParams& p, int row0, int m,
+                          int tid, int nthr) {
     constexpr int kBatch = 4;
     const int nchunk = p.kpad / 8;
     const int total = kTcBM * nchunk;
@@ -237,9 +296,7 @@ EMB_DEV void tc_load_rows(uint8_t* smem, const TcSmem& L, const T* __restrict__ 
             const int r = t / nchunk, kc = t % nchunk;
             const int g = row0 + r;
             if (g >= m) continue;
-            size_t src = p.gather2 ? (size_t)p.gather2[g] : (size_t)g;
-            if (p.gather) src = p.gather[src];
-            const T* xr = x + src * (size_t)p.d;
+            const T* xr = x + tc_src_row(p, g) * (size_t)p.d;
             const int k0 = kc * 8;
             if (sizeof(T) == 4 && p.xvec && k0 + 8 <= p.d) {
                 const float4 a = *reinterpret_cast<const float4*>(xr + k0);
@@ -266,8 +323,82 @@ EMB_DEV void tc_load_rows(uint8_t* smem, const TcSmem& L, const T* __restrict__ 
                 lw[i] = (uint32_t)__bfloat16_as_ushort(l0) | ((uint32_t)__bfloat16_as_ushort(l1) << 16);
             }
             const uint32_t off = sw128_offset(r, kc, kTcBM);
-            *reinterpret_cast<uint4*>(smem + L.a_hi + off) = make_uint4(hw[0], hw[1], hw[2], hw[3]);
-            if (p.nterms == 3) *reinterpret_cast<uint4*>(smem + L.a_lo + off) = make_uint4(lw[0], lw[1], lw[2], lw[3]);
+            *reinterpret_cast<uint4*>(a_hi + off) = make_uint4(hw[0], hw[1], hw[2], hw[3]);
+            if (p.nterms == 3) *reinterpret_cast<uint4*>(a_lo + off) = make_uint4(lw[0], lw[1], lw[2], lw[3]);
+        }
+    }
+}
+
+// Largest magnitudes for which the FP8 operands keep their error bound: the
+// scale below stays a normal power of two and e4m3 rounding stays relative
+// (plus a floor the bound covers) for elements near the largest.
+constexpr float kFp8MinMag = 0x1p-60f, kFp8MaxMag = 0x1p60f;
+
+// Power-of-two scale that maps a largest magnitude mx into (224, 448], the top
+// binade of e4m3 (448 is its largest finite value). Outside [kFp8MinMag,
+// kFp8MaxMag] (zero, tiny, huge, inf or NaN) the scale is 1 and *ok false.
+EMB_DEV float fp8_scale(float mx, bool* ok) {
+    *ok = mx >= kFp8MinMag && mx <= kFp8MaxMag;
+    if (!*ok) return 1.0f;
+    return __uint_as_float(__float_as_uint(448.0f / mx) & 0xFF800000u);  // round down to a power of two
+}
+
+// Two scaled values -> two e4m3 bytes (round to nearest, saturating to +-448).
+EMB_DEV uint32_t fp8x2(float a, float b) {
+    uint16_t r;
+    asm("cvt.rn.satfinite.e4m3x2.f32 %0, %2, %1;" : "=h"(r) : "f"(a), "f"(b));
+    return r;
+}
+
+// Row tile -> e4m3, one power-of-two scale per row (fp8_scale of its largest
+// magnitude), K-major 128B-swizzled: 16-byte chunks of 16 elements, kpad / 16 (8
+// or 16) consecutive threads per row, the row maximum reduced across them by
+// shuffles. rscale[r] = 1 / scale (exact). Threads tid = 0 .. 63.
+template <typename T>
+EMB_DEV void tc_load_rows_fp8(uint8_t* a, float* rscale, const T* __restrict__ x, const TcParams& p, int row0, int m,
+                              int tid) {
+    const int cpr = p.kpad / 16;          // 8 or 16 threads per row
+    const int rpp = 64 / cpr;             // rows per pass
+    for (int rb = 0; rb < kTcBM; rb += 2 * rpp) {
+        float v[2][16];
+#pragma unroll
+        for (int u = 0; u < 2; u++) {
+            const int r = rb + u * rpp + tid / cpr, kc = tid % cpr;
+            const int g = row0 + r;
+#pragma unroll
+            for (int i = 0; i < 16; i++) v[u][i] = 0.0f;
+            if (g < m) {
+                const T* xr = x + tc_src_row(p, g) * (size_t)p.d;
+                const int k0 = kc * 16;
+                if (sizeof(T) == 4 && p.xvec && k0 + 16 <= p.d) {
+#pragma unroll
+                    for (int q = 0; q < 4; q++) {
+                        const float4 f = *reinterpret_cast<const float4*>(xr + k0 + 4 * q);
+                        v[u][4 * q] = f.x; v[u][4 * q + 1] = f.y; v[u][4 * q + 2] = f.z; v[u][4 * q + 3] = f.w;
+                    }
+                } else {
+                    for (int i = 0; i < 16; i++) v[u][i] = (k0 + i < p.d) ? to_f32(xr[k0 + i]) : 0.0f;
+                }
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < 2; u++) {
+            const int r = rb + u * rpp + tid / cpr, kc = tid % cpr;
+            float mx = 0.0f;
+#pragma unroll
+            for (int i = 0; i < 16; i++) mx = fmaxf(mx, fabsf(v[u][i]));
+            for (int o = cpr >> 1; o; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+            bool in_range;
+            const float sc = fp8_scale(mx, &in_range);
+            uint32_t w[4];
+#pragma unroll
+            for (int q = 0; q < 4; q++)
+                w[q] = fp8x2(v[u][4 * q] * sc, v[u][4 * q + 1] * sc) | (fp8x2(v[u][4 * q + 2] * sc, v[u][4 * q + 3] * sc) << 16);
+            *reinterpret_cast<uint4*>(a + sw128_offset(r, kc, kTcBM)) = make_uint4(w[0], w[1], w[2], w[3]);
+            // A zero row is exact (every product 0). Any other row outside the range
+            // gets a NaN scale: all its scores are NaN, no candidate survives, and
+            // the certification sends it to the exact search.
+            if (kc == 0) rscale[r] = in_range ? 1.0f / sc : (mx == 0.0f ? 1.0f : __int_as_float(0x7fc00000));
         }
     }
 }
@@ -416,42 +547,185 @@ EMB_DEV void tc_regs_ready(uint32_t (&v)[32]) {
     for (int j = 0; j < 32; j++) asm volatile("" : "+r"(v[j]));
 }
 
-// Grid: (ceil(m / 128), nsplit); CTA (bx, by) walks centroid tiles by, by + nsplit, ...
-// COLLECT = false: per-row top-2 of approximate scores to part_s/part_i.
+// FP8 centroid operands: per centroid a power-of-two scale (fp8_scale of its
+// largest magnitude), the e4m3 codes of c * scale in rows of kp8 bytes (zeros
+// past d), and w[j] = -2 / scale (exact), 0 for the padding up to kp. A centroid
+// whose largest magnitude is outside [kFp8MinMag, kFp8MaxMag] (and not zero) gets
+// w = 0 and scoring norm nf8[j] = -3e38: its approximate score is below every
+// other, so it can only be a row's first candidate, which the certification
+// re-scores exactly (two such columns leave no margin: refine). nf8 holds the
+// reference norms otherwise. One warp per centroid.
+__global__ void k_prep_fp8(const float* __restrict__ c, int k, int d, int kp8, int kp, uint8_t* __restrict__ c8,
+                           float* __restrict__ w, float* __restrict__ nf8) {
+    const int j = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (j >= kp) return;
+    if (j >= k) {
+        if (lane == 0) w[j] = 0.0f;
+        return;
+    }
+    const float* cj = c + (size_t)j * d;
+    float mx = 0.0f;
+    for (int i = lane; i < d; i += 32) mx = fmaxf(mx, fabsf(cj[i]));
+    for (int o = 16; o; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    bool in_range;
+    const float sc = fp8_scale(mx, &in_range);
+    for (int i = 2 * lane; i < kp8; i += 64) {
+        const float a = i < d ? cj[i] * sc : 0.0f, b = i + 1 < d ? cj[i + 1] * sc : 0.0f;
+        *reinterpret_cast<uint16_t*>(c8 + (size_t)j * kp8 + i) = (uint16_t)fp8x2(a, b);
+    }
+    if (lane == 0) {
+        w[j] = in_range ? -2.0f / sc : 0.0f;
+        if (!in_range && mx != 0.0f) nf8[j] = -3.0e38f;
+    }
+}
+
+// The bias on the FP8 scoring norms (set_bias adds it to the reference norms;
+// a -3e38 entry stays far below every real score).
+__global__ void k_add_bias_f8(float* __restrict__ nf8, const float* __restrict__ bias, int k) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j < k) nf8[j] = __fadd_rn(nf8[j], bias[j]);
+}
+
+#define EMB_TMEM_LD16(taddr, r)                                                                                  \
+    asm volatile(                                                                                                \
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];" \
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),      \
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])  \
+        : "r"(taddr))
+
+EMB_DEV void tc_regs_ready16(uint32_t (&v)[16]) {
+#pragma unroll
+    for (int j = 0; j < 16; j++) asm volatile("" : "+r"(v[j]));
+}
+
+// FP8 (e4m3 x e4m3 -> f32) instruction descriptor, both operands K-major, M x N.
+__host__ __device__ constexpr uint32_t idesc_e4m3(int M, int N) {
+    return (1u << 4) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
+EMB_DEV void mma_e4m3(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc, uint32_t accumulate) {
+    asm volatile(
+        "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+        " tcgen05.mma.cta_group::1.kind::f8f6f4 [%0], %1, %2, %3, p;\n}\n"
+        ::"r"(d_tmem), "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate));
+}
+
+// Scores of 16 accumulator columns (in place): s = norm - 2 acc (BF16), or
+// s = norm + (acc r) w (FP8: acc r undoes the row's power-of-two scale exactly,
+// w = -2 / the centroid's scale), one rounding each.
+template <bool FP8>
+EMB_DEV void tc_scores16(uint32_t (&v)[16], const float* __restrict__ nrm, const float* __restrict__ wcol, float rs,
+                         float (&s)[16]) {
+#pragma unroll
+    for (int j = 0; j < 16; j += 4) {
+        const float4 n4 = *reinterpret_cast<const float4*>(nrm + j);
+        if (FP8) {
+            const float4 w4 = *reinterpret_cast<const float4*>(wcol + j);
+            s[j] = fmaf(__uint_as_float(v[j]) * rs, w4.x, n4.x);
+            s[j + 1] = fmaf(__uint_as_float(v[j + 1]) * rs, w4.y, n4.y);
+            s[j + 2] = fmaf(__uint_as_float(v[j + 2]) * rs, w4.z, n4.z);
+            s[j + 3] = fmaf(__uint_as_float(v[j + 3]) * rs, w4.w, n4.w);
+        } else {
+            fma2_scores(__uint_as_float(v[j]), __uint_as_float(v[j + 1]), n4.x, n4.y, s[j], s[j + 1]);
+            fma2_scores(__uint_as_float(v[j + 2]), __uint_as_float(v[j + 3]), n4.z, n4.w, s[j + 2], s[j + 3]);
+        }
+    }
+}
+
+// Smallest of 16 scores (NaN-ignoring).
+EMB_DEV float tc_min16s(const float (&s)[16]) {
+    const float a = min3f(s[0], s[1], s[2]), b = min3f(s[3], s[4], s[5]), c = min3f(s[6], s[7], s[8]);
+    const float d = min3f(s[9], s[10], s[11]), e = min3f(s[12], s[13], s[14]);
+    return fminf(min3f(a, b, c), min3f(d, e, s[15]));
+}
+
+// Two smallest keys of 16 scores: each score's 5 low mantissa bits replaced by
+// its column jb + j (jb a multiple of 16 within a 32-column chunk; a relative
+// change below 2^-18, which the error bound covers), so min/max carry the column.
+EMB_DEV void tc_top2_16s(const float (&s)[16], uint32_t jb, float& k1, float& k2) {
+    float lo[8], hi[8];
+#pragma unroll
+    for (int q = 0; q < 8; q++) {
+        const float a = __uint_as_float((__float_as_uint(s[2 * q]) & ~31u) | (jb + 2 * q));
+        const float b = __uint_as_float((__float_as_uint(s[2 * q + 1]) & ~31u) | (jb + 2 * q + 1));
+        lo[q] = fminf(a, b);
+        hi[q] = fmaxf(a, b);
+    }
+#pragma unroll
+    for (int w = 4; w >= 1; w >>= 1) {
+#pragma unroll
+        for (int q = 0; q < w; q++) {
+            const float a1 = lo[q], a2 = hi[q], b1 = lo[q + w], b2 = hi[q + w];
+            lo[q] = fminf(a1, b1);
+            hi[q] = min3f(fmaxf(a1, b1), a2, b2);
+        }
+    }
+    k1 = lo[0];
+    k2 = hi[0];
+}
+
+// The per-row state of one epilogue warp (a quarter of each tile's columns).
+// s1 is the key of column i1; s2 lower-bounds the approximate score of every
+// other column the warp has scored. s2 < s1 is allowed: a half-chunk whose
+// smallest score cannot be the row's best (another quarter already holds a
+// smaller key) only lowers s2 and costs one min, and the keyed tournament that
+// tracks columns runs only where a new best is possible.
+struct TcBest {
+    float s1, s2;
+    uint32_t i1;
+};
+
+// Persistent fused search. Grid: one CTA per SM (at most the number of work
+// items). Work item w = (row tile w / nsplit, column split w % nsplit); CTA b takes
+// items b, b + gridDim.x, ... A split walks centroid tiles split, split + nsplit, ...
+//   warp 0      TMA producer of the centroid stages (and each tile's norms)
+//   warp 1      TMEM allocation; tcgen05.mma issue (one thread)
+//   warps 2-3   row loaders: the next work item's row tile into the other buffer
+//               (BF16 hi/lo split or e4m3 with a per-row scale)
+//   warps 4-19  epilogue, four warps per TMEM lane quarter, 64 columns of each
+//               256-column tile per warp, read 16 at a time with the next TMEM
+//               load in flight while the current 16 are scored
+// COLLECT = false: per-row (best key, column, lower bound of the rest) to part_s/part_i.
 // COLLECT = true : every centroid with approximate score <= theta[row] is appended
 //                  to cand[row][*] (cand_count[row] counts all, capped storage).
-template <typename T, bool COLLECT>
-__global__ void __launch_bounds__(kTcThreads, 1)
+template <typename T, bool COLLECT, bool FP8>
+__global__ void __launch_bounds__(kTcPThreads, 1)
 k_assign_tc(const T* __restrict__ x, const __grid_constant__ CUtensorMap map_hi,
             const __grid_constant__ CUtensorMap map_lo, const TcParams p) {
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
-    const TcSmem L = tc_smem_layout(p.kpad, p.nterms);
-    const int S = L.stages;
+    const TcLayout L = tc_layout(p.kpad, p.nterms, FP8);
+    const int S = L.stages, NB = L.nbuf;
     uint64_t* full = (uint64_t*)(smem + L.bars);          // [kTcMaxStages]
     uint64_t* empty = full + kTcMaxStages;                // [kTcMaxStages]
     uint64_t* acc_full = empty + kTcMaxStages;            // [2]
     uint64_t* acc_empty = acc_full + 2;                   // [2]
     uint64_t* norms_full = acc_empty + 2;                 // [kTcNormSlots]
-    uint32_t* tmem_slot = (uint32_t*)(norms_full + kTcNormSlots);
+    uint64_t* a_full = norms_full + kTcNormSlots;         // [2] row tile loaded
+    uint64_t* a_empty = a_full + 2;                       // [2] every MMA reading the row buffer completed
+    uint64_t* rs_full = a_empty + 2;                      // [kTcRowScaleSlots] FP8 row scales written
+    uint64_t* mma_done = rs_full + kTcRowScaleSlots;      // every issued MMA completed (teardown)
+    uint64_t* stall_bar = mma_done + 1;                   // never completed (abort-path test)
+    uint32_t* tmem_slot = (uint32_t*)(stall_bar + 1);     // 30 barriers: 240 of the 256 bytes
     volatile int* abort_flag = (volatile int*)(tmem_slot + 1);
     float* norms_s = (float*)(smem + L.norms);
+    float* rscale_s = (float*)(smem + L.rscale);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int row0 = blockIdx.x * kTcBM;
     int m = p.m;
     if (COLLECT && p.m_dev) {
-        // Row count known only on the device (graph-captured refine): CTAs past it leave at once.
+        // Row count known only on the device (graph-captured refine).
         const int md = (int)*p.m_dev;
         m = md < m ? md : m;
-        if (row0 >= m) return;
     }
-    const int nsplit = gridDim.y;
+    const int nsplit = p.nsplit;
+    const int nitems = ((m + kTcBM - 1) / kTcBM) * nsplit;
+    if ((int)blockIdx.x >= nitems) return;  // no work: the whole CTA leaves before any setup
+    const int my_items = (nitems - (int)blockIdx.x + (int)gridDim.x - 1) / (int)gridDim.x;
     const int ntiles_all = (p.k + kTcBN - 1) / kTcBN;
-    const int my_tiles = (int)blockIdx.y < ntiles_all ? (ntiles_all - (int)blockIdx.y + nsplit - 1) / nsplit : 0;
-    // Column of this CTA's tile t: col_first + t * col_step.
-    const int col_first = (int)blockIdx.y * kTcBN, col_step = nsplit * kTcBN;
-    const int natoms = p.kpad / 64;
+    auto item_of = [&](int i) { return (int)blockIdx.x + i * (int)gridDim.x; };
+    auto tiles_of = [&](int split) { return split < ntiles_all ? (ntiles_all - split + nsplit - 1) / nsplit : 0; };
+    const int natoms = FP8 ? p.kpad / 128 : p.kpad / 64;
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < kTcMaxStages; s++) {
@@ -461,41 +735,21 @@ k_assign_tc(const T* __restrict__ x, const __grid_constant__ CUtensorMap map_hi,
         for (int b = 0; b < 2; b++) {
             mbar_init(&acc_full[b], 1);
             mbar_init(&acc_empty[b], kTcEpiWarps);  // one arrival per epilogue warp
+            mbar_init(&a_full[b], kTcLoadWarps * 32);
+            mbar_init(&a_empty[b], 1);
         }
         for (int i = 0; i < kTcNormSlots; i++) mbar_init(&norms_full[i], 1);
+        for (int i = 0; i < kTcRowScaleSlots; i++) mbar_init(&rs_full[i], kTcLoadWarps * 32);
+        mbar_init(mma_done, 1);
+        mbar_init(stall_bar, 1);
         *abort_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     if (warp == 1) tmem_alloc(tmem_slot, kTcTmemCols);
-    // ---- TMA producer unit u = (tile t, K atom a) into stage u % S; norms once per tile
-    const int nunits = my_tiles * natoms;
-    auto issue = [&](int u) {
-        const int t = u / natoms, a = u - t * natoms;
-        const int s = u % S;
-        const int col = col_first + t * col_step;
-        uint8_t* stage = smem + L.b0 + s * L.stage_bytes;
-        mbar_expect_tx(&full[s], L.stage_bytes);
-        tma_load_2d(stage, &map_hi, &full[s], a * 64, col);
-        if (p.nterms > 1) tma_load_2d(stage + L.term_bytes, &map_lo, &full[s], a * 64, col);
-        if (a == 0) {
-            const int ns = t % kTcNormSlots;
-            mbar_expect_tx(&norms_full[ns], kTcBN * 4);
-            bulk_load(norms_s + ns * kTcBN, p.norms + (size_t)col, kTcBN * 4, &norms_full[ns]);
-        }
-    };
-    __syncthreads();  // barriers initialised: the first stages load while the rows are gathered
-    int issued = 0;
-    if (warp == 0 && lane == 0) {
-        // The first S stages are free: no wait on `empty` before them.
-        issued = nunits < S ? nunits : S;
-        for (int u = 0; u < issued; u++) issue(u);
+    {  // published best keys start at +inf
+        float* pub = (float*)(smem + L.pub);
+        for (int i = threadIdx.x; i < 4 * kTcBM; i += blockDim.x) pub[i] = INFINITY;
     }
-    tc_load_rows(smem, L, x, p, row0, m, threadIdx.x, blockDim.x);
-    {  // published top-2 pairs of the single-term epilogue start at +inf
-        float2* pub = (float2*)(smem + L.pub);
-        for (int i = threadIdx.x; i < 4 * kTcBM; i += blockDim.x) pub[i] = make_float2(INFINITY, INFINITY);
-    }
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
@@ -503,183 +757,258 @@ k_assign_tc(const T* __restrict__ x, const __grid_constant__ CUtensorMap map_hi,
 
     if (warp == 0) {
         if (lane == 0) {
-            for (int u = issued; u < nunits; u++) {
-                const int s = u % S;
-                const uint32_t ph = (uint32_t)(u / S) & 1u;
-                if (!mbar_wait(&empty[s], ph ^ 1u, abort_flag)) break;
-                issue(u);
-                issued = u + 1;
+            // ---- TMA producer: unit u = (item, tile, K atom) into stage u % S
+            int u = 0, tg = 0, nissued = 0;  // units issued, tiles begun, tiles whose norms were issued
+            bool ok = true;
+            for (int i = 0; i < my_items && ok; i++) {
+                const int w = item_of(i), split = w % nsplit;
+                const int nt = tiles_of(split);
+                for (int t = 0; t < nt && ok; t++, tg++) {
+                    const int col = (split + t * nsplit) * kTcBN;
+                    for (int a = 0; a < natoms; a++, u++) {
+                        const int s = u % S;
+                        if (u >= S && !mbar_wait(&empty[s], ((uint32_t)(u / S) & 1u) ^ 1u, abort_flag)) {
+                            ok = false;
+                            break;
+                        }
+                        uint8_t* stage = smem + L.b0 + s * L.stage_bytes;
+                        mbar_expect_tx(&full[s], L.stage_bytes);
+                        tma_load_2d(stage, &map_hi, &full[s], a * (FP8 ? 128 : 64), col);
+                        if (!FP8 && p.nterms > 1) tma_load_2d(stage + L.term_bytes, &map_lo, &full[s], a * 64, col);
+                        if (a == 0) {
+                            const int ns = tg % kTcNormSlots;
+                            float* dst = norms_s + ns * (L.nrm_slot_bytes / 4);
+                            mbar_expect_tx(&norms_full[ns], L.nrm_slot_bytes);
+                            bulk_load(dst, p.norms + (size_t)col, kTcBN * 4, &norms_full[ns]);
+                            if (FP8) bulk_load(dst + kTcBN, p.wf8 + (size_t)col, kTcBN * 4, &norms_full[ns]);
+                            nissued = tg + 1;
+                        }
+                    }
+                }
             }
             // After an abort, let the copies still in flight land before the CTA
             // exits; bounded like every wait.
             if (*abort_flag) {
-                const uint64_t t0 = global_ns();
-                for (int u = issued > S ? issued - S : 0; u < issued; u++) {
-                    const uint32_t ph = (uint32_t)(u / S) & 1u;
-                    while (!mbar_try(&full[u % S], ph) && global_ns() - t0 < kWaitLimitNs) {
-                    }
-                }
-                const int tl = issued > 0 ? (issued - 1) / natoms : -1;
-                for (int t = tl >= kTcNormSlots ? tl - kTcNormSlots + 1 : 0; t <= tl; t++) {
-                    const uint32_t nph = (uint32_t)(t / kTcNormSlots) & 1u;
-                    while (!mbar_try(&norms_full[t % kTcNormSlots], nph) && global_ns() - t0 < kWaitLimitNs) {
-                    }
-                }
+                for (int v = u > S ? u - S : 0; v < u; v++) mbar_drain(&full[v % S], (uint32_t)(v / S) & 1u);
+                for (int t = nissued > kTcNormSlots ? nissued - kTcNormSlots : 0; t < nissued; t++)
+                    mbar_drain(&norms_full[t % kTcNormSlots], (uint32_t)(t / kTcNormSlots) & 1u);
             }
         }
     } else if (warp == 1) {
         if (lane == 0) {
-            // ---- MMA issuer: per unit, nterms x 4 MMAs of M=128 N=256 K=16
-            const uint32_t idesc = idesc_bf16(kTcBM, kTcBN);
-            const uint64_t a_hi0 = sw128_desc(smem_u32(smem + L.a_hi));
-            const uint64_t a_lo0 = sw128_desc(smem_u32(smem + L.a_lo));
+            // ---- MMA issuer: per unit, nterms x 4 MMAs of M=128 N=256 (K=16 BF16 / K=32 e4m3)
+            const uint32_t idesc = FP8 ? idesc_e4m3(kTcBM, kTcBN) : idesc_bf16(kTcBM, kTcBN);
             const uint32_t a_atom = (kTcBM * 128) >> 4;  // descriptor units (16 B) per A atom
+            int u = 0, tg = 0;
             bool ok = true;
-            int u = 0;
-            for (int t = 0; t < my_tiles && ok; t++) {
-                const int b = t & 1;
-                const uint32_t bph = (uint32_t)(t >> 1) & 1u;
-                if (!mbar_wait(&acc_empty[b], bph ^ 1u, abort_flag)) break;
+            for (int i = 0; i < my_items && ok; i++) {
+                const int w = item_of(i), split = w % nsplit;
+                const int nt = tiles_of(split);
+                const int ab = i % NB;
+                if (!mbar_wait(&a_full[ab], (uint32_t)(i / NB) & 1u, abort_flag)) break;
                 tc_fence_after();
-                const uint32_t d_tmem = tmem_base + (uint32_t)(b * kTcBN);
-                for (int a = 0; a < natoms; a++, u++) {
-                    const int s = u % S;
-                    const uint32_t ph = (uint32_t)(u / S) & 1u;
-                    if (!mbar_wait(&full[s], ph, abort_flag)) {
+                const uint64_t a_hi0 = sw128_desc(smem_u32(smem + ab * L.a_buf));
+                const uint64_t a_lo0 = sw128_desc(smem_u32(smem + ab * L.a_buf + L.a_lo));
+                for (int t = 0; t < nt && ok; t++, tg++) {
+                    const int b = tg & 1;
+                    if (!mbar_wait(&acc_empty[b], ((uint32_t)(tg >> 1) & 1u) ^ 1u, abort_flag)) {
                         ok = false;
                         break;
                     }
                     tc_fence_after();
-                    const uint64_t bh = sw128_desc(smem_u32(smem + L.b0 + s * L.stage_bytes));
-                    const uint64_t bl = bh + (L.term_bytes >> 4);
-                    const uint64_t ah = a_hi0 + (uint64_t)(a * a_atom), al = a_lo0 + (uint64_t)(a * a_atom);
-                    uint32_t acc = a > 0 ? 1u : 0u;
+                    const uint32_t d_tmem = tmem_base + (uint32_t)(b * kTcBN);
+                    for (int a = 0; a < natoms; a++, u++) {
+                        const int s = u % S;
+                        if (!mbar_wait(&full[s], (uint32_t)(u / S) & 1u, abort_flag)) {
+                            ok = false;
+                            break;
+                        }
+                        tc_fence_after();
+                        const uint64_t bh = sw128_desc(smem_u32(smem + L.b0 + s * L.stage_bytes));
+                        const uint64_t bl = bh + (L.term_bytes >> 4);
+                        const uint64_t ah = a_hi0 + (uint64_t)(a * a_atom), al = a_lo0 + (uint64_t)(a * a_atom);
 #pragma unroll
-                    for (int kk = 0; kk < 4; kk++) {  // 16 BF16 = 32 B = 2 descriptor units per K step
-                        mma_bf16(d_tmem, ah + 2 * kk, bh + 2 * kk, idesc, acc);
-                        acc = 1;
-                    }
-                    if (p.nterms > 1) {
+                        for (int kk = 0; kk < 4; kk++) {  // 32 bytes of K per MMA = 2 descriptor units
+                            const uint32_t acc = (a > 0 || kk > 0) ? 1u : 0u;
+                            if (FP8) mma_e4m3(d_tmem, ah + 2 * kk, bh + 2 * kk, idesc, acc);
+                            else mma_bf16(d_tmem, ah + 2 * kk, bh + 2 * kk, idesc, acc);
+                        }
+                        if (!FP8 && p.nterms > 1) {
 #pragma unroll
-                        for (int kk = 0; kk < 4; kk++) mma_bf16(d_tmem, ah + 2 * kk, bl + 2 * kk, idesc, 1u);
-                    }
-                    if (p.nterms > 2) {
+                            for (int kk = 0; kk < 4; kk++) mma_bf16(d_tmem, ah + 2 * kk, bl + 2 * kk, idesc, 1u);
+                        }
+                        if (!FP8 && p.nterms > 2) {
 #pragma unroll
-                        for (int kk = 0; kk < 4; kk++) mma_bf16(d_tmem, al + 2 * kk, bh + 2 * kk, idesc, 1u);
+                            for (int kk = 0; kk < 4; kk++) mma_bf16(d_tmem, al + 2 * kk, bh + 2 * kk, idesc, 1u);
+                        }
+                        mma_commit(&empty[s]);
                     }
-                    mma_commit(&empty[s]);
+                    if (ok) mma_commit(&acc_full[b]);
                 }
-                if (ok) mma_commit(&acc_full[b]);
+                if (ok) mma_commit(&a_empty[ab]);  // the row buffer is free once these MMAs complete
             }
+            // Normally every MMA has completed by now; after an abort some may still
+            // run. Either way none may outlive the TMEM allocation or the stages it reads.
+            mma_drain(mma_done);
+        }
+    } else if (warp < kTcEpi0) {
+        // ---- row loaders: item i's row tile into buffer i % NB once the MMAs of
+        // item i - NB have completed
+        const int ltid = threadIdx.x - 64;
+        for (int i = 0; i < my_items; i++) {
+            const int w = item_of(i);
+            const int ab = i % NB;
+            if (!mbar_wait(&a_empty[ab], ((uint32_t)(i / NB) & 1u) ^ 1u, abort_flag)) break;
+            uint8_t* a = smem + ab * L.a_buf;
+            if (FP8)
+                tc_load_rows_fp8(a, rscale_s + (i % kTcRowScaleSlots) * kTcBM, x, p, (w / nsplit) * kTcBM, m, ltid);
+            else
+                tc_load_rows(a, a + L.a_lo, x, p, (w / nsplit) * kTcBM, m, ltid, kTcLoadWarps * 32);
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // visible to the tensor cores
+            mbar_arrive(&a_full[ab]);
+            // The epilogue reads slot i % 4 of the row scales at item i. The loader
+            // cannot be four items ahead of it: item i + 4 needs the MMAs of item
+            // i + 2 done, which need the epilogue to have released tiles of item i.
+            if (FP8) mbar_arrive(&rs_full[i % kTcRowScaleSlots]);
         }
     } else {
-        // ---- epilogue: warps 2..17. Thread = row (TMEM lane); warp w takes the
-        // 64-column quarter (w - 2) / 4 of every tile, as two 32-column chunks.
+        // ---- epilogue: warps 4..19. Thread = row (TMEM lane); warp w takes the
+        // 64-column quarter (w - 4) / 4 of every tile, as four 16-column halves.
         const int q = warp & 3;  // TMEM lane quarter this warp may access
-        const int cq = (warp - 2) >> 2;
+        const int cq = (warp - kTcEpi0) >> 2;
         const int r = q * 32 + lane;
-        const int row = row0 + r;
-        Top2 top;
-        top.init();
-        float theta = 0.0f;
-        if (COLLECT) theta = row < m ? p.theta[row] : __int_as_float(0x7fc00000);
-        for (int t = 0; t < my_tiles; t++) {
-            const int b = t & 1;
-            const uint32_t bph = (uint32_t)(t >> 1) & 1u;
-            if (!mbar_wait(&acc_full[b], bph, abort_flag, 20000)) break;
-            if (!mbar_wait(&norms_full[t % kTcNormSlots], (uint32_t)(t / kTcNormSlots) & 1u, abort_flag)) break;
-            tc_fence_after();
-            const int cq0 = col_first + t * col_step + cq * 64;
-            const float* nrm = norms_s + (t % kTcNormSlots) * kTcBN + cq * 64;
-            const uint32_t taddr = tmem_base + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * kTcBN + cq * 64);
-            // The published bound is read once per tile (the epilogue is issue-bound);
-            // within the tile the warp's own second key tightens it.
-            const float tile_bound = (!COLLECT && p.nterms == 1) ? tc_row_bound((const float2*)(smem + L.pub), r) : 0.0f;
-#pragma unroll
-            for (int ch = 0; ch < 2; ch++) {
-                uint32_t v[32];
-                float s[32];
-                EMB_TMEM_LD32(taddr + ch * 32, v);
-                tmem_wait_ld();
-                tc_regs_ready(v);
-                if (ch == 1) {
-                    // Both chunks of this warp are in registers: release the accumulator.
-                    tc_fence_before();
-                    __syncwarp();
-                    if (lane == 0) mbar_arrive(&acc_empty[b]);
+        float* pub = (float*)(smem + L.pub);
+        uint32_t* mg = (uint32_t*)(smem + L.merge);
+        int tg = 0;
+        bool ok = true;
+        for (int i = 0; i < my_items; i++) {
+            const int w = item_of(i), split = w % nsplit;
+            const int nt = tiles_of(split);
+            const int row = (w / nsplit) * kTcBM + r;
+            TcBest best{INFINITY, INFINITY, 0xffffffffu};
+            float theta = 0.0f;
+            if (COLLECT) theta = row < m ? p.theta[row] : __int_as_float(0x7fc00000);
+            float rs = 1.0f;
+            for (int t = 0; t < nt && ok; t++, tg++) {
+                const int b = tg & 1;
+                if (!mbar_wait(&acc_full[b], (uint32_t)(tg >> 1) & 1u, abort_flag, 20000) ||
+                    !mbar_wait(&norms_full[tg % kTcNormSlots], (uint32_t)(tg / kTcNormSlots) & 1u, abort_flag) ||
+                    (p.stall_ns && t == p.stall_tile && warp == kTcEpi0 &&
+                     !mbar_wait(stall_bar, 0, abort_flag, 0, p.stall_ns))) {
+                    ok = false;
+                    break;
                 }
-                tc_scores32(v, nrm + ch * 32, s);
-                const int cb = cq0 + ch * 32;
-                if (!COLLECT) {
-                    // Single-term search (epilogue-bound): the keyed tournament only for
-                    // chunks that can hold one of the row's final two keys, judged
-                    // against the top-2 pairs that the row's four column-quarter warps
-                    // publish in shared memory (the branch stays uniform across the
-                    // warp). The three-term search is tensor-bound and takes every chunk.
-                    float2* pub = (float2*)(smem + L.pub);
-                    if (p.nterms > 1) {
-                        float k1, k2;
-                        tc_top2_32(s, k1, k2);
-                        top2_merge_keys(top, k1, k2, cb);
-                    } else {
-                        // Judged per 16-column half: a half needs its tournament less
-                        // often than the whole chunk, and costs less than half of it.
-                        // The warp's own running s2 is an upper bound of the row's final
-                        // s2 too (its columns are a subset of the row's).
-                        const float bound = fminf(tile_bound, top.s2);
-                        bool changed = false;
+                tc_fence_after();
+                if (FP8 && t == 0) {
+                    if (!mbar_wait(&rs_full[i % kTcRowScaleSlots], (uint32_t)(i / kTcRowScaleSlots) & 1u, abort_flag)) {
+                        ok = false;
+                        break;
+                    }
+                    rs = rscale_s[(i % kTcRowScaleSlots) * kTcBM + r];
+                }
+                const float* nrm = norms_s + (tg % kTcNormSlots) * (L.nrm_slot_bytes / 4) + cq * 64;
+                const uint32_t taddr = tmem_base + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * kTcBN + cq * 64);
+                const int cb = (split + t * nsplit) * kTcBN + cq * 64;
+                // The row's best key over all four quarters so far (read once per
+                // tile; keys only decrease, so a stale value is still an upper
+                // bound), raised by 2^-17 relative to cover a key's column bits.
+                float g1 = fminf(fminf(pub[r], pub[kTcBM + r]), fminf(pub[2 * kTcBM + r], pub[3 * kTcBM + r]));
+                g1 = fmaf(fabsf(g1), 0x1p-17f, g1);
+                uint32_t va[16], vb[16];
+                EMB_TMEM_LD16(taddr, va);
+                tmem_wait_ld();
+                tc_regs_ready16(va);
 #pragma unroll
-                        for (int hh = 0; hh < 2; hh++) {
-                            if (__any_sync(__activemask(), tc_min_may_enter(tc_min16(s, hh), bound))) {
-                                float k1, k2;
-                                tc_top2_16(s, hh, k1, k2);
-                                top2_merge_keys(top, k1, k2, cb);
-                                changed = true;
+                for (int h = 0; h < 4; h++) {
+                    uint32_t(&cur)[16] = (h & 1) ? vb : va;
+                    uint32_t(&nxt)[16] = (h & 1) ? va : vb;
+                    if (h < 3) {
+                        EMB_TMEM_LD16(taddr + (h + 1) * 16, nxt);  // in flight while this half is scored
+                    } else {
+                        // All four loads of this tile are complete: release the accumulator.
+                        tc_fence_before();
+                        __syncwarp();
+                        if (lane == 0) mbar_arrive(&acc_empty[b]);
+                    }
+                    float sc[16];
+                    tc_scores16<FP8>(cur, nrm + h * 16, nrm + kTcBN + h * 16, rs, sc);
+                    const float mn = tc_min16s(sc);
+                    if (!COLLECT) {
+                        if (__any_sync(0xffffffffu, mn < fminf(g1, best.s1))) {
+                            float k1, k2;
+                            const uint32_t jb = (uint32_t)((h & 1) * 16);
+                            tc_top2_16s(sc, jb, k1, k2);
+                            const uint32_t j1 = (uint32_t)(cb + (h >> 1) * 32) + (__float_as_uint(k1) & 31u);
+                            if (k1 < best.s1) {
+                                best.s2 = min3f(best.s2, best.s1, k2);
+                                best.s1 = k1;
+                                best.i1 = j1;
+                            } else {
+                                best.s2 = fminf(best.s2, k1);
+                            }
+                        } else {
+                            best.s2 = fminf(best.s2, mn);
+                        }
+                    } else if (mn <= theta) {
+#pragma unroll
+                        for (int j = 0; j < 16; j++) {
+                            const int col = cb + h * 16 + j;
+                            if (sc[j] <= theta && col < p.k) {
+                                const uint32_t slot = atomicAdd(&p.cand_count[row], 1u);
+                                if (slot < (uint32_t)p.cand_cap) p.cand[(size_t)row * p.cand_cap + slot] = (uint32_t)col;
                             }
                         }
-                        if (changed)
-                            asm volatile("st.volatile.shared.v2.f32 [%0], {%1, %2};" ::"r"(smem_u32(pub + cq * kTcBM + r)),
-                                         "f"(top.s1), "f"(top.s2)
-                                         : "memory");
                     }
-                } else if (tc_min32(s) <= theta) {
+                    if (h < 3) {
+                        tmem_wait_ld();
+                        tc_regs_ready16(nxt);
+                    }
+                }
+                if (!COLLECT) pub[cq * kTcBM + r] = best.s1;  // the quarter's best key, for the other quarters
+            }
+            // After an abort the warp still walks every remaining item and reaches
+            // both named barriers of each (bar.sync cannot time out), without waits.
+            if (!COLLECT) {
+                // Merge the four column quarters of each row: the best key over all,
+                // and below it the smallest of everything else (the other quarters'
+                // best keys and every quarter's bound of the rest).
+                if (cq > 0) {
+                    uint32_t* e = mg + ((cq - 1) * kTcBM + r) * 4;
+                    e[0] = __float_as_uint(best.s1);
+                    e[1] = best.i1;
+                    e[2] = __float_as_uint(best.s2);
+                }
+                asm volatile("bar.sync 1, %0;" ::"n"(kTcEpiWarps * 32) : "memory");
+                if (cq == 0 && row < m) {
+                    float s1 = best.s1, s2 = best.s2;
+                    uint32_t i1 = best.i1;
 #pragma unroll
-                    for (int j = 0; j < 32; j++) {
-                        if (s[j] <= theta && cb + j < p.k) {
-                            uint32_t slot = atomicAdd(&p.cand_count[row], 1u);
-                            if (slot < (uint32_t)p.cand_cap) p.cand[(size_t)row * p.cand_cap + slot] = (uint32_t)(cb + j);
+                    for (int o = 0; o < 3; o++) {
+                        const uint32_t* e = mg + (o * kTcBM + r) * 4;
+                        const float os1 = __uint_as_float(e[0]), os2 = __uint_as_float(e[2]);
+                        const uint32_t oi1 = e[1];
+                        if (lex_less(os1, oi1, s1, i1)) {
+                            s2 = min3f(s2, s1, os2);
+                            s1 = os1;
+                            i1 = oi1;
+                        } else {
+                            s2 = min3f(s2, os1, os2);
                         }
                     }
+                    // Written as a top-2 pair whose second entry repeats the column: a
+                    // certified row always takes the first candidate, and s2 bounds
+                    // every other column's approximate score from below. s2 >= s1
+                    // holds by construction (every value folded into s2 is at least
+                    // the final best key); were it ever violated, raising s2 to s1
+                    // leaves no margin, so the row goes to the refine pass.
+                    const size_t oo = ((size_t)split * p.m + row) * 2;
+                    p.part_s[oo] = s1;
+                    p.part_i[oo] = i1;
+                    p.part_s[oo + 1] = fmaxf(s2, s1);
+                    p.part_i[oo + 1] = i1;
                 }
-            }
-        }
-        if (!COLLECT) {
-            // Merge the four column quarters of each row through shared memory.
-            uint32_t* mg = (uint32_t*)(smem + L.merge);
-            if (cq > 0) {
-                uint32_t* e = mg + ((cq - 1) * kTcBM + r) * 4;
-                e[0] = __float_as_uint(top.s1);
-                e[1] = top.i1;
-                e[2] = __float_as_uint(top.s2);
-                e[3] = top.i2;
-            }
-            asm volatile("bar.sync 1, %0;" ::"n"(kTcEpiWarps * 32) : "memory");
-            if (cq == 0 && row < m) {
-#pragma unroll
-                for (int o = 0; o < 3; o++) {
-                    const uint32_t* e = mg + (o * kTcBM + r) * 4;
-                    Top2 ot;
-                    ot.s1 = __uint_as_float(e[0]);
-                    ot.i1 = e[1];
-                    ot.s2 = __uint_as_float(e[2]);
-                    ot.i2 = e[3];
-                    top.merge(ot);
-                }
-                size_t oo = ((size_t)blockIdx.y * p.m + row) * 2;
-                p.part_s[oo] = top.s1;
-                p.part_i[oo] = top.i1;
-                p.part_s[oo + 1] = top.s2;
-                p.part_i[oo + 1] = top.i2;
+                pub[cq * kTcBM + r] = INFINITY;  // the next item starts afresh
+                asm volatile("bar.sync 1, %0;" ::"n"(kTcEpiWarps * 32) : "memory");
             }
         }
     }

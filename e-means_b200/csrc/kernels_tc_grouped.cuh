@@ -87,7 +87,8 @@ k_assign_grouped(const __grid_constant__ CUtensorMap map_hi, const __grid_consta
     uint64_t* norms_full = acc_empty + kGrpAcc;    // [kGrpNormSlots]
     uint64_t* a_full = norms_full + kGrpNormSlots; // [2] row buffer gathered
     uint64_t* a_empty = a_full + 2;                // [2] every MMA reading the row buffer completed
-    uint32_t* tmem_slot = (uint32_t*)(a_empty + 2);
+    uint64_t* mma_done = a_empty + 2;              // every issued MMA completed (teardown)
+    uint32_t* tmem_slot = (uint32_t*)(mma_done + 1);
     volatile int* abort_flag = (volatile int*)(tmem_slot + 1);
     float* norms_s = (float*)(smem + L.norms);
 
@@ -119,6 +120,7 @@ k_assign_grouped(const __grid_constant__ CUtensorMap map_hi, const __grid_consta
             mbar_init(&a_full[b], 1);
             mbar_init(&a_empty[b], 1);
         }
+        mbar_init(mma_done, 1);
         *abort_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
@@ -232,6 +234,7 @@ k_assign_grouped(const __grid_constant__ CUtensorMap map_hi, const __grid_consta
                 if (ok) mma_commit(&a_empty[ab]);  // the row buffer is free once these MMAs complete
                 cur = nxt;
             }
+            mma_drain(mma_done);  // no MMA may outlive the TMEM allocation (see k_assign_tc)
         }
     } else if (warp == kGrpRowWarp) {
         // ---- row gatherer: lane l gathers rows 4l .. 4l + 3 of every bucket tile

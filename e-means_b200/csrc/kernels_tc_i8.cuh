@@ -29,6 +29,8 @@ struct TcI8Params {
     long long* part_s;         // [split][row] exact score
     uint32_t* part_i;          // [split][row] label
     int* err;
+    int stall_tile;            // abort-path test, as TcParams::stall_tile
+    uint64_t stall_ns;
 };
 
 __host__ __device__ inline TcSmem tc_i8_smem_layout(int kpad) {
@@ -74,7 +76,9 @@ k_assign_tc_i8(const int8_t* __restrict__ x, const __grid_constant__ CUtensorMap
     uint64_t* acc_full = empty + kTcMaxStages;
     uint64_t* acc_empty = acc_full + 2;
     uint64_t* keys_full = acc_empty + 2;
-    uint32_t* tmem_slot = (uint32_t*)(keys_full + kTcNormSlots);
+    uint64_t* mma_done = keys_full + kTcNormSlots;  // every issued MMA completed (teardown)
+    uint64_t* stall_bar = mma_done + 1;             // never completed (abort-path test)
+    uint32_t* tmem_slot = (uint32_t*)(stall_bar + 1);
     volatile int* abort_flag = (volatile int*)(tmem_slot + 1);
     int* keys_s = (int*)(smem + L.norms);
 
@@ -95,6 +99,8 @@ k_assign_tc_i8(const int8_t* __restrict__ x, const __grid_constant__ CUtensorMap
             mbar_init(&acc_empty[b], kTcEpiWarps);
         }
         for (int i = 0; i < kTcNormSlots; i++) mbar_init(&keys_full[i], 1);
+        mbar_init(mma_done, 1);
+        mbar_init(stall_bar, 1);
         *abort_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
@@ -147,18 +153,10 @@ k_assign_tc_i8(const int8_t* __restrict__ x, const __grid_constant__ CUtensorMap
                 issued = u + 1;
             }
             if (*abort_flag) {
-                const uint64_t t0 = global_ns();
-                for (int u = issued > S ? issued - S : 0; u < issued; u++) {
-                    const uint32_t ph = (uint32_t)(u / S) & 1u;
-                    while (!mbar_try(&full[u % S], ph) && global_ns() - t0 < kWaitLimitNs) {
-                    }
-                }
+                for (int u = issued > S ? issued - S : 0; u < issued; u++) mbar_drain(&full[u % S], (uint32_t)(u / S) & 1u);
                 const int tl = issued > 0 ? (issued - 1) / natoms : -1;
-                for (int t = tl >= kTcNormSlots ? tl - kTcNormSlots + 1 : 0; t <= tl; t++) {
-                    const uint32_t nph = (uint32_t)(t / kTcNormSlots) & 1u;
-                    while (!mbar_try(&keys_full[t % kTcNormSlots], nph) && global_ns() - t0 < kWaitLimitNs) {
-                    }
-                }
+                for (int t = tl >= kTcNormSlots ? tl - kTcNormSlots + 1 : 0; t <= tl; t++)
+                    mbar_drain(&keys_full[t % kTcNormSlots], (uint32_t)(t / kTcNormSlots) & 1u);
             }
         }
     } else if (warp == 1) {
@@ -191,6 +189,7 @@ k_assign_tc_i8(const int8_t* __restrict__ x, const __grid_constant__ CUtensorMap
                 }
                 if (ok) mma_commit(&acc_full[b]);
             }
+            mma_drain(mma_done);  // no MMA may outlive the TMEM allocation (see k_assign_tc)
         }
     } else {
         const int q = warp & 3;
@@ -204,6 +203,7 @@ k_assign_tc_i8(const int8_t* __restrict__ x, const __grid_constant__ CUtensorMap
             const uint32_t bph = (uint32_t)(t >> 1) & 1u;
             if (!mbar_wait(&acc_full[b], bph, abort_flag, 20000)) break;
             if (!mbar_wait(&keys_full[t % kTcNormSlots], (uint32_t)(t / kTcNormSlots) & 1u, abort_flag)) break;
+            if (p.stall_ns && t == p.stall_tile && warp == 2 && !mbar_wait(stall_bar, 0, abort_flag, 0, p.stall_ns)) break;
             tc_fence_after();
             const int cq0 = (blockIdx.y + t * nsplit) * kTcBN + cq * 64;
             const int* pk = keys_s + (t % kTcNormSlots) * kTcBN + cq * 64;

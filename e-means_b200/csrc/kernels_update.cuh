@@ -112,21 +112,11 @@ EMB_DEV const uint32_t* warp_sort_segment(uint32_t* seg, uint32_t c, uint32_t* s
 // together while each dimension's adds keep the row order. MAXG = 0: one
 // dimension group at a time.
 template <typename T, int MAXG>
-__global__ void k_segment_sums(const T* __restrict__ x, const uint32_t* __restrict__ rows, int d, int k,
-                               const uint32_t* __restrict__ counts, const uint32_t* __restrict__ offsets,
-                               uint32_t* __restrict__ list, uint32_t* __restrict__ scratch, float* __restrict__ sums,
-                               const int* __restrict__ last_pass,
-                               unsigned long long* __restrict__ pass_counts, float* __restrict__ pass_sums,
-                               double* __restrict__ pass_sums64) {
-    const int l = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int lane = threadIdx.x & 31;
-    if (l >= k) return;
-    const uint32_t c = counts[l];
-    if (c == 0) return;
-    const int is_last = *last_pass;
-    // Segment l sorts in scratch[2 offsets[l] ...): next_pow2(c) <= 2c entries,
-    // disjoint from every other segment's region.
-    const uint32_t* seg = warp_sort_segment(list + offsets[l], c, scratch + 2 * (size_t)offsets[l], lane);
+EMB_DEV void segment_sums_warp(const T* __restrict__ x, const uint32_t* __restrict__ rows, int d, int l,
+                               uint32_t c, uint32_t* seg_list, uint32_t* seg_scratch, float* __restrict__ sums,
+                               int is_last, unsigned long long* __restrict__ pass_counts,
+                               float* __restrict__ pass_sums, double* __restrict__ pass_sums64, int lane) {
+    const uint32_t* seg = warp_sort_segment(seg_list, c, seg_scratch, lane);
     auto store = [&](int t, float acc, double acc64) {
         sums[(size_t)l * d + t] = acc;
         if (is_last) {
@@ -182,6 +172,34 @@ __global__ void k_segment_sums(const T* __restrict__ x, const uint32_t* __restri
     if (is_last && lane == 0) pass_counts[l] += c;
 }
 
+template <typename T, int MAXG>
+__global__ void k_segment_sums(const T* __restrict__ x, const uint32_t* __restrict__ rows, int d, int k,
+                               const uint32_t* __restrict__ counts, const uint32_t* __restrict__ offsets,
+                               uint32_t* __restrict__ list, uint32_t* __restrict__ scratch, float* __restrict__ sums,
+                               const int* __restrict__ last_pass,
+                               unsigned long long* __restrict__ pass_counts, float* __restrict__ pass_sums,
+                               double* __restrict__ pass_sums64) {
+    const int l = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (l >= k) return;
+    const uint32_t c = counts[l];
+    if (c == 0) return;
+    // Segment l sorts in scratch[2 offsets[l] ...): next_pow2(c) <= 2c entries,
+    // disjoint from every other segment's region.
+    segment_sums_warp<T, MAXG>(x, rows, d, l, c, list + offsets[l], scratch + 2 * (size_t)offsets[l], sums,
+                               *last_pass, pass_counts, pass_sums, pass_sums64, lane);
+}
+
+// The batch's rows gathered into one contiguous block (the proposer's search
+// reads contiguous rows).
+__global__ void k_gather_rows(const float* __restrict__ x, const uint32_t* __restrict__ rows, int m, int d,
+                              float* __restrict__ out) {
+    const size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= (size_t)m * d) return;
+    const size_t i = e / d, t = e - i * d;
+    out[e] = x[(size_t)rows[i] * d + t];
+}
+
 // Last pass: labels[i] = l for every row of the batch (src/lib.rs:438-440).
 __global__ void k_store_labels(const uint32_t* __restrict__ batch_labels, const uint32_t* __restrict__ rows, int m,
                                uint32_t* __restrict__ labels_all, const int* __restrict__ last_pass) {
@@ -192,13 +210,8 @@ __global__ void k_store_labels(const uint32_t* __restrict__ batch_labels, const 
 // State::apply (src/lib.rs:287-309), one warp per cluster: N *= (1 - a) for all
 // clusters; touched ones take mass = N + a n, w = a n / mass, c += w (s/n - c)
 // (c = s/n when w == 1). alpha = alphas[*step]: the host-computed cosine schedule.
-__global__ void k_apply(int k, int d, float* __restrict__ c, float* __restrict__ usage,
-                        const uint32_t* __restrict__ counts, const float* __restrict__ sums,
-                        const float* __restrict__ alphas, const int* __restrict__ step) {
-    const int j = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int lane = threadIdx.x & 31;
-    if (j >= k) return;
-    const float alpha = alphas[*step];
+EMB_DEV void apply_warp(int j, int d, float alpha, float* __restrict__ c, float* __restrict__ usage,
+                        const uint32_t* __restrict__ counts, const float* __restrict__ sums, int lane) {
     const bool replace = alpha == 1.0f;
     float u = usage[j];
     if (!replace) u = __fmul_rn(u, __fsub_rn(1.0f, alpha));
@@ -218,6 +231,15 @@ __global__ void k_apply(int k, int d, float* __restrict__ c, float* __restrict__
         u = mass;
     }
     if (lane == 0) usage[j] = u;
+}
+
+__global__ void k_apply(int k, int d, float* __restrict__ c, float* __restrict__ usage,
+                        const uint32_t* __restrict__ counts, const float* __restrict__ sums,
+                        const float* __restrict__ alphas, const int* __restrict__ step) {
+    const int j = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (j >= k) return;
+    apply_warp(j, d, alphas[*step], c, usage, counts, sums, lane);
 }
 
 // Balance penalty (src/lib.rs:411-417): when balance > 0 and the previous batch's
@@ -298,17 +320,16 @@ constexpr size_t kReviveSmemBytes = kReviveSmemSort * (sizeof(double) + sizeof(u
 //   key descending, the first min(|unused|, |donors|) split into the unused slots.
 // Scratch: keys and didx with room for next_pow2(k) entries, unused[k]; cursor and
 // n_splits updated.
-__global__ void __launch_bounds__(1024) k_revive(int k, int d, float* __restrict__ c, float* __restrict__ usage,
-                                                 float tau, const double* __restrict__ gstream,
-                                                 unsigned long long* __restrict__ cursor, double* __restrict__ keys,
-                                                 uint32_t* __restrict__ didx, uint32_t* __restrict__ unused,
-                                                 unsigned long long* __restrict__ n_splits,
-                                                 unsigned long long capacity, const int* __restrict__ step,
-                                                 int every) {
+// The body of k_revive for one CTA of 1024 threads (called by every thread of
+// the block); sort_smem: dynamic shared memory for smem_sort donors.
+EMB_DEV void revive_cta(int k, int d, float* __restrict__ c, float* __restrict__ usage, float tau,
+                        const double* __restrict__ gstream, unsigned long long* __restrict__ cursor,
+                        double* __restrict__ keys, uint32_t* __restrict__ didx, uint32_t* __restrict__ unused,
+                        unsigned long long* __restrict__ n_splits, unsigned long long capacity,
+                        double* sort_keys, uint32_t smem_sort) {
     __shared__ float thr_s;
     __shared__ uint32_t wsum_u[32], wsum_d[32];
     __shared__ uint32_t nun_s, ndon_s;
-    if ((*step + 1) % every != 0 || !(tau > 0.0f)) return;  // every 5th step (src/lib.rs:463-465)
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     if (tid == 0) {
         float total = -0.0f;
@@ -362,10 +383,9 @@ __global__ void __launch_bounds__(1024) k_revive(int k, int d, float* __restrict
     // Up to kReviveSmemSort entries the sort runs in shared memory.
     uint32_t n2 = 1;
     while (n2 < ndon) n2 <<= 1;
-    extern __shared__ double sort_keys[];
-    const bool in_smem = n2 <= kReviveSmemSort;
+    const bool in_smem = n2 <= smem_sort;
     double* sk = in_smem ? sort_keys : keys;
-    uint32_t* si = in_smem ? (uint32_t*)(sort_keys + kReviveSmemSort) : didx;
+    uint32_t* si = in_smem ? (uint32_t*)(sort_keys + smem_sort) : didx;
     for (uint32_t i = tid; i < n2; i += 1024) {
         if (i < ndon) {
             const uint32_t j = didx[i];
@@ -429,6 +449,19 @@ __global__ void __launch_bounds__(1024) k_revive(int k, int d, float* __restrict
         *cursor = cur + ndon;
         *n_splits += nsplit;
     }
+}
+
+__global__ void __launch_bounds__(1024) k_revive(int k, int d, float* __restrict__ c, float* __restrict__ usage,
+                                                 float tau, const double* __restrict__ gstream,
+                                                 unsigned long long* __restrict__ cursor, double* __restrict__ keys,
+                                                 uint32_t* __restrict__ didx, uint32_t* __restrict__ unused,
+                                                 unsigned long long* __restrict__ n_splits,
+                                                 unsigned long long capacity, const int* __restrict__ step,
+                                                 int every) {
+    extern __shared__ double sort_keys[];
+    if ((*step + 1) % every != 0 || !(tau > 0.0f)) return;  // every 5th step (src/lib.rs:463-465)
+    revive_cta(k, d, c, usage, tau, gstream, cursor, keys, didx, unused, n_splits, capacity, sort_keys,
+               kReviveSmemSort);
 }
 
 __global__ void k_step_incr(int* step) { *step += 1; }

@@ -48,6 +48,9 @@ typedef struct emb200_handle emb200_handle;
 #define EMB200_PREC_FP32 0  /* FP32 SIMT contraction */
 #define EMB200_PREC_BF16 1  /* tcgen05 BF16, three-term split (hi*hi + hi*lo + lo*hi), FP32 accumulate */
 #define EMB200_PREC_BF16X1 2 /* tcgen05 BF16 single term, FP32 accumulate (wider bound, more re-search) */
+#define EMB200_PREC_FP8 3    /* tcgen05 FP8 e4m3 operands (kind::f8f6f4), a power-of-two scale per row and per
+                                centroid, FP32 accumulate; f32 rows with d <= 256 (else as BF16X1). Its error
+                                bound (e4m3 unit roundoff 2^-4) is wide: most rows go on to the refine pass */
 
 /* Centroid representation for i8 rows (src/cpu_i8.rs:21-25). */
 #define EMB200_CENTROIDS_F32 0 /* CpuAssigner semantics: rows widened to f32 */
@@ -67,7 +70,9 @@ typedef struct {
     int match_kernel;  /* EMB200_MATCH_* (default AVX512) */
     int train_eager;   /* 1: launch the training loop's kernels one by one instead of
                           capturing each epoch as a CUDA graph and replaying it (default 0) */
-    int reserved[4];
+    int batched_streams; /* emb200_train_batched: 0 (default) runs the instances in lockstep with
+                            batched kernels where supported; 1 gives each instance its own stream */
+    int reserved[3];
 } emb200_opts;
 
 /* Config, src/lib.rs:104-124. Optional fields use sentinels:
@@ -100,7 +105,8 @@ typedef struct {
     uint64_t rows_researched; /* rows searched exhaustively with exact arithmetic */
     uint64_t kernel_launches; /* kernels launched by the call */
     double ms_total;          /* device time of the call (CUDA events) */
-    int32_t fast_kernel;      /* fast contraction used: 0 FP32 SIMT, 1 tcgen05 BF16, 2 exact int8 */
+    int32_t fast_kernel;      /* fast contraction used: 0 FP32 SIMT, 1 tcgen05 BF16, 2 exact int8 (dp4a),
+                                 3 exact int8 (tcgen05 kind::i8), 4 tcgen05 FP8 e4m3 */
     int32_t fast_aborted;     /* 1 if a bounded wait in the fast kernel gave up (rows then re-searched) */
     uint64_t rows_refined;    /* uncertified rows sent through the candidate-collecting refine pass */
     double fast_ms;           /* device time of the fast contraction kernel(s) (CUDA events, summed) */
@@ -151,6 +157,23 @@ int emb200_load_rows(emb200_handle* h, int dtype, const void* x, size_t n, size_
  * centroids. labels/dist: host arrays of n, or NULL to keep results on device. */
 int emb200_assign_resident(emb200_handle* h, uint32_t* labels, float* dist);
 
+/* Test of the bounded-wait abort path (no counterpart in the reference: its
+ * CudaAssigner has no device-side waits). With stall_tile >= 0 and stall_ns > 0,
+ * the next fast tensor-core searches on this handle (BF16 and int8 kind::i8)
+ * make their first epilogue warp wait, at that centroid tile of each CTA, on a
+ * barrier that nothing completes, bounded by stall_ns. The wait runs out, the
+ * kernel lets its copies and MMAs in flight finish, frees its TMEM and flags the
+ * abort; the call then settles every row with the exact search (the same labels
+ * and distances) and reports stats.fast_aborted = 1. stall_tile < 0 or
+ * stall_ns = 0 turns it off (the default). */
+int emb200_set_abort_test(emb200_handle* h, int stall_tile, uint64_t stall_ns);
+
+/* FP32 SIMT throughput of device `ordinal` (no counterpart in the reference): the
+ * measured denominator of the FP32 search's roofline. Runs 8 independent FMA
+ * chains per thread over 64 warps per SM, scalar fma.rn.f32 (tflops) and paired
+ * fma.rn.f32x2 (tflops_paired); best of four timed launches each, CUDA events. */
+int emb200_measure_simt_peak(int ordinal, double* tflops, double* tflops_paired);
+
 /* ---- training (src/lib.rs:201-225 and 348-491) --------------------------- */
 
 /* resolve_recipe, src/lib.rs:201-225. epoch_rows: array of max_epochs. */
@@ -170,11 +193,19 @@ int emb200_train(emb200_handle* h, const emb200_config* cfg, size_t k, float* ce
  *
  * train() (src/lib.rs:348-491) run for `count` independent instances at once,
  * each over rows [row0, row0 + n) of the resident rows (same d and dtype, same
- * config) with its own k. Instances run concurrently, each on its own stream
- * with its epochs replayed as CUDA graphs, at most max_concurrency at a time
- * (0: 16). Outputs are concatenated in instance order: centroids sum(k_i) x d,
- * labels sum(n_i) (instance-local row order), objective sum(n_epochs_i),
- * n_splits[count]. Each instance's results equal a single train() call's. */
+ * config) with its own k. By default the instances advance in lockstep, one
+ * global step at a time: each step is a chain of batched kernels over all
+ * instances (the search a persistent kernel over an (instance, row tile, column
+ * split) work queue, FP32 SIMT, with its tile shape and split policy picked by a
+ * measured sweep cached in $EMB200_AUTOTUNE_CACHE or
+ * $HOME/.cache/emb200/autotune.txt), captured once as a CUDA graph and replayed
+ * until the longest instance is done. This covers CpuAssigner semantics
+ * (centroid_bits 0), balance 0 and up to 256 instances; otherwise, or with
+ * opts.batched_streams = 1, each instance runs on its own stream with its epochs
+ * replayed as CUDA graphs, at most max_concurrency at a time (0: 16). Outputs
+ * are concatenated in instance order: centroids sum(k_i) x d, labels sum(n_i)
+ * (instance-local row order), objective sum(n_epochs_i), n_splits[count]. Each
+ * instance's results equal a single train() call's. */
 typedef struct {
     uint64_t row0;
     uint64_t n;
@@ -183,6 +214,11 @@ typedef struct {
 int emb200_train_batched(emb200_handle* h, const emb200_config* cfg, const emb200_instance* inst, size_t count,
                          size_t max_concurrency, float* centroids, uint32_t* labels, double* objective,
                          uint64_t* n_splits);
+/* The search tile the autotuner chose for the last lockstep emb200_train_batched
+ * call on this handle (no counterpart in the reference): rows x centroids per
+ * work item, and whether an item covers one centroid tile (split_all = 1) or all
+ * of them. EMB200_ESTATE before any lockstep run. */
+int emb200_batched_search_choice(const emb200_handle* h, int* rows, int* centroids, int* split_all);
 
 /* ---- learned proposer (no counterpart in the reference's code) -----------
  *
@@ -222,6 +258,22 @@ typedef struct {
 /* Groups the current centroids, builds the group-sorted copy and initialises the
  * network (input standardisation from the resident rows when present). d <= 128. */
 int emb200_proposer_init(emb200_handle* h, const emb200_proposer_config* cfg);
+/* train() (src/lib.rs:348-491) with the learned proposer in its last
+ * `late_epochs` epochs (no counterpart in the reference; at least one
+ * full-search epoch always comes first). The epochs before run as emb200_train;
+ * the labels the full search gives in the epoch just before the late ones train
+ * the network (emb200_proposer_init with *pcfg over the centroids of that moment,
+ * then emb200_proposer_train for net_steps Adam steps), and each late batch is
+ * searched through the proposer: the exact kernel scores each row against its
+ * proposed groups' centroids only, with the certification, the refine pass over
+ * all k and the full search for low-confidence rows as in
+ * emb200_assign_proposed_*. A label then differs from train()'s only where the
+ * nearest centroid lies outside the proposed groups. Resident f32 rows, d <= 128,
+ * balance 0. Outputs as emb200_train; stats count the proposed rows. The
+ * proposer stays on the handle for later emb200_assign_proposed_* calls. */
+int emb200_train_proposed(emb200_handle* h, const emb200_config* cfg, size_t k, const emb200_proposer_config* pcfg,
+                          uint32_t late_epochs, uint32_t net_steps, float* centroids, uint32_t* labels,
+                          double* objective, uint64_t* n_splits, emb200_recipe* recipe);
 /* Adam steps on mini-batches of resident rows with known labels (host array of
  * rows_n labels, e.g. train()'s output; UINT32_MAX rows are skipped): targets
  * are the labels' groups. losses: optional host array of `steps` mean losses. */
@@ -365,14 +417,16 @@ int emb200_report_families(emb200_handle* h, uint32_t* leader, uint64_t* size, d
  * those of the FP32 search: labels and distances equal to CpuAssigner's.
  *
  * Working memory is one static device array (9.5 MiB) that every GPU
- * loading the library holds until the process exits; its device address is
- * looked up on a device's first call (so make that first call before any stream
- * capture). All calls share it and find the previous call's contents (each call
- * clears what must start at zero): calls that overlap on the GPU race on it and
- * must be ordered by the caller.
+ * loading the library holds until the process exits. Its device address in the
+ * current context is looked up on every call (a host-side query that allocates
+ * nothing), so the call stays valid after the caller resets the device or
+ * switches contexts. All calls share the array and find the previous call's
+ * contents (each call clears what must start at zero): calls that overlap on
+ * the GPU race on it and must be ordered by the caller.
  *
  * Limits: m <= EMB200_NOALLOC_MAX_ROWS, k <= EMB200_NOALLOC_MAX_K; larger
- * sizes return EMB200_ELIMIT without doing anything. match_kernel: EMB200_MATCH_*. */
+ * sizes return EMB200_ELIMIT without doing anything. d must be at most
+ * 2^31 - 64 (EMB200_EINVAL beyond). match_kernel: EMB200_MATCH_*. */
 #define EMB200_NOALLOC_MAX_ROWS 65536
 #define EMB200_NOALLOC_MAX_K 262144
 int emb200_assign_f32_noalloc(const float* x_dev, size_t m, size_t d, const float* centroids_dev, size_t k,

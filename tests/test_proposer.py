@@ -244,3 +244,32 @@ def test_grouped_search_with_a_half_k_atom(emb, orc, d):
     assert np.all(dist_p >= dist_f)
     assert same.mean() > 0.9, same.mean()
     a.close()
+
+
+@pytest.mark.gpu
+def test_proposer_in_late_training_epochs(emb):
+    # train() with the learned proposer searching the last epoch's batches: the
+    # epochs before are the plain training's (bit for bit), the network is fitted
+    # on the labels of the epoch before, and the result stays close to the full
+    # search's: final MSE within 0.5 %, most last-pass labels equal. With no late
+    # epoch the call is train() itself.
+    x = emb.datasets.heavy_tailed(120_000, 48, latent=16, components=512, nu=3.0, seed=4)
+    k = 2048
+    cfg = emb.Config(nepochs=3.0)
+    a = emb.B200Assigner(0, precision="bf16")
+    a.load_rows(x)
+    full = a.train_resident(k, cfg)
+    same = a.train_resident_proposed(k, cfg, late_epochs=0, net_steps=10, groups=64, top=8)
+    assert np.array_equal(same.labels, full.labels)
+    assert np.array_equal(same.centroids.view(np.uint32), full.centroids.view(np.uint32))
+    prop = a.train_resident_proposed(k, cfg, late_epochs=1, net_steps=1500, groups=64, top=16, mass=0.999)
+    st = prop.stats
+    assert st["rows_proposed"] > 0.5 * len(x), st
+    assert np.mean(prop.labels == full.labels) > 0.9
+    a.set_centroids(full.centroids)
+    _, d_full = a.assign_resident()
+    a.set_centroids(prop.centroids)
+    _, d_prop = a.assign_resident()
+    a.close()
+    mse_full, mse_prop = d_full.astype(np.float64).mean(), d_prop.astype(np.float64).mean()
+    assert abs(mse_prop / mse_full - 1.0) < 0.005, (mse_full, mse_prop)

@@ -189,3 +189,67 @@ def test_graph_epoch_with_a_short_last_batch(emb):
     assert outs[0].recipe.batch_size == 19_200
     assert np.array_equal(outs[0].labels, outs[1].labels)
     assert same_f32(outs[0].centroids, outs[1].centroids)
+
+
+def _uneven_instances(emb, d, sizes, ks, seed, dtype=np.float32):
+    rng = np.random.default_rng(seed)
+    parts = [emb.datasets.blobs(n, d, n_blobs=max(8, k // 2), seed=seed + i) + rng.standard_normal(d).astype(np.float32) * 5
+             for i, (n, k) in enumerate(zip(sizes, ks))]
+    if dtype != np.float32:
+        info = np.iinfo(dtype)
+        parts = [np.clip(np.rint(p * 6), info.min, info.max).astype(dtype) for p in parts]
+    x = np.ascontiguousarray(np.concatenate(parts))
+    starts = np.concatenate([[0], np.cumsum(sizes)[:-1]])
+    return parts, x, [(int(s0), n, k) for s0, n, k in zip(starts, sizes, ks)]
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.int8, np.uint8])
+@pytest.mark.parametrize("closing_f64", [False, True])
+def test_lockstep_instances_equal_single_runs(emb, dtype, closing_f64):
+    # The lockstep kernels (every instance advancing one global step at a time,
+    # batched search over an (instance, row tile) queue) against each instance's
+    # own train(): labels, centroids, revival counts and objective bit for bit.
+    # Sizes give instances with a few and with many steps, a batch as large as
+    # the rows, and k from 16 to 200.
+    sizes = [2500, 14000, 900, 7000, 30000, 4100, 600]
+    ks = [16, 60, 30, 200, 120, 25, 40]
+    parts, x, inst = _uneven_instances(emb, 24, sizes, ks, 70, dtype)
+    cfg = emb.Config(nepochs=3.0, closing_f64=closing_f64)
+    a = emb.B200Assigner(0, precision="fp32")
+    a.load_rows(x)
+    outs = a.train_batched(inst, cfg)
+    a.close()
+    for i, (n, k) in enumerate(zip(sizes, ks)):
+        b = emb.B200Assigner(0, precision="fp32")
+        single = emb.train(parts[i], 24, k, cfg, assigner=b)
+        b.close()
+        assert np.array_equal(outs[i].labels, single.labels), i
+        assert same_f32(outs[i].centroids, single.centroids), i
+        assert outs[i].n_splits == single.n_splits, i
+        assert np.array_equal(outs[i].objective, single.objective), i
+
+
+def test_lockstep_graph_eager_streams_agree(emb, orc, tmp_path, monkeypatch):
+    # The captured global step replayed, the same kernels launched one by one, and
+    # the per-instance streams mode give the same bits; k = 5000 takes the
+    # revival's global-memory donor sort; the autotuner records its choice.
+    monkeypatch.setenv("EMB200_AUTOTUNE_CACHE", str(tmp_path / "tune.txt"))
+    sizes = [60000, 3000, 12000]
+    ks = [5000, 20, 300]
+    parts, x, inst = _uneven_instances(emb, 16, sizes, ks, 90)
+    cfg = emb.Config(nepochs=2.0)
+    res = []
+    for eager, streams in [(False, False), (True, False), (False, True)]:
+        a = emb.B200Assigner(0, precision="fp32", train_eager=eager, batched_streams=streams)
+        a.load_rows(x)
+        res.append(a.train_batched(inst, cfg))
+        a.close()
+    for r in res[1:]:
+        for o, q in zip(res[0], r):
+            assert np.array_equal(o.labels, q.labels) and same_f32(o.centroids, q.centroids)
+            assert o.n_splits == q.n_splits
+    assert res[0][0].n_splits > 0
+    ref = orc.train(parts[0], ks[0], orc.make_config(nepochs=2.0), emulate=not orc.has_kernel("avx512"))
+    check_same(res[0][0], ref)
+    lines = open(tmp_path / "tune.txt").read().split()
+    assert lines[0].startswith("b_search:d=16:") and 0 <= int(lines[1]) < 6

@@ -3,10 +3,13 @@
 It serves callers that cannot allocate device memory when they search (their
 GPU memory belongs to their own pool or budget, or an allocation could stall or
 fail on a latency-critical path): they pass every buffer, and the library's
-working memory is one static device array shared by all calls. This test runs
-it twice in a row through the C ABI and checks both results against the
-ordinary entry point (emb200_assign_device), bit for bit, and that sizes beyond
-its limits are refused. It lives in its own file, collected last.
+working memory is one static device array shared by all calls. These tests call
+it through the C ABI, two calls in a row each time, and check its labels and
+distances bit for bit against the ordinary entry point (emb200_assign_device)
+and against the oracle (the reference CpuAssigner restated), including a full
+65,536-row call, rows that the certification cannot settle (duplicated
+centroids, exact hits) in all three roundings, and the refusal of sizes beyond
+its limits. The file is collected last.
 """
 import ctypes
 
@@ -16,7 +19,9 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 EMB200_ELIMIT = -6
+EMB200_EINVAL = -1
 MAX_ROWS = 65536
+MATCH = {"avx512": 0, "avx2": 1, "portable": 2}
 
 
 def noalloc_fn(emb):
@@ -25,6 +30,26 @@ def noalloc_fn(emb):
     f.argtypes = [P, S, S, P, S, P, P, ctypes.c_int, P]
     f.restype = ctypes.c_int
     return f
+
+
+def run_noalloc(f, x, c, match=0):
+    """One call on device copies of x and c; returns host (labels, dist)."""
+    import torch
+
+    m, d = x.shape
+    k = c.shape[0]
+    xd = torch.from_numpy(np.ascontiguousarray(x)).cuda()
+    cd = torch.from_numpy(np.ascontiguousarray(c)).cuda()
+    lab = torch.full((m,), 0x7FFF, dtype=torch.int32, device="cuda")
+    dst = torch.full((m,), -1.0, dtype=torch.float32, device="cuda")
+    rc = f(xd.data_ptr(), m, d, cd.data_ptr(), k, lab.data_ptr(), dst.data_ptr(), match, None)
+    assert rc == 0
+    torch.cuda.synchronize()
+    return lab.cpu().numpy().view(np.uint32), dst.cpu().numpy()
+
+
+def same_f32(a, b):
+    return np.array_equal(np.asarray(a, np.float32).view(np.uint32), np.asarray(b, np.float32).view(np.uint32))
 
 
 def test_noalloc_matches_assign_device_twice(emb):
@@ -52,8 +77,42 @@ def test_noalloc_matches_assign_device_twice(emb):
     ref.close()
 
 
+def test_noalloc_matches_oracle_full_call_twice(emb, orc):
+    # A full call (m = 65536 rows, the limit) of embedding rows against centroids
+    # drawn from them, then a smaller call on other shapes: both equal the oracle.
+    f = noalloc_fn(emb)
+    x = emb.datasets.embeddings(MAX_ROWS, 128, latent=32, seed=5)
+    c = x[np.random.default_rng(5).choice(MAX_ROWS, 4096, replace=False)] * np.float32(0.97)
+    for (xs, cs) in [(x, c), (x[:5000, :72].copy(), c[:700, :72].copy())]:
+        lab, dist = run_noalloc(f, xs, cs)
+        rl, rd = orc.cpu_assign(xs, cs, emulate=not orc.has_kernel("avx512"))
+        assert np.array_equal(lab, rl) and same_f32(dist, rd)
+
+
+@pytest.mark.parametrize("match", ["avx512", "avx2", "portable"])
+def test_noalloc_uncertified_rows_match_oracle(emb, orc, match):
+    # Every centroid duplicated (so no row's top-2 has a margin: all rows go to
+    # the exhaustive re-search), exact hits at distance 0, and d = 37 (not a
+    # multiple of 16 or 8: every tail path of the three roundings). Ties go to
+    # the lowest index as in the reference's strict-< scan.
+    f = noalloc_fn(emb)
+    rng = np.random.default_rng(37)
+    base = rng.standard_normal((60, 37)).astype(np.float32)
+    c = np.concatenate([base, base, base[::-1]])
+    x = base[rng.integers(0, 60, 3000)] + rng.standard_normal((3000, 37)).astype(np.float32) * 0.01
+    x[:60] = base
+    for rows in (x, x[::-1].copy()):  # two calls in a row
+        lab, dist = run_noalloc(f, rows, c, MATCH[match])
+        rl, rd = orc.cpu_assign(rows, c, kernel=match, emulate=True)
+        assert np.array_equal(lab, rl) and same_f32(dist, rd)
+        assert np.all(lab < 60)
+
+
 def test_noalloc_refuses_sizes_beyond_its_limit(emb):
     f = noalloc_fn(emb)
     rc = f(ctypes.c_void_p(16), MAX_ROWS + 1, 8, ctypes.c_void_p(16), 4, ctypes.c_void_p(16), ctypes.c_void_p(16),
            0, None)
     assert rc == EMB200_ELIMIT
+    rc = f(ctypes.c_void_p(16), 4, (1 << 31) - 63, ctypes.c_void_p(16), 4, ctypes.c_void_p(16), ctypes.c_void_p(16),
+           0, None)
+    assert rc == EMB200_EINVAL
