@@ -423,7 +423,8 @@ __global__ void k_b_scatter(BArgs a) {
 // Per-cluster sums in row order, last-pass sums (one warp per cluster, the
 // single-instance segment_sums_warp). Grid (ceil(kmax / 8), count).
 template <typename T, int MAXG>
-__global__ void k_b_segsums(const T* __restrict__ x, BArgs a) {
+__global__ void k_b_segsums(const T* __restrict__ x, BArgs a, int R) {
+    extern __shared__ float seg_stage[];  // R > 0: (blockDim / 32) x 2 R d floats
     const int i = blockIdx.y;
     BStep st;
     if (!b_active(a, i, &st)) return;
@@ -436,7 +437,8 @@ __global__ void k_b_segsums(const T* __restrict__ x, BArgs a) {
     segment_sums_warp<T, MAXG>(x + I.row0 * (size_t)a.d, b_rows(a, I, st), a.d, l, c, a.list + I.b_off + off,
                                a.scratch + 2 * ((size_t)I.b_off + off), a.sums + I.c_off, (int)st.last,
                                a.pass_counts + I.k_off, a.pass_sums ? a.pass_sums + I.c_off : nullptr,
-                               a.pass_sums64 ? a.pass_sums64 + I.c_off : nullptr, lane);
+                               a.pass_sums64 ? a.pass_sums64 + I.c_off : nullptr, lane,
+                               R ? seg_stage + (size_t)(threadIdx.x >> 5) * 2 * R * a.d : nullptr, R);
 }
 
 // Last pass: the row's label (src/lib.rs:438-440).

@@ -111,11 +111,41 @@ EMB_DEV const uint32_t* warp_sort_segment(uint32_t* seg, uint32_t c, uint32_t* s
 // them by shuffle, so the loads of several rows and dimension groups are in flight
 // together while each dimension's adds keep the row order. MAXG = 0: one
 // dimension group at a time.
+EMB_DEV void cp_async16(void* smem, const void* gmem) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"((uint32_t)__cvta_generic_to_shared(smem)),
+                 "l"(gmem)
+                 : "memory");
+}
+EMB_DEV void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+EMB_DEV void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+// Shared memory of a 256-thread block of staged segment sums at most: 8 warps x
+// 2 chunks x R d <= 1536 floats.
+constexpr size_t kSegStageMaxBytes = (size_t)8 * 2 * 1536 * sizeof(float);
+
+// Rows per staging chunk of segment_sums_warp (two chunks per warp, at most
+// 12 KB), or 0 for the unstaged form: f32 rows with d % 4 == 0 only.
+inline int segment_stage_rows(size_t d, bool f32_rows) {
+    if (!f32_rows || d % 4 != 0 || d > 768) return 0;
+    int r = 32;
+    while (r > 2 && (size_t)r * d > 1536) r >>= 1;
+    return r;
+}
+
+// Sums of one cluster's c batch rows per dimension, in row order. With `stage`
+// (2 R d floats of this warp's shared memory; f32 rows, d % 4 == 0, 16-byte
+// aligned), the rows come in chunks of R by cp.async, the next chunk in flight
+// while this one is summed: every row of a chunk is requested at once instead of
+// a few at a time. Each dimension's adds keep the row order either way.
 template <typename T, int MAXG>
 EMB_DEV void segment_sums_warp(const T* __restrict__ x, const uint32_t* __restrict__ rows, int d, int l,
                                uint32_t c, uint32_t* seg_list, uint32_t* seg_scratch, float* __restrict__ sums,
                                int is_last, unsigned long long* __restrict__ pass_counts,
-                               float* __restrict__ pass_sums, double* __restrict__ pass_sums64, int lane) {
+                               float* __restrict__ pass_sums, double* __restrict__ pass_sums64, int lane,
+                               float* stage = nullptr, int R = 0) {
     const uint32_t* seg = warp_sort_segment(seg_list, c, seg_scratch, lane);
     auto store = [&](int t, float acc, double acc64) {
         sums[(size_t)l * d + t] = acc;
@@ -132,7 +162,47 @@ EMB_DEV void segment_sums_warp(const T* __restrict__ x, const uint32_t* __restri
             acc[g] = 0.0f;
             acc64[g] = 0.0;
         }
-        for (uint32_t j0 = 0; j0 < c; j0 += 32) {
+        const bool staged = sizeof(T) == 4 && stage && R > 0 && (d & 3) == 0 && (((uintptr_t)x & 15) == 0);
+        if (staged) {
+            const uint32_t vpr = (uint32_t)d >> 2;  // 16-byte pieces per row
+            const uint32_t nq = (c + (uint32_t)R - 1) / (uint32_t)R;
+            auto issue = [&](uint32_t q) {
+                const uint32_t j0 = q * (uint32_t)R, n = min((uint32_t)R, c - j0);
+                const uint32_t myrow = (uint32_t)lane < n ? rows[seg[j0 + lane]] : 0u;
+                float* buf = stage + (q & 1) * (size_t)R * d;
+                for (uint32_t e0 = 0; e0 < n * vpr; e0 += 32) {
+                    const uint32_t e = e0 + lane, jj = e / vpr, pc = e - jj * vpr;
+                    const uint32_t src = __shfl_sync(0xffffffffu, myrow, (int)min(jj, 31u));
+                    if (e < n * vpr) cp_async16(buf + jj * d + 4 * pc, (const float*)x + (size_t)src * d + 4 * pc);
+                }
+                cp_async_commit();
+            };
+            issue(0);
+            for (uint32_t q = 0; q < nq; q++) {
+                if (q + 1 < nq) {
+                    issue(q + 1);
+                    cp_async_wait<1>();
+                } else {
+                    cp_async_wait<0>();
+                }
+                __syncwarp();
+                const float* buf = stage + (q & 1) * (size_t)R * d;
+                const uint32_t n = min((uint32_t)R, c - q * (uint32_t)R);
+                for (uint32_t jj = 0; jj < n; jj++) {
+#pragma unroll
+                    for (int g = 0; g < MAXG; g++) {
+                        const int t = g * 32 + lane;
+                        if (t < d) {
+                            const float v = buf[jj * d + t];
+                            acc[g] = __fadd_rn(acc[g], v);
+                            if (pass_sums64) acc64[g] += (double)v;
+                        }
+                    }
+                }
+                __syncwarp();  // this buffer is refilled two chunks on
+            }
+        }
+        for (uint32_t j0 = 0; j0 < (staged ? 0u : c); j0 += 32) {
             const uint32_t n = min(32u, c - j0);
             const uint32_t myrow = (uint32_t)lane < n ? rows[seg[j0 + lane]] : 0u;
 #pragma unroll 4
@@ -178,7 +248,8 @@ __global__ void k_segment_sums(const T* __restrict__ x, const uint32_t* __restri
                                uint32_t* __restrict__ list, uint32_t* __restrict__ scratch, float* __restrict__ sums,
                                const int* __restrict__ last_pass,
                                unsigned long long* __restrict__ pass_counts, float* __restrict__ pass_sums,
-                               double* __restrict__ pass_sums64) {
+                               double* __restrict__ pass_sums64, int R) {
+    extern __shared__ float seg_stage[];  // R > 0: (blockDim / 32) x 2 R d floats
     const int l = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (l >= k) return;
@@ -186,8 +257,9 @@ __global__ void k_segment_sums(const T* __restrict__ x, const uint32_t* __restri
     if (c == 0) return;
     // Segment l sorts in scratch[2 offsets[l] ...): next_pow2(c) <= 2c entries,
     // disjoint from every other segment's region.
+    float* stage = R ? seg_stage + (size_t)(threadIdx.x >> 5) * 2 * R * d : nullptr;
     segment_sums_warp<T, MAXG>(x, rows, d, l, c, list + offsets[l], scratch + 2 * (size_t)offsets[l], sums,
-                               *last_pass, pass_counts, pass_sums, pass_sums64, lane);
+                               *last_pass, pass_counts, pass_sums, pass_sums64, lane, stage, R);
 }
 
 // The batch's rows gathered into one contiguous block (the proposer's search
