@@ -424,6 +424,21 @@ def run_c1(args):
             times.append(t1 - t0)
     t = float(np.median(times))
     rows = sum(out.recipe.epoch_rows) + len(x)
+    # The update kernels' roofline: one run with eager launches, each batch's
+    # update chain (label histogram to revival) timed by CUDA events.
+    e = emb.B200Assigner(0, precision="bf16", train_eager=True)
+    emb.train(x, 96, 1024, emb.Config(), assigner=e)
+    ust = e.stats()
+    e.close()
+    hbm = measured_peaks()
+    upd_gbs = ust["update_bytes"] / (ust["update_ms"] / 1e3) / 1e9
+    line_update = {"bound": "hbm", "achieved": upd_gbs, "peak": hbm["hbm_gbs"], "unit": "GB/s",
+                   "frac": upd_gbs / hbm["hbm_gbs"], "peak_note": f"hbm {hbm['source']}",
+                   "kernels": "k_label_hist, k_exclusive_scan, k_label_scatter, k_segment_sums, k_store_labels, "
+                              "k_batch_objective, k_apply, k_revive, k_step_incr (per batch)",
+                   "algorithmic_bytes": ust["update_bytes"], "device_ms": ust["update_ms"],
+                   "training_device_ms_eager": ust["ms_total"],
+                   "note": "latency-bound: one warp sums a cluster's rows in row order (the reference's f32 order)"}
     line = {"metric": "e-means train + exact assign, 200k x 96, k=1024, 5 epochs (rows/s)", "value": rows / t,
             "unit": "rows/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3,
             "higher_is_better": True, "dtype": "bf16x3->f32 search, f32 update",
@@ -431,6 +446,7 @@ def run_c1(args):
                        "recipe": {"batch": out.recipe.batch_size, "alpha0": out.recipe.alpha0,
                                   "steps": out.recipe.total_steps}},
             "final_mse": float(dist.astype(np.float64).mean()), "n_splits": out.n_splits,
+            "update_roofline": line_update,
             "note": "wall clock of the whole host call (upload, training, exact pass, copies)"}
     if not args.no_cpu:
         t0 = time.perf_counter()

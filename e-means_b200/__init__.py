@@ -55,7 +55,8 @@ class _Stats(ctypes.Structure):
                 ("fast_aborted", ctypes.c_int32), ("rows_refined", ctypes.c_uint64), ("fast_ms", ctypes.c_double),
                 ("fast_launches", ctypes.c_uint64), ("rows_proposed", ctypes.c_uint64),
                 ("rows_lowconf", ctypes.c_uint64), ("propose_ms", ctypes.c_double),
-                ("groups_searched", ctypes.c_uint64)]
+                ("groups_searched", ctypes.c_uint64), ("update_ms", ctypes.c_double),
+                ("update_bytes", ctypes.c_uint64)]
 
 
 class _ProposerConfig(ctypes.Structure):

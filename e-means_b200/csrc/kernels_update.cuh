@@ -403,10 +403,23 @@ EMB_DEV void revive_cta(int k, int d, float* __restrict__ c, float* __restrict__
     __shared__ uint32_t wsum_u[32], wsum_d[32];
     __shared__ uint32_t nun_s, ndon_s;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    if (tid == 0) {
+    {
+        // total = the sequential f32 sum of usage (src/lib.rs:315). The chain of k
+        // dependent adds runs in one thread; usage comes through shared memory
+        // (the sort region, free until the sort), staged by all threads in
+        // chunks, so each add waits on a shared load rather than a global one.
+        float* stage = (float*)sort_keys;
+        const int cap = (int)smem_sort * 3;  // floats in the sort region (12 B per entry)
         float total = -0.0f;
-        for (int j = 0; j < k; j++) total = __fadd_rn(total, usage[j]);
-        thr_s = __fdiv_rn(__fmul_rn(total, tau), (float)k);
+        for (int c0 = 0; c0 < k; c0 += cap) {
+            const int n = min(cap, k - c0);
+            for (int i = tid; i < n; i += blockDim.x) stage[i] = usage[c0 + i];
+            __syncthreads();
+            if (tid == 0)
+                for (int i = 0; i < n; i++) total = __fadd_rn(total, stage[i]);
+            __syncthreads();
+        }
+        if (tid == 0) thr_s = __fdiv_rn(__fmul_rn(total, tau), (float)k);
     }
     __syncthreads();
     const float thr = thr_s;

@@ -115,6 +115,10 @@ typedef struct {
     uint64_t rows_lowconf;    /* proposer assign: rows below the confidence threshold (full search) */
     double propose_ms;        /* proposer assign: device time of the proposals (network or group centroids) */
     uint64_t groups_searched; /* proposer assign: (row, group) pairs scored by the grouped search */
+    double update_ms;         /* train with opts.train_eager: device time of the per-batch update kernels
+                                 (label histogram to revival; CUDA events around each batch's chain) */
+    uint64_t update_bytes;    /* their algorithmic bytes: each batch row re-read once, per-row and
+                                 per-cluster arrays, centroids and sums read and written once */
 } emb200_stats;
 
 /* ---- lifecycle ---------------------------------------------------------- */
