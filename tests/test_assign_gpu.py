@@ -365,7 +365,7 @@ def test_bounded_wait_abort_path(emb, orc, precision, bits, stall_tile):
 @pytest.mark.parametrize("extreme", [False, True])
 def test_fp8_search_bit_exact(emb, orc, assigners, d, extreme):
     # tcgen05 kind::f8f6f4 with e4m3 operands and a power-of-two scale per row and
-    # per centroid (d <= 256; beyond it the single-term BF16 search serves). With
+    # per centroid (d <= 256; beyond it the FP32 search serves). With
     # `extreme`, a zero row, rows and centroids whose largest magnitude leaves the
     # FP8 range (tiny and huge) are in the data. Every label and distance must be
     # the oracle's, through the host and the resident paths.
@@ -381,7 +381,8 @@ def test_fp8_search_bit_exact(emb, orc, assigners, d, extreme):
     a.set_centroids(c)
     lab, dist = a.assign(x)
     st = a.stats()
-    assert st["fast_kernel"] == (4 if d <= 256 else 1) and st["fast_aborted"] == 0, st
+    # d > 256: neither FP8 operands nor the BF16 split (both need d <= 256): the FP32 search serves
+    assert st["fast_kernel"] == (4 if d <= 256 else 0) and st["fast_aborted"] == 0, st
     rl, rd = orc.cpu_assign(x, c, emulate=True)
     assert np.array_equal(lab, rl) and same_f32(dist, rd)
     a.load_rows(x)
