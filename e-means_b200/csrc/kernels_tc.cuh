@@ -613,22 +613,30 @@ EMB_DEV void mma_e4m3(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t 
 // Scores of 16 accumulator columns (in place): s = norm - 2 acc (BF16), or
 // s = norm + (acc r) w (FP8: acc r undoes the row's power-of-two scale exactly,
 // w = -2 / the centroid's scale), one rounding each.
+// Paired f32 operations (fma.rn.f32x2 / mul.rn.f32x2: two IEEE roundings), with
+// the register pairs left to the compiler.
 template <bool FP8>
 EMB_DEV void tc_scores16(uint32_t (&v)[16], const float* __restrict__ nrm, const float* __restrict__ wcol, float rs,
                          float (&s)[16]) {
+    const float2 m2 = make_float2(-2.0f, -2.0f), r2 = make_float2(rs, rs);
 #pragma unroll
     for (int j = 0; j < 16; j += 4) {
         const float4 n4 = *reinterpret_cast<const float4*>(nrm + j);
+        const float2 a01 = make_float2(__uint_as_float(v[j]), __uint_as_float(v[j + 1]));
+        const float2 a23 = make_float2(__uint_as_float(v[j + 2]), __uint_as_float(v[j + 3]));
+        float2 s01, s23;
         if (FP8) {
             const float4 w4 = *reinterpret_cast<const float4*>(wcol + j);
-            s[j] = fmaf(__uint_as_float(v[j]) * rs, w4.x, n4.x);
-            s[j + 1] = fmaf(__uint_as_float(v[j + 1]) * rs, w4.y, n4.y);
-            s[j + 2] = fmaf(__uint_as_float(v[j + 2]) * rs, w4.z, n4.z);
-            s[j + 3] = fmaf(__uint_as_float(v[j + 3]) * rs, w4.w, n4.w);
+            s01 = __ffma2_rn(__fmul2_rn(a01, r2), make_float2(w4.x, w4.y), make_float2(n4.x, n4.y));
+            s23 = __ffma2_rn(__fmul2_rn(a23, r2), make_float2(w4.z, w4.w), make_float2(n4.z, n4.w));
         } else {
-            fma2_scores(__uint_as_float(v[j]), __uint_as_float(v[j + 1]), n4.x, n4.y, s[j], s[j + 1]);
-            fma2_scores(__uint_as_float(v[j + 2]), __uint_as_float(v[j + 3]), n4.z, n4.w, s[j + 2], s[j + 3]);
+            s01 = __ffma2_rn(a01, m2, make_float2(n4.x, n4.y));
+            s23 = __ffma2_rn(a23, m2, make_float2(n4.z, n4.w));
         }
+        s[j] = s01.x;
+        s[j + 1] = s01.y;
+        s[j + 2] = s23.x;
+        s[j + 3] = s23.y;
     }
 }
 
