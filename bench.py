@@ -824,7 +824,7 @@ def run_c5(args):
         p.load_rows(x)
         t0 = time.perf_counter()
         outp = p.train_resident_proposed(k, emb.Config(nepochs=5.0), late_epochs=1,
-                                         net_steps=args.proposer_steps, groups=groups, top=32, mass=0.999)
+                                         net_steps=args.late_net_steps, groups=groups, top=32, mass=0.999)
         t_late = time.perf_counter() - t0
         stp = outp.stats
         p.set_centroids(outp.centroids)
@@ -836,6 +836,8 @@ def run_c5(args):
                 "speedup": t_train / t_late,
                 "final_mse_delta": float(dist_p.astype(np.float64).mean()) / mse_f - 1.0,
                 "last_pass_label_agreement": float(np.mean(outp.labels == out.labels)),
+                "late_epoch_device_ms": stp["late_epochs_ms"], "proposer_fit_ms": stp["late_fit_ms"],
+                "full_search_epoch_ms_estimate": t_train * 1e3 / len(out.recipe.epoch_rows),
                 "rows_proposed_in_late_epoch": int(stp["rows_proposed"]),
                 "rows_lowconf_in_late_epoch": int(stp["rows_lowconf"]),
                 "note": "wall clock of each whole train call (the proposed one includes grouping the centroids "
@@ -970,6 +972,8 @@ def main():
     ap.add_argument("--proposer-configs", default="32:0:0.999,32:0:0.9999,16:0:0.99,8:0:0",
                     help="c5: top:confidence:mass settings of the proposer assign; the first is the headline")
     ap.add_argument("--c5-rows", type=int, default=10_000_000, help="c5: rows of the workload")
+    ap.add_argument("--late-net-steps", type=int, default=3000,
+                    help="c5: Adam steps of the network fitted inside the proposed training run")
     ap.add_argument("--proposer-training", type=int, default=1,
                     help="c5: also train with the proposer in the last epoch (1) or not (0)")
     ap.add_argument("--profile-proposer", action="store_true",

@@ -56,7 +56,8 @@ class _Stats(ctypes.Structure):
                 ("fast_launches", ctypes.c_uint64), ("rows_proposed", ctypes.c_uint64),
                 ("rows_lowconf", ctypes.c_uint64), ("propose_ms", ctypes.c_double),
                 ("groups_searched", ctypes.c_uint64), ("update_ms", ctypes.c_double),
-                ("update_bytes", ctypes.c_uint64)]
+                ("update_bytes", ctypes.c_uint64), ("late_fit_ms", ctypes.c_double),
+                ("late_epochs_ms", ctypes.c_double)]
 
 
 class _ProposerConfig(ctypes.Structure):

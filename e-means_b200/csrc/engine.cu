@@ -198,6 +198,10 @@ struct emb200_handle {
 namespace {
 
 int fail(emb200_handle* h, int code, const char* fmt, ...) {
+    // The error is reported here: clear the runtime's last-error state, so that a
+    // later call's launch checks do not report this one again (a sticky error,
+    // such as an illegal address, still fails every later call by itself).
+    cudaGetLastError();
     char buf[512];
     va_list ap;
     va_start(ap, fmt);
@@ -1251,6 +1255,7 @@ extern "C" int emb200_assign_f32_noalloc(const float* x_dev, size_t m, size_t d,
     if (match_kernel < 0 || match_kernel > 2) return EMB200_EINVAL;
     if (m == 0) return EMB200_OK;
     if (!x_dev || !centroids_dev || !labels_dev || !dist_dev) return EMB200_EINVAL;
+    cudaGetLastError();  // the launch check below reports this call's launches only
     void* base = nullptr;
     int rc = noalloc_scratch(&base);
     if (rc) return rc;

@@ -119,6 +119,8 @@ typedef struct {
                                  (label histogram to revival; CUDA events around each batch's chain) */
     uint64_t update_bytes;    /* their algorithmic bytes: each batch row re-read once, per-row and
                                  per-cluster arrays, centroids and sums read and written once */
+    double late_fit_ms;       /* emb200_train_proposed: host time of building and fitting the proposer */
+    double late_epochs_ms;    /* emb200_train_proposed: device time of the epochs searched through it */
 } emb200_stats;
 
 /* ---- lifecycle ---------------------------------------------------------- */
