@@ -27,6 +27,7 @@
 #include "kernels_update.cuh"
 #include "kernels_mlp.cuh"
 #include "kernels_mlp_tc.cuh"
+#include "kernels_gemm_tc.cuh"
 #include "kernels_proposer.cuh"
 #include "kernels_quant.cuh"
 #include "kernels_report.cuh"
