@@ -10,6 +10,7 @@
 #include <cstdio>
 #include <atomic>
 #include <cstring>
+#include <map>
 #include <mutex>
 #include <thread>
 #include <string>

@@ -282,6 +282,140 @@ __global__ void __launch_bounds__(256, 1) k_b_search(const T* __restrict__ x, BA
     }
 }
 
+// The search for small d (d <= D <= 32): one thread per batch row, an item being
+// 256 rows against centroid chunks split, split + nsplit, ... of 512 centroids,
+// each chunk staged in shared memory 8192 / D centroids at a time (every thread
+// reads the same centroid: a broadcast). Score = norm - 2 x.c with the dot
+// product as an FMA chain over the dimensions; a running top-2 per row;
+// partials as k_b_search writes them.
+constexpr int kBSmallRows = 256, kBSmallCols = 512;
+
+template <typename T, int D>
+__global__ void __launch_bounds__(256) k_b_search_small(const T* __restrict__ x, BArgs a) {
+    constexpr int SUB = 8192 / D < kBSmallCols ? 8192 / D : kBSmallCols;  // 32 KB of staged centroids
+    __shared__ __align__(16) float cs[SUB * D];
+    __shared__ float ns[SUB];
+    __shared__ uint32_t item_s;
+    const int tid = threadIdx.x, d = a.d;
+    for (;;) {
+        if (tid == 0) item_s = atomicAdd(&a.ctl->qhead, 1u);
+        __syncthreads();
+        const uint32_t it = item_s;
+        __syncthreads();
+        if (it >= a.total_items) break;
+        const int i = (int)a.item_inst[it];
+        BStep st;
+        if (!b_active(a, i, &st)) continue;
+        const BInst& I = a.inst[i];
+        const uint32_t local = it - I.item_off;
+        const int rt = (int)(local / I.nsplit), split = (int)(local % I.nsplit);
+        if (rt * kBSmallRows >= (int)st.bn) continue;
+        const int row = rt * kBSmallRows + tid;
+        const bool have = row < (int)st.bn;
+        float xr[D];
+        {
+            const T* src = x + (I.row0 + b_rows(a, I, st)[have ? row : 0]) * (size_t)d;
+#pragma unroll
+            for (int t = 0; t < D; t++) xr[t] = (have && t < d) ? to_f32(src[t]) : 0.0f;
+        }
+        const int k = (int)I.k, ntiles = (k + kBSmallCols - 1) / kBSmallCols;
+        const float* ci = a.c + I.c_off;
+        const float* ni = a.norms + I.k_off;
+        Top2 top;
+        top.init();
+        for (int tile = split; tile < ntiles; tile += (int)I.nsplit)
+#pragma unroll 1
+        for (int sub = 0; sub < kBSmallCols / SUB; sub++) {
+            const int col0 = tile * kBSmallCols + sub * SUB, nc = min(SUB, k - col0);
+            if (nc <= 0) break;  // uniform across the block
+            __syncthreads();  // the previous chunk's readers are done
+            for (int e = tid; e < nc * D; e += 256) {
+                const int j = e / D, t = e - j * D;
+                cs[e] = t < d ? ci[(size_t)(col0 + j) * d + t] : 0.0f;
+            }
+            for (int j = tid; j < nc; j += 256) ns[j] = ni[col0 + j];
+            __syncthreads();
+            for (int j = 0; j < nc; j++) {
+                float dot = 0.0f;
+#pragma unroll
+                for (int t = 0; t < D; t++) dot = __fmaf_rn(xr[t], cs[j * D + t], dot);
+                top.push(__fmaf_rn(-2.0f, dot, ns[j]), (uint32_t)(col0 + j));
+            }
+        }
+        if (have) {
+            const size_t o = (I.p_off + (size_t)split * I.batch + row) * 2;
+            a.part_s[o] = top.s1;
+            a.part_i[o] = top.i1;
+            a.part_s[o + 1] = top.s2;
+            a.part_i[o + 1] = top.i2;
+        }
+    }
+}
+
+// Certification for small d: one thread per batch row, the reference's rounding
+// through the single-thread restatements (sqnorm_ref, dot_ref), the same decision
+// as k_b_certify. Grid (ceil(max batch / 256), count).
+template <typename T>
+__global__ void k_b_certify_small(const T* __restrict__ x, BArgs a) {
+    const int i = blockIdx.y;
+    BStep st;
+    if (!b_active(a, i, &st)) return;
+    const BInst& I = a.inst[i];
+    const int row = blockIdx.x * blockDim.x + threadIdx.x;
+    if (row >= (int)st.bn) return;
+    const int d = a.d, k = (int)I.k;
+    const T* xr = x + (I.row0 + b_rows(a, I, st)[row]) * (size_t)d;
+    Top2 t;
+    t.init();
+    for (uint32_t s = 0; s < I.nsplit; s++) {
+        const size_t o = (I.p_off + (size_t)s * I.batch + row) * 2;
+        t.push(a.part_s[o], a.part_i[o]);
+        t.push(a.part_s[o + 1], a.part_i[o + 1]);
+    }
+    const float xn = sqnorm_ref(xr, d);
+    const uint32_t j1 = t.i1 < (uint32_t)k ? t.i1 : 0u;
+    const uint32_t j2 = t.i2 < (uint32_t)k ? t.i2 : j1;
+    const float* ci = a.c + I.c_off;
+    const float d1 = dot_ref(a.match, xr, ci + (size_t)j1 * d, d);
+    const float d2 = j2 == j1 ? d1 : dot_ref(a.match, xr, ci + (size_t)j2 * d, d);
+    float theta = 0.0f;
+    if (!certify_decide(row, t, j1, j2, d1, d2, xn, k, a.norms + I.k_off, &a.bounds[i], a.ka, a.kb,
+                        a.blabels + I.b_off, a.bdist + I.b_off, nullptr, 0.0f, 0.0f, nullptr, &theta)) {
+        const uint32_t slot = atomicAdd(&a.ctl->redo, 1u);
+        a.redo_list[slot] = ((uint32_t)i << 24) | (uint32_t)row;
+    }
+}
+
+// Exhaustive exact search for small d: one thread per listed row, the reference's
+// strict-< scan over ascending centroids (lowest index on ties, label 0 when no
+// score beats +inf) in its rounding.
+template <typename T>
+__global__ void k_b_research_small(const T* __restrict__ x, BArgs a) {
+    const uint32_t n = a.ctl->redo;
+    const int d = a.d;
+    for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
+        const uint32_t e = a.redo_list[r];
+        const int i = (int)(e >> 24), row = (int)(e & 0xFFFFFFu);
+        BStep st;
+        b_active(a, i, &st);
+        const BInst& I = a.inst[i];
+        const T* xr = x + (I.row0 + b_rows(a, I, st)[row]) * (size_t)d;
+        const float* ci = a.c + I.c_off;
+        const float* ni = a.norms + I.k_off;
+        float best = __int_as_float(0x7f800000);
+        uint32_t lab = 0;
+        for (int j = 0; j < (int)I.k; j++) {
+            const float sc = score_ref(ni[j], dot_ref(a.match, xr, ci + (size_t)j * d, d));
+            if (sc < best) {
+                best = sc;
+                lab = (uint32_t)j;
+            }
+        }
+        a.blabels[I.b_off + row] = lab;
+        a.bdist[I.b_off + row] = fmaxf(__fadd_rn(best, sqnorm_ref(xr, d)), 0.0f);
+    }
+}
+
 // Certification of every active instance's batch rows (one warp per row, the
 // reference's rounding for the selected match kernel, as k_certify); rows the
 // bound cannot settle are listed for the exhaustive search.

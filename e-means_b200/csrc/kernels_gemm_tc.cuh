@@ -32,7 +32,7 @@ k_gemm_tc(int M, int N, int K, int kc, const __grid_constant__ CUtensorMap map_a
           const __grid_constant__ CUtensorMap map_b, void* __restrict__ C, size_t ldc, const float* __restrict__ bias,
           float* __restrict__ part, int* __restrict__ err) {
     extern __shared__ __align__(1024) uint8_t smem_raw[];
-    uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+    uint8_t* smem = smem_align1024(smem_raw);
     uint64_t* full = (uint64_t*)(smem + kGtStages * kGtStageBytes);  // [kGtStages]
     uint64_t* empty = full + kGtStages;                              // [kGtStages]
     uint64_t* acc_full = empty + kGtStages;

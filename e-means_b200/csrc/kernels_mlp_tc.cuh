@@ -123,7 +123,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
 k_mlp_tc(const __grid_constant__ CUtensorMap map_w1, const __grid_constant__ CUtensorMap map_w2,
          const __grid_constant__ CUtensorMap map_w3, const MlpTcParams p) {
     extern __shared__ __align__(1024) uint8_t smem_raw[];
-    uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+    uint8_t* smem = smem_align1024(smem_raw);
     const MlpTcSmem L = mlp_tc_smem(p.kin, p.H, TOPC);
     const int S = L.nstages;
     uint64_t* full = (uint64_t*)(smem + L.bars);  // [kMlpMaxStages]

@@ -41,6 +41,10 @@ constexpr int kTcTmemCols = 512;  // two 256-column accumulators
 // therefore refilled (for tile t+8) only after every warp is done with tile t.
 constexpr int kTcNormSlots = 8;
 constexpr int kTcSmemLimit = 227 * 1024;
+// Suspend-time hint of the control warps' barrier waits (producer, MMA issuer,
+// row loaders): a waiting thread sleeps until the phase completes (or the hint
+// runs out) instead of spinning on issue slots the epilogue warps need.
+constexpr uint32_t kTcCtlSleepNs = 2000;
 // The persistent search kernel k_assign_tc adds two row-loading warps (2, 3)
 // before its 16 epilogue warps (4..19).
 constexpr int kTcLoadWarps = 2;
@@ -84,6 +88,12 @@ struct TcParams {
 
 // ---- PTX wrappers -----------------------------------------------------------
 EMB_DEV uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// The dynamic shared memory base raised to a 1024-byte boundary (the 128-byte
+// swizzle atoms' alignment). Pointer arithmetic on the shared array, not an
+// integer round trip, so the compiler keeps the accesses in the shared window
+// (ld.shared / st.shared) instead of generic loads.
+EMB_DEV uint8_t* smem_align1024(uint8_t* raw) { return raw + ((1024u - (smem_u32(raw) & 1023u)) & 1023u); }
 
 EMB_DEV void mbar_init(uint64_t* bar, uint32_t count) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
@@ -701,7 +711,7 @@ __global__ void __launch_bounds__(kTcPThreads, 1)
 k_assign_tc(const T* __restrict__ x, const __grid_constant__ CUtensorMap map_hi,
             const __grid_constant__ CUtensorMap map_lo, const TcParams p) {
     extern __shared__ __align__(1024) uint8_t smem_raw[];
-    uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+    uint8_t* smem = smem_align1024(smem_raw);
     const TcLayout L = tc_layout(p.kpad, p.nterms, FP8);
     const int S = L.stages, NB = L.nbuf;
     uint64_t* full = (uint64_t*)(smem + L.bars);          // [kTcMaxStages]
@@ -775,7 +785,7 @@ k_assign_tc(const T* __restrict__ x, const __grid_constant__ CUtensorMap map_hi,
                     const int col = (split + t * nsplit) * kTcBN;
                     for (int a = 0; a < natoms; a++, u++) {
                         const int s = u % S;
-                        if (u >= S && !mbar_wait(&empty[s], ((uint32_t)(u / S) & 1u) ^ 1u, abort_flag)) {
+                        if (u >= S && !mbar_wait(&empty[s], ((uint32_t)(u / S) & 1u) ^ 1u, abort_flag, kTcCtlSleepNs)) {
                             ok = false;
                             break;
                         }
@@ -813,13 +823,13 @@ k_assign_tc(const T* __restrict__ x, const __grid_constant__ CUtensorMap map_hi,
                 const int w = item_of(i), split = w % nsplit;
                 const int nt = tiles_of(split);
                 const int ab = i % NB;
-                if (!mbar_wait(&a_full[ab], (uint32_t)(i / NB) & 1u, abort_flag)) break;
+                if (!mbar_wait(&a_full[ab], (uint32_t)(i / NB) & 1u, abort_flag, kTcCtlSleepNs)) break;
                 tc_fence_after();
                 const uint64_t a_hi0 = sw128_desc(smem_u32(smem + ab * L.a_buf));
                 const uint64_t a_lo0 = sw128_desc(smem_u32(smem + ab * L.a_buf + L.a_lo));
                 for (int t = 0; t < nt && ok; t++, tg++) {
                     const int b = tg & 1;
-                    if (!mbar_wait(&acc_empty[b], ((uint32_t)(tg >> 1) & 1u) ^ 1u, abort_flag)) {
+                    if (!mbar_wait(&acc_empty[b], ((uint32_t)(tg >> 1) & 1u) ^ 1u, abort_flag, kTcCtlSleepNs)) {
                         ok = false;
                         break;
                     }
@@ -827,7 +837,7 @@ k_assign_tc(const T* __restrict__ x, const __grid_constant__ CUtensorMap map_hi,
                     const uint32_t d_tmem = tmem_base + (uint32_t)(b * kTcBN);
                     for (int a = 0; a < natoms; a++, u++) {
                         const int s = u % S;
-                        if (!mbar_wait(&full[s], (uint32_t)(u / S) & 1u, abort_flag)) {
+                        if (!mbar_wait(&full[s], (uint32_t)(u / S) & 1u, abort_flag, kTcCtlSleepNs)) {
                             ok = false;
                             break;
                         }
@@ -866,7 +876,7 @@ k_assign_tc(const T* __restrict__ x, const __grid_constant__ CUtensorMap map_hi,
         for (int i = 0; i < my_items; i++) {
             const int w = item_of(i);
             const int ab = i % NB;
-            if (!mbar_wait(&a_empty[ab], ((uint32_t)(i / NB) & 1u) ^ 1u, abort_flag)) break;
+            if (!mbar_wait(&a_empty[ab], ((uint32_t)(i / NB) & 1u) ^ 1u, abort_flag, kTcCtlSleepNs)) break;
             uint8_t* a = smem + ab * L.a_buf;
             if (FP8)
                 tc_load_rows_fp8(a, rscale_s + (i % kTcRowScaleSlots) * kTcBM, x, p, (w / nsplit) * kTcBM, m, ltid);

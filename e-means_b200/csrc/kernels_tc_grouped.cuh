@@ -77,7 +77,7 @@ k_assign_grouped(const __grid_constant__ CUtensorMap map_hi, const __grid_consta
                  const __grid_constant__ CUtensorMap map_rows_hi, const __grid_constant__ CUtensorMap map_rows_lo,
                  const TcParams p) {
     extern __shared__ __align__(1024) uint8_t smem_raw[];
-    uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+    uint8_t* smem = smem_align1024(smem_raw);
     const GrpSmem L = grp_smem_layout(p.kpad, p.nterms);
     const int S = L.stages;
     uint64_t* full = (uint64_t*)(smem + L.bars);   // [kGrpMaxStages]

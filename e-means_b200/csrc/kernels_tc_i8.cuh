@@ -68,7 +68,7 @@ EMB_DEV void mma_s8(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t id
 __global__ void __launch_bounds__(kTcThreads, 1)
 k_assign_tc_i8(const int8_t* __restrict__ x, const __grid_constant__ CUtensorMap map_c8, const TcI8Params p) {
     extern __shared__ __align__(1024) uint8_t smem_raw[];
-    uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+    uint8_t* smem = smem_align1024(smem_raw);
     const TcSmem L = tc_i8_smem_layout(p.kpad);
     const int S = L.stages;
     uint64_t* full = (uint64_t*)(smem + L.bars);

@@ -60,11 +60,61 @@ __global__ void k_label_scatter(const uint32_t* __restrict__ labels, const uint3
     if (i < m) list[offsets[labels[i]] + slot[i]] = (uint32_t)i;
 }
 
-// Ascending sort of one segment of c batch positions by one warp. Up to 32
+// Bitonic sort of E * 32 entries held E per lane (entry lane + 32 h in v[h]),
+// ascending; distances below 32 exchange through shuffles, longer ones within
+// the lane.
+template <int E>
+EMB_DEV void warp_bitonic_regs(uint32_t (&v)[E], int lane) {
+#pragma unroll
+    for (int k2 = 2; k2 <= 32 * E; k2 <<= 1) {
+#pragma unroll
+        for (int j = k2 >> 1; j > 0; j >>= 1) {
+            if (j < 32) {
+#pragma unroll
+                for (int h = 0; h < E; h++) {
+                    const uint32_t e = (uint32_t)(lane + 32 * h);
+                    const uint32_t o = __shfl_xor_sync(0xffffffffu, v[h], j);
+                    const bool up = (e & (uint32_t)k2) == 0, lower = (e & (uint32_t)j) == 0;
+                    v[h] = (lower == up) ? min(v[h], o) : max(v[h], o);
+                }
+            } else {
+#pragma unroll
+                for (int h = 0; h < E; h++) {
+                    const int h2 = h ^ (j >> 5);
+                    if (h2 > h) {
+                        const uint32_t e = (uint32_t)(lane + 32 * h);
+                        const bool up = (e & (uint32_t)k2) == 0;
+                        const uint32_t mn = min(v[h], v[h2]), mx = max(v[h], v[h2]);
+                        v[h] = up ? mn : mx;
+                        v[h2] = up ? mx : mn;
+                    }
+                }
+            }
+        }
+    }
+}
+
+template <int E>
+EMB_DEV const uint32_t* warp_sort_regs(uint32_t* seg, uint32_t c, int lane) {
+    uint32_t v[E];
+#pragma unroll
+    for (int h = 0; h < E; h++) v[h] = (uint32_t)(lane + 32 * h) < c ? seg[lane + 32 * h] : 0xffffffffu;
+    warp_bitonic_regs<E>(v, lane);
+#pragma unroll
+    for (int h = 0; h < E; h++)
+        if ((uint32_t)(lane + 32 * h) < c) seg[lane + 32 * h] = v[h];
+    __syncwarp();
+    return seg;
+}
+
+// Ascending sort of one segment of c batch positions by one warp. Up to 128
 // entries are sorted in registers; longer segments are copied to `scratch`
 // (room for next_pow2(c) <= 2c entries), padded with UINT32_MAX and sorted there
 // by a bitonic network. Returns the sorted segment (seg or scratch).
 EMB_DEV const uint32_t* warp_sort_segment(uint32_t* seg, uint32_t c, uint32_t* scratch, int lane) {
+    // Up to 128 entries the network runs in registers (two or four per lane).
+    if (c > 32 && c <= 64) return warp_sort_regs<2>(seg, c, lane);
+    if (c > 64 && c <= 128) return warp_sort_regs<4>(seg, c, lane);
     if (c <= 32) {
         uint32_t v = (uint32_t)lane < c ? seg[lane] : 0xffffffffu;
         for (int k2 = 2; k2 <= 32; k2 <<= 1) {
