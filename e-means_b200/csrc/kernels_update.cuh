@@ -312,6 +312,90 @@ __global__ void k_segment_sums(const T* __restrict__ x, const uint32_t* __restri
                                *last_pass, pass_counts, pass_sums, pass_sums64, lane, stage, R);
 }
 
+// Per-cluster sums with the dimensions split over warps (f32 rows, d % 4 == 0,
+// 16-byte aligned rows, d <= kDgMaxD): block l sums cluster l, warp g dimensions
+// [32 g, 32 g + 32). Warp 0 puts the cluster's batch positions in row order
+// (as segment_sums_warp) and the block shares the sorted list; each warp then
+// streams its 128-byte slice of every row through a ring of kDgStages chunks of
+// kDgRows rows (cp.async, kDgStages - 1 chunks in flight) and adds them in row
+// order, lane t one dimension. A crowded cluster's rows are read by d / 32 warps
+// with up to 14 KB in flight each, where the one-warp form has 12 KB for all d.
+constexpr int kDgRows = 16, kDgStages = 8;
+constexpr size_t kDgWarpBytes = (size_t)kDgStages * kDgRows * 32 * sizeof(float);
+constexpr int kDgMaxD = 384;  // 12 warps x 16 KB of ring
+
+__global__ void __launch_bounds__(1024) k_segment_sums_dg(const float* __restrict__ x,
+                                                         const uint32_t* __restrict__ rows, int d,
+                                                         const uint32_t* __restrict__ counts,
+                                                         const uint32_t* __restrict__ offsets,
+                                                         uint32_t* __restrict__ list, uint32_t* __restrict__ scratch,
+                                                         float* __restrict__ sums, const int* __restrict__ last_pass,
+                                                         unsigned long long* __restrict__ pass_counts,
+                                                         float* __restrict__ pass_sums,
+                                                         double* __restrict__ pass_sums64) {
+    extern __shared__ float dg_stage[];  // (blockDim / 32) x kDgStages x kDgRows x 32 floats
+    __shared__ int use_scratch;
+    const int l = blockIdx.x, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t c = counts[l];
+    if (c == 0) return;  // uniform over the block
+    uint32_t* seg_list = list + offsets[l];
+    uint32_t* seg_scratch = scratch + 2 * (size_t)offsets[l];
+    if (warp == 0) {
+        const uint32_t* sorted = warp_sort_segment(seg_list, c, seg_scratch, lane);
+        if (lane == 0) use_scratch = sorted != seg_list;
+    }
+    __syncthreads();
+    const uint32_t* seg = use_scratch ? seg_scratch : seg_list;
+    const int t0 = warp * 32;
+    const int nd = min(32, d - t0);  // dimensions of this warp (a multiple of 4)
+    const int ppr = nd >> 2;         // 16-byte pieces per row
+    float* ring = dg_stage + (size_t)warp * kDgStages * kDgRows * 32;
+    const uint32_t nq = (c + kDgRows - 1) / kDgRows;
+    auto issue = [&](uint32_t q) {
+        if (q < nq) {
+            const uint32_t j0 = q * kDgRows, n = min((uint32_t)kDgRows, c - j0);
+            const uint32_t myrow = (uint32_t)lane < n ? rows[seg[j0 + lane]] : 0u;
+            float* buf = ring + (size_t)(q % kDgStages) * kDgRows * 32;
+            for (uint32_t e0 = 0; e0 < n * (uint32_t)ppr; e0 += 32) {
+                const uint32_t e = e0 + lane, jj = e / (uint32_t)ppr, pc = e - jj * (uint32_t)ppr;
+                const uint32_t src = __shfl_sync(0xffffffffu, myrow, (int)min(jj, 31u));
+                if (e < n * (uint32_t)ppr) cp_async16(buf + jj * 32 + 4 * pc, x + (size_t)src * d + t0 + 4 * pc);
+            }
+        }
+        cp_async_commit();  // an empty group past the end keeps the group count uniform
+    };
+#pragma unroll
+    for (int q = 0; q < kDgStages - 1; q++) issue((uint32_t)q);
+    float acc = 0.0f;
+    double acc64 = 0.0;
+    const bool mine = lane < nd;
+    for (uint32_t q = 0; q < nq; q++) {
+        cp_async_wait<kDgStages - 2>();  // chunk q has landed
+        __syncwarp();
+        const float* buf = ring + (size_t)(q % kDgStages) * kDgRows * 32;
+        const uint32_t n = min((uint32_t)kDgRows, c - q * kDgRows);
+        if (mine) {
+            for (uint32_t jj = 0; jj < n; jj++) {
+                const float v = buf[jj * 32 + lane];
+                acc = __fadd_rn(acc, v);
+                if (pass_sums64) acc64 += (double)v;
+            }
+        }
+        __syncwarp();  // this buffer is refilled below, kDgStages - 1 chunks on
+        issue(q + kDgStages - 1);
+    }
+    cp_async_wait<0>();
+    if (mine) {
+        const int t = t0 + lane;
+        sums[(size_t)l * d + t] = acc;
+        if (*last_pass) {
+            if (pass_sums64) pass_sums64[(size_t)l * d + t] += acc64;
+            else pass_sums[(size_t)l * d + t] = __fadd_rn(pass_sums[(size_t)l * d + t], acc);
+        }
+    }
+    if (*last_pass && threadIdx.x == 0) pass_counts[l] += c;
+}
+
 // The batch's rows gathered into one contiguous block (the proposer's search
 // reads contiguous rows).
 __global__ void k_gather_rows(const float* __restrict__ x, const uint32_t* __restrict__ rows, int m, int d,

@@ -60,6 +60,19 @@ def test_blob_mixture_bit_exact(emb, orc, precision):
     assert st["fast_aborted"] == 0
 
 
+@pytest.mark.parametrize("d", [100, 36])
+def test_crowded_clusters_bit_exact(emb, orc, d):
+    # Most rows in one tight blob: a batch puts hundreds of rows in a few clusters
+    # (row lists past 128 entries sorted in scratch, many chunks per warp through
+    # the staging ring), with d not a multiple of 32 (a partly filled last warp).
+    rng = np.random.default_rng(d)
+    big = rng.standard_normal((15_000, d)).astype(np.float32) * np.float32(0.05)
+    rest = emb.datasets.blobs(5_000, d, n_blobs=40, seed=d)
+    x = np.concatenate([big, rest])[rng.permutation(20_000)]
+    out, ref, _ = run_both(emb, orc, x, 24, "fp32", nepochs=2.0, batch_size=8192)
+    check_same(out, ref)
+
+
 def test_embeddings_bit_exact(emb, orc):
     x = emb.datasets.embeddings(40_000, 128, seed=5)
     out, ref, _ = run_both(emb, orc, x, 512, "bf16", nepochs=2.0)
