@@ -107,14 +107,16 @@ EMB_DEV const uint32_t* warp_sort_regs(uint32_t* seg, uint32_t c, int lane) {
     return seg;
 }
 
-// Ascending sort of one segment of c batch positions by one warp. Up to 128
+// Ascending sort of one segment of c batch positions by one warp. Up to 512
 // entries are sorted in registers; longer segments are copied to `scratch`
 // (room for next_pow2(c) <= 2c entries), padded with UINT32_MAX and sorted there
 // by a bitonic network. Returns the sorted segment (seg or scratch).
 EMB_DEV const uint32_t* warp_sort_segment(uint32_t* seg, uint32_t c, uint32_t* scratch, int lane) {
-    // Up to 128 entries the network runs in registers (two or four per lane).
+    // Up to 512 entries the network runs in registers (2 to 16 per lane).
     if (c > 32 && c <= 64) return warp_sort_regs<2>(seg, c, lane);
     if (c > 64 && c <= 128) return warp_sort_regs<4>(seg, c, lane);
+    if (c > 128 && c <= 256) return warp_sort_regs<8>(seg, c, lane);
+    if (c > 256 && c <= 512) return warp_sort_regs<16>(seg, c, lane);
     if (c <= 32) {
         uint32_t v = (uint32_t)lane < c ? seg[lane] : 0xffffffffu;
         for (int k2 = 2; k2 <= 32; k2 <<= 1) {
@@ -324,7 +326,7 @@ constexpr int kDgRows = 16, kDgStages = 8;
 constexpr size_t kDgWarpBytes = (size_t)kDgStages * kDgRows * 32 * sizeof(float);
 constexpr int kDgMaxD = 384;  // 12 warps x 16 KB of ring
 
-__global__ void __launch_bounds__(1024) k_segment_sums_dg(const float* __restrict__ x,
+__global__ void __launch_bounds__(384) k_segment_sums_dg(const float* __restrict__ x,
                                                          const uint32_t* __restrict__ rows, int d,
                                                          const uint32_t* __restrict__ counts,
                                                          const uint32_t* __restrict__ offsets,
