@@ -15,22 +15,33 @@ namespace emb {
 // BF16 store of relu(acc + bias[n]); FP32 store of (acc + bias[n]); BF16 store of acc.
 enum { kEpiF32 = 0, kEpiBiasBf16 = 1, kEpiBiasReluBf16 = 2, kEpiBiasF32 = 3, kEpiBf16 = 4 };
 
-// Standardised BF16 network input: (x - mean) * inv_std per dimension.
+// Standardised BF16 network input: (x - mean) * inv_std per dimension, rows of
+// stride ld >= d.
 template <typename T>
 __global__ void k_mlp_input(const T* __restrict__ x, const uint32_t* __restrict__ rows, int m, int d,
                             const float* __restrict__ mean, const float* __restrict__ inv_std,
-                            __nv_bfloat16* __restrict__ out) {
+                            __nv_bfloat16* __restrict__ out, size_t ld) {
     const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= (size_t)m * d) return;
     const size_t r = i / d, t = i - r * d;
     const size_t src = rows ? rows[r] : r;
-    out[i] = __float2bfloat16_rn((to_f32(x[src * d + t]) - mean[t]) * inv_std[t]);
+    out[r * ld + t] = __float2bfloat16_rn((to_f32(x[src * d + t]) - mean[t]) * inv_std[t]);
+}
+
+// BF16 rows of C elements copied to row stride ld (the tail left as it is: the
+// GEMM's tensor map reads zeros past C).
+__global__ void k_pad_rows_bf16(const __nv_bfloat16* __restrict__ src, int R, int C, __nv_bfloat16* __restrict__ dst,
+                                size_t ld) {
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (size_t)R * C) return;
+    const size_t r = i / C, c = i - r * C;
+    dst[r * ld + c] = src[i];
 }
 
 // Softmax cross-entropy over G logits per row (one warp per row): writes the
 // gradient (softmax - onehot) / scale as BF16 and accumulates the loss.
 __global__ void k_softmax_xent(const float* __restrict__ logits, const uint32_t* __restrict__ target, int m, int G,
-                               float scale, __nv_bfloat16* __restrict__ grad, float* __restrict__ loss) {
+                               float scale, __nv_bfloat16* __restrict__ grad, size_t ldg, float* __restrict__ loss) {
     const int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
     if (row >= m) return;
     const float* l = logits + (size_t)row * G;
@@ -44,7 +55,7 @@ __global__ void k_softmax_xent(const float* __restrict__ logits, const uint32_t*
     const float inv = 1.0f / se;
     for (int g = lane; g < G; g += 32) {
         const float p = __expf(l[g] - mx) * inv;
-        grad[(size_t)row * G + g] = __float2bfloat16_rn((p - (g == (int)t ? 1.0f : 0.0f)) / scale);
+        grad[(size_t)row * ldg + g] = __float2bfloat16_rn((p - (g == (int)t ? 1.0f : 0.0f)) / scale);
     }
     if (lane == 0 && loss) atomicAdd(loss, (logf(se) + mx - l[t]) / scale);
 }
@@ -55,12 +66,13 @@ __global__ void k_relu_grad(__nv_bfloat16* __restrict__ g, const __nv_bfloat16* 
     if (i < n && !(__bfloat162float(h[i]) > 0.0f)) g[i] = __float2bfloat16(0.0f);
 }
 
-// Bias gradient: column sums of a BF16 m x n matrix into FP32 (one thread per column).
-__global__ void k_colsum(const __nv_bfloat16* __restrict__ g, int m, int n, float* __restrict__ out) {
+// Bias gradient: column sums of a BF16 m x n matrix (row stride ld) into FP32
+// (one thread per column).
+__global__ void k_colsum(const __nv_bfloat16* __restrict__ g, int m, int n, size_t ld, float* __restrict__ out) {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= n) return;
     float s = 0.0f;
-    for (int r = 0; r < m; r++) s += __bfloat162float(g[(size_t)r * n + c]);
+    for (int r = 0; r < m; r++) s += __bfloat162float(g[(size_t)r * ld + c]);
     out[c] = s;
 }
 
