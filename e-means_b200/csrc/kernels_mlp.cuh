@@ -82,12 +82,16 @@ __global__ void k_f32_to_bf16(const float* __restrict__ w, __nv_bfloat16* __rest
     if (i < n) wb[i] = __float2bfloat16_rn(w[i]);
 }
 
-// Adam on FP32 master weights, refreshing their BF16 copy.
+// Adam on FP32 master weights, refreshing their BF16 copy. The step's learning
+// rate and bias corrections come from sched[3 s .. 3 s + 2], s = *step (the
+// training loop's device step counter, so that one captured step replays).
 __global__ void k_adam(float* __restrict__ w, __nv_bfloat16* __restrict__ wb, const float* __restrict__ g,
-                       float* __restrict__ m1, float* __restrict__ m2, size_t n, float lr, float b1, float b2,
-                       float eps, float c1, float c2) {
+                       float* __restrict__ m1, float* __restrict__ m2, size_t n, const float* __restrict__ sched,
+                       const uint32_t* __restrict__ step, float b1, float b2, float eps) {
     const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
+    const float* sc = sched + 3 * (size_t)*step;
+    const float lr = sc[0], c1 = sc[1], c2 = sc[2];
     const float gi = g[i];
     const float a = b1 * m1[i] + (1.0f - b1) * gi;
     const float b = b2 * m2[i] + (1.0f - b2) * gi * gi;
@@ -96,6 +100,26 @@ __global__ void k_adam(float* __restrict__ w, __nv_bfloat16* __restrict__ wb, co
     const float v = w[i] - lr * (a / c1) / (sqrtf(b / c2) + eps);
     w[i] = v;
     if (wb) wb[i] = __float2bfloat16_rn(v);
+}
+
+// One training step's rows and group targets: rows brows[(step % per_upload) B ..)
+// of the uploaded block into cur_rows, their label's group into tgt.
+__global__ void k_step_rows(const uint32_t* __restrict__ brows, const uint32_t* __restrict__ step, uint32_t per_upload,
+                            int B, const uint32_t* __restrict__ labels, const uint32_t* __restrict__ group_of,
+                            uint32_t* __restrict__ cur_rows, uint32_t* __restrict__ tgt) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= B) return;
+    const uint32_t r = brows[(size_t)(*step % per_upload) * B + i];
+    cur_rows[i] = r;
+    tgt[i] = group_of[labels[r]];
+}
+
+// End of a training step: its loss into losses[step], the accumulator cleared,
+// the step counter advanced (one thread).
+__global__ void k_step_end(uint32_t* __restrict__ step, float* __restrict__ loss_acc, float* __restrict__ losses) {
+    losses[*step] = *loss_acc;
+    *loss_acc = 0.0f;
+    *step += 1;
 }
 
 // Top-m groups per row from G logits (one warp per row), the softmax mass those
