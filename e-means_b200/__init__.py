@@ -125,6 +125,7 @@ def lib():
     L.emb200_assign_resident.argtypes = [P, P, P]
     L.emb200_set_abort_test.argtypes = [P, I, ctypes.c_uint64]
     L.emb200_measure_simt_peak.argtypes = [I, P, P]
+    L.emb200_measure_mma_peak.argtypes = [I, P, P]
     L.emb200_batched_search_choice.argtypes = [P, P, P, P]
     L.emb200_train_proposed.argtypes = [P, ctypes.POINTER(_Config), S, ctypes.POINTER(_ProposerConfig), ctypes.c_uint32,
                                         ctypes.c_uint32, P, P, P, P, ctypes.POINTER(_Recipe)]
@@ -240,6 +241,16 @@ def measure_simt_peak(ordinal=0):
     rc = lib().emb200_measure_simt_peak(ordinal, ctypes.byref(a), ctypes.byref(b))
     if rc != 0:
         raise EngineError(f"emb200_measure_simt_peak failed ({rc})")
+    return a.value, b.value
+
+
+def measure_mma_peak(ordinal=0):
+    """(cta_group::1 M=128 N=256, cta_group::2 M=256 N=256) tcgen05 BF16 TF/s of
+    this device, operands resident in shared memory."""
+    a, b = ctypes.c_double(), ctypes.c_double()
+    rc = lib().emb200_measure_mma_peak(ordinal, ctypes.byref(a), ctypes.byref(b))
+    if rc != 0:
+        raise EngineError(f"emb200_measure_mma_peak failed ({rc})")
     return a.value, b.value
 
 

@@ -33,6 +33,7 @@
 #include "kernels_quant.cuh"
 #include "kernels_report.cuh"
 #include "kernels_peak.cuh"
+#include "kernels_peak_tc.cuh"
 #include "kernels_batched.cuh"
 
 constexpr int kRefineCap = 32;  // candidates kept per refined row
@@ -1188,6 +1189,69 @@ int emb200_measure_simt_peak(int ordinal, double* tflops, double* tflops_paired)
     if (e0) cudaEventDestroy(e0);
     if (e1) cudaEventDestroy(e1);
     cudaFree(out);
+    return rc;
+}
+
+int emb200_measure_mma_peak(int ordinal, double* tflops_1sm, double* tflops_2sm) {
+    if (!tflops_1sm || !tflops_2sm) return EMB200_EINVAL;
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || ordinal < 0 || ordinal >= n) return EMB200_EDEVICE;
+    if (cudaSetDevice(ordinal) != cudaSuccess) return EMB200_ECUDA;
+    int sms = 0;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ordinal) != cudaSuccess) return EMB200_ECUDA;
+    const int iters = 1 << 16;
+    int* err = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    int rc = EMB200_OK;
+    if (cudaMalloc(&err, sizeof(int)) != cudaSuccess) return EMB200_ENOMEM;
+    cudaMemset(err, 0, sizeof(int));
+    if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) rc = EMB200_ECUDA;
+    if (cudaFuncSetAttribute(k_mma_peak<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPeakSmem) !=
+            cudaSuccess ||
+        cudaFuncSetAttribute(k_mma_peak<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPeakSmem) !=
+            cudaSuccess)
+        rc = EMB200_ECUDA;
+    for (int pair = 0; pair < 2 && rc == EMB200_OK; pair++) {
+        // 2 x 128 x 256 x 16 flops per CTA and MMA step either way (a pair's
+        // M = 256 instruction covers two SMs)
+        const int ctas = pair ? sms / 2 * 2 : sms;
+        const double flops = 2.0 * 128 * 256 * 16 * 4.0 * iters * ctas;
+        float best = 1e30f;
+        for (int rep = 0; rep < 5 && rc == EMB200_OK; rep++) {
+            cudaEventRecord(e0);
+            if (pair) {
+                cudaLaunchConfig_t lc = {};
+                lc.gridDim = dim3((unsigned)ctas);
+                lc.blockDim = dim3(128);
+                lc.dynamicSmemBytes = kPeakSmem;
+                cudaLaunchAttribute at[1];
+                at[0].id = cudaLaunchAttributeClusterDimension;
+                at[0].val.clusterDim.x = 2;
+                at[0].val.clusterDim.y = 1;
+                at[0].val.clusterDim.z = 1;
+                lc.attrs = at;
+                lc.numAttrs = 1;
+                if (cudaLaunchKernelEx(&lc, k_mma_peak<true>, iters, err) != cudaSuccess) rc = EMB200_ECUDA;
+            } else {
+                k_mma_peak<false><<<ctas, 128, kPeakSmem>>>(iters, err);
+            }
+            cudaEventRecord(e1);
+            if (cudaEventSynchronize(e1) != cudaSuccess) {
+                rc = EMB200_ECUDA;
+                break;
+            }
+            float ms = 0.0f;
+            cudaEventElapsedTime(&ms, e0, e1);
+            if (rep >= 1) best = std::min(best, ms);
+        }
+        (pair ? *tflops_2sm : *tflops_1sm) = flops / (best * 1e-3) / 1e12;
+    }
+    int e = 0;
+    if (rc == EMB200_OK && (cudaMemcpy(&e, err, sizeof e, cudaMemcpyDeviceToHost) != cudaSuccess || e)) rc = EMB200_ECUDA;
+    if (cudaGetLastError() != cudaSuccess) rc = EMB200_ECUDA;
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    cudaFree(err);
     return rc;
 }
 

@@ -51,7 +51,7 @@ struct BCtl {
     int gstep;       // global step
     uint32_t qhead;  // search work queue head
     uint32_t redo;   // rows listed for the exhaustive search
-    uint32_t pad;
+    uint32_t redo_total;  // summed over the steps of the call
 };
 
 struct BArgs {
@@ -636,6 +636,7 @@ __global__ void k_b_step_end(BArgs a) {
     if (threadIdx.x == 0) {
         a.ctl->gstep += 1;
         a.ctl->qhead = 0;
+        a.ctl->redo_total += a.ctl->redo;
         a.ctl->redo = 0;
     }
 }

@@ -108,7 +108,8 @@ typedef struct {
     int32_t fast_kernel;      /* fast contraction used: 0 FP32 SIMT, 1 tcgen05 BF16, 2 exact int8 (dp4a),
                                  3 exact int8 (tcgen05 kind::i8), 4 tcgen05 FP8 e4m3 */
     int32_t fast_aborted;     /* 1 if a bounded wait in the fast kernel gave up (rows then re-searched) */
-    uint64_t rows_refined;    /* uncertified rows sent through the candidate-collecting refine pass */
+    uint64_t rows_refined;    /* uncertified rows sent through the candidate-collecting refine pass (lockstep
+                                 batched training: batch rows settled by the exhaustive search, all steps) */
     double fast_ms;           /* device time of the fast contraction kernel(s) (CUDA events, summed) */
     uint64_t fast_launches;   /* launches of the fast contraction kernel */
     uint64_t rows_proposed;   /* proposer assign: rows searched in their proposed groups only */
@@ -179,6 +180,12 @@ int emb200_set_abort_test(emb200_handle* h, int stall_tile, uint64_t stall_ns);
  * chains per thread over 64 warps per SM, scalar fma.rn.f32 (tflops) and paired
  * fma.rn.f32x2 (tflops_paired); best of four timed launches each, CUDA events. */
 int emb200_measure_simt_peak(int ordinal, double* tflops, double* tflops_paired);
+
+/* tcgen05 BF16 MMA throughput of this device (TF/s) with operands resident in
+ * shared memory: cta_group::1 M=128 N=256 (the shape k_assign_tc issues) and a
+ * CTA pair's cta_group::2 M=256 N=256. A measurement for rooflines; no
+ * counterpart in the reference. */
+int emb200_measure_mma_peak(int ordinal, double* tflops_1sm, double* tflops_2sm);
 
 /* ---- training (src/lib.rs:201-225 and 348-491) --------------------------- */
 
