@@ -416,6 +416,74 @@ __global__ void k_b_research_small(const T* __restrict__ x, BArgs a) {
     }
 }
 
+// Exhaustive exact search with a CTA per listed row (256 threads): warp w scans
+// the centroids [w k / 8, (w + 1) k / 8) in ascending order in groups as
+// k_b_research does, and the warps' results merge by (score, index), finite
+// scores only: the lowest index among the smallest scores, label 0 when no score
+// beats +inf, as the reference's strict-< scan over all k. A row's centroid
+// loads are spread over eight warps, where k_b_research walks all k in one.
+template <typename T>
+__global__ void __launch_bounds__(256) k_b_research_cta(const T* __restrict__ x, BArgs a) {
+    __shared__ float wbest[8];
+    __shared__ uint32_t wlab[8];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint32_t n = a.ctl->redo;
+    const int gsz = a.match == kMatchAvx512 ? 16 : 8, gpw = 32 / gsz, g = lane / gsz;
+    const int d = a.d;
+    const float inf = __int_as_float(0x7f800000);
+    for (uint32_t r = blockIdx.x; r < n; r += gridDim.x) {
+        const uint32_t e = a.redo_list[r];
+        const int i = (int)(e >> 24), row = (int)(e & 0xFFFFFFu);
+        BStep st;
+        b_active(a, i, &st);
+        const BInst& I = a.inst[i];
+        const int k = (int)I.k;
+        const T* xr = x + (I.row0 + b_rows(a, I, st)[row]) * (size_t)d;
+        const float* ci = a.c + I.c_off;
+        const float* ni = a.norms + I.k_off;
+        const int jb = (int)(((long long)k * warp) / 8), je = (int)(((long long)k * (warp + 1)) / 8);
+        float best = inf;
+        uint32_t lab = 0;
+        for (int j0 = jb; j0 < je; j0 += gpw) {
+            const int j = j0 + g, jc = j < je ? j : je - 1;
+            const float dj = group_dot_ref(a.match, xr, ci + (size_t)jc * d, d, lane);
+            if (j < je) {
+                const float sc = score_ref(ni[j], dj);
+                if (sc < best) {
+                    best = sc;
+                    lab = (uint32_t)j;
+                }
+            }
+        }
+        for (int o = gsz; o < 32; o <<= 1) {
+            const float ob = __shfl_xor_sync(kFull, best, o);
+            const uint32_t ol = __shfl_xor_sync(kFull, lab, o);
+            if (ob < inf && (!(best < inf) || lex_less(ob, ol, best, lab))) {
+                best = ob;
+                lab = ol;
+            }
+        }
+        if (lane == 0) {
+            wbest[warp] = best;
+            wlab[warp] = lab;
+        }
+        const float xn = warp_sqnorm_ref(xr, d, lane);
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            float b = inf;
+            uint32_t l = 0;
+            for (int w = 0; w < 8; w++)
+                if (wbest[w] < inf && (!(b < inf) || lex_less(wbest[w], wlab[w], b, l))) {
+                    b = wbest[w];
+                    l = wlab[w];
+                }
+            a.blabels[I.b_off + row] = l;
+            a.bdist[I.b_off + row] = fmaxf(__fadd_rn(b, xn), 0.0f);
+        }
+        __syncthreads();  // wbest / wlab are rewritten for the next row
+    }
+}
+
 // Certification of every active instance's batch rows (one warp per row, the
 // reference's rounding for the selected match kernel, as k_certify); rows the
 // bound cannot settle are listed for the exhaustive search.
