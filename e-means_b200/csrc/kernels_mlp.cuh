@@ -66,14 +66,26 @@ __global__ void k_relu_grad(__nv_bfloat16* __restrict__ g, const __nv_bfloat16* 
     if (i < n && !(__bfloat162float(h[i]) > 0.0f)) g[i] = __float2bfloat16(0.0f);
 }
 
-// Bias gradient: column sums of a BF16 m x n matrix (row stride ld) into FP32
-// (one thread per column).
-__global__ void k_colsum(const __nv_bfloat16* __restrict__ g, int m, int n, size_t ld, float* __restrict__ out) {
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= n) return;
+// Bias gradient: column sums of a BF16 m x n matrix (row stride ld) into FP32.
+// A block of 256 threads per 32 columns: warp p adds rows p, p + 8, ... of its
+// lane's column in row order, then the eight partial sums are added in warp
+// order (a fixed order: the same bits on every run).
+__global__ void __launch_bounds__(256) k_colsum(const __nv_bfloat16* __restrict__ g, int m, int n, size_t ld,
+                                                float* __restrict__ out) {
+    __shared__ float part[8][32];
+    const int lane = threadIdx.x & 31, p = threadIdx.x >> 5;
+    const int c = blockIdx.x * 32 + lane;
     float s = 0.0f;
-    for (int r = 0; r < m; r++) s += __bfloat162float(g[(size_t)r * ld + c]);
-    out[c] = s;
+    if (c < n)
+        for (int r = p; r < m; r += 8) s += __bfloat162float(g[(size_t)r * ld + c]);
+    part[p][lane] = s;
+    __syncthreads();
+    if (p == 0 && c < n) {
+        float t = part[0][lane];
+#pragma unroll
+        for (int q = 1; q < 8; q++) t += part[q][lane];
+        out[c] = t;
+    }
 }
 
 // BF16 copy of FP32 values.
