@@ -701,8 +701,8 @@ struct TcBest {
 //   warps 2-3   row loaders: the next work item's row tile into the other buffer
 //               (BF16 hi/lo split or e4m3 with a per-row scale)
 //   warps 4-19  epilogue, four warps per TMEM lane quarter, 64 columns of each
-//               256-column tile per warp, read 16 at a time with the next TMEM
-//               load in flight while the current 16 are scored
+//               256-column tile per warp: all 64 loaded (four 16-column loads,
+//               one wait), the accumulator released, then the 64 scored
 // COLLECT = false: per-row (best key, column, lower bound of the rest) to part_s/part_i.
 // COLLECT = true : every centroid with approximate score <= theta[row] is appended
 //                  to cand[row][*] (cand_count[row] counts all, capped storage).
@@ -932,54 +932,67 @@ k_assign_tc(const T* __restrict__ x, const __grid_constant__ CUtensorMap map_hi,
                 // bound), raised by 2^-17 relative to cover a key's column bits.
                 float g1 = fminf(fminf(pub[r], pub[kTcBM + r]), fminf(pub[2 * kTcBM + r], pub[3 * kTcBM + r]));
                 g1 = fmaf(fabsf(g1), 0x1p-17f, g1);
-                uint32_t va[16], vb[16];
-                EMB_TMEM_LD16(taddr, va);
+                // The warp's 64 columns into registers (four 16-column loads, one
+                // wait), then the accumulator is released before they are scored.
+                uint32_t v4[4][16];
+                EMB_TMEM_LD16(taddr, v4[0]);
+                EMB_TMEM_LD16(taddr + 16, v4[1]);
+                EMB_TMEM_LD16(taddr + 32, v4[2]);
+                EMB_TMEM_LD16(taddr + 48, v4[3]);
                 tmem_wait_ld();
-                tc_regs_ready16(va);
+#pragma unroll
+                for (int h = 0; h < 4; h++) tc_regs_ready16(v4[h]);
+                tc_fence_before();
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&acc_empty[b]);
+                float sc4[4][16], mnh[4];
 #pragma unroll
                 for (int h = 0; h < 4; h++) {
-                    uint32_t(&cur)[16] = (h & 1) ? vb : va;
-                    uint32_t(&nxt)[16] = (h & 1) ? va : vb;
-                    if (h < 3) {
-                        EMB_TMEM_LD16(taddr + (h + 1) * 16, nxt);  // in flight while this half is scored
+                    tc_scores16<FP8>(v4[h], nrm + h * 16, nrm + kTcBN + h * 16, rs, sc4[h]);
+                    mnh[h] = tc_min16s(sc4[h]);
+                }
+                if (!COLLECT) {
+                    // One vote for the tile: when no row of the warp has a half whose
+                    // minimum is below the bound at the tile's start, every half only
+                    // lowers s2 (what the per-half rule below does in that case too).
+                    const float thr = fminf(g1, best.s1);
+                    const bool low = (mnh[0] < thr) | (mnh[1] < thr) | (mnh[2] < thr) | (mnh[3] < thr);
+                    if (!__any_sync(0xffffffffu, low)) {
+                        best.s2 = fminf(best.s2, fminf(fminf(mnh[0], mnh[1]), fminf(mnh[2], mnh[3])));
                     } else {
-                        // All four loads of this tile are complete: release the accumulator.
-                        tc_fence_before();
-                        __syncwarp();
-                        if (lane == 0) mbar_arrive(&acc_empty[b]);
-                    }
-                    float sc[16];
-                    tc_scores16<FP8>(cur, nrm + h * 16, nrm + kTcBN + h * 16, rs, sc);
-                    const float mn = tc_min16s(sc);
-                    if (!COLLECT) {
-                        if (__any_sync(0xffffffffu, mn < fminf(g1, best.s1))) {
-                            float k1, k2;
-                            const uint32_t jb = (uint32_t)((h & 1) * 16);
-                            tc_top2_16s(sc, jb, k1, k2);
-                            const uint32_t j1 = (uint32_t)(cb + (h >> 1) * 32) + (__float_as_uint(k1) & 31u);
-                            if (k1 < best.s1) {
-                                best.s2 = min3f(best.s2, best.s1, k2);
-                                best.s1 = k1;
-                                best.i1 = j1;
-                            } else {
-                                best.s2 = fminf(best.s2, k1);
-                            }
-                        } else {
-                            best.s2 = fminf(best.s2, mn);
-                        }
-                    } else if (mn <= theta) {
 #pragma unroll
-                        for (int j = 0; j < 16; j++) {
-                            const int col = cb + h * 16 + j;
-                            if (sc[j] <= theta && col < p.k) {
-                                const uint32_t slot = atomicAdd(&p.cand_count[row], 1u);
-                                if (slot < (uint32_t)p.cand_cap) p.cand[(size_t)row * p.cand_cap + slot] = (uint32_t)col;
+                        for (int h = 0; h < 4; h++) {
+                            if (__any_sync(0xffffffffu, mnh[h] < fminf(g1, best.s1))) {
+                                float k1, k2;
+                                const uint32_t jb = (uint32_t)((h & 1) * 16);
+                                tc_top2_16s(sc4[h], jb, k1, k2);
+                                const uint32_t j1 = (uint32_t)(cb + (h >> 1) * 32) + (__float_as_uint(k1) & 31u);
+                                if (k1 < best.s1) {
+                                    best.s2 = min3f(best.s2, best.s1, k2);
+                                    best.s1 = k1;
+                                    best.i1 = j1;
+                                } else {
+                                    best.s2 = fminf(best.s2, k1);
+                                }
+                            } else {
+                                best.s2 = fminf(best.s2, mnh[h]);
                             }
                         }
                     }
-                    if (h < 3) {
-                        tmem_wait_ld();
-                        tc_regs_ready16(nxt);
+                } else {
+#pragma unroll
+                    for (int h = 0; h < 4; h++) {
+                        if (mnh[h] <= theta) {
+#pragma unroll
+                            for (int j = 0; j < 16; j++) {
+                                const int col = cb + h * 16 + j;
+                                if (sc4[h][j] <= theta && col < p.k) {
+                                    const uint32_t slot = atomicAdd(&p.cand_count[row], 1u);
+                                    if (slot < (uint32_t)p.cand_cap)
+                                        p.cand[(size_t)row * p.cand_cap + slot] = (uint32_t)col;
+                                }
+                            }
+                        }
                     }
                 }
                 if (!COLLECT) pub[cq * kTcBM + r] = best.s1;  // the quarter's best key, for the other quarters
