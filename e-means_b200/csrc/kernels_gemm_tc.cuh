@@ -22,6 +22,12 @@
 namespace emb {
 
 constexpr int kGtBM = 128, kGtBN = 128, kGtStages = 4, kGtThreads = 192;
+
+// Two FP32 values as round-to-nearest BF16 in one word (the lower column in the low half).
+EMB_DEV uint32_t pack_bf16x2(float lo, float hi) {
+    return (uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(lo)) |
+           ((uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(hi)) << 16);
+}
 constexpr uint32_t kGtAtomBytes = 128 * 128;                  // 128 rows x one 128-byte K atom
 constexpr uint32_t kGtStageBytes = 2 * kGtAtomBytes;          // A and B atoms
 constexpr size_t kGtSmemBytes = kGtStages * kGtStageBytes + 256 + 1024;
@@ -116,23 +122,43 @@ k_gemm_tc(int M, int N, int K, int kc, const __grid_constant__ CUtensorMap map_a
             }
             if (row >= M || *abort_flag) continue;
             const int c0 = n0 + ch * 32;
+            // The lane's 32 consecutive columns of its row: 16-byte stores when the
+            // whole chunk is inside the matrix and the row is 16-byte aligned.
+            float o[32];
 #pragma unroll
             for (int j = 0; j < 32; j++) {
-                const int col = c0 + j;
-                if (col >= N) break;
                 float x = __uint_as_float(v[j]);
-                if (part) {
-                    part[((size_t)blockIdx.z * M + row) * N + col] = x;
-                } else if (EPI == kEpiF32) {
-                    ((float*)C)[(size_t)row * ldc + col] = x;
-                } else if (EPI == kEpiBiasF32) {
-                    ((float*)C)[(size_t)row * ldc + col] = x + bias[col];
-                } else if (EPI == kEpiBf16) {
-                    ((__nv_bfloat16*)C)[(size_t)row * ldc + col] = __float2bfloat16_rn(x);
+                if (!part && (EPI == kEpiBiasF32 || EPI == kEpiBiasBf16 || EPI == kEpiBiasReluBf16))
+                    x += c0 + j < N ? bias[c0 + j] : 0.0f;
+                if (!part && EPI == kEpiBiasReluBf16) x = fmaxf(x, 0.0f);
+                o[j] = x;
+            }
+            const bool f32out = part || EPI == kEpiF32 || EPI == kEpiBiasF32;
+            void* dst = part ? (void*)(part + ((size_t)blockIdx.z * M + row) * N + c0)
+                             : (f32out ? (void*)((float*)C + (size_t)row * ldc + c0)
+                                       : (void*)((__nv_bfloat16*)C + (size_t)row * ldc + c0));
+            if (c0 + 32 <= N && ((uintptr_t)dst & 15) == 0) {
+                if (f32out) {
+#pragma unroll
+                    for (int j = 0; j < 32; j += 4)
+                        reinterpret_cast<float4*>(dst)[j / 4] = make_float4(o[j], o[j + 1], o[j + 2], o[j + 3]);
                 } else {
-                    x += bias[col];
-                    if (EPI == kEpiBiasReluBf16) x = fmaxf(x, 0.0f);
-                    ((__nv_bfloat16*)C)[(size_t)row * ldc + col] = __float2bfloat16_rn(x);
+#pragma unroll
+                    for (int j = 0; j < 32; j += 8) {
+                        uint4 w;
+                        w.x = pack_bf16x2(o[j], o[j + 1]);
+                        w.y = pack_bf16x2(o[j + 2], o[j + 3]);
+                        w.z = pack_bf16x2(o[j + 4], o[j + 5]);
+                        w.w = pack_bf16x2(o[j + 6], o[j + 7]);
+                        reinterpret_cast<uint4*>(dst)[j / 8] = w;
+                    }
+                }
+            } else {
+#pragma unroll
+                for (int j = 0; j < 32; j++) {
+                    if (c0 + j >= N) break;
+                    if (f32out) ((float*)dst)[j] = o[j];
+                    else ((__nv_bfloat16*)dst)[j] = __float2bfloat16_rn(o[j]);
                 }
             }
         }

@@ -66,26 +66,41 @@ __global__ void k_relu_grad(__nv_bfloat16* __restrict__ g, const __nv_bfloat16* 
     if (i < n && !(__bfloat162float(h[i]) > 0.0f)) g[i] = __float2bfloat16(0.0f);
 }
 
-// Bias gradient: column sums of a BF16 m x n matrix (row stride ld) into FP32.
-// A block of 256 threads per 32 columns: warp p adds rows p, p + 8, ... of its
-// lane's column in row order, then the eight partial sums are added in warp
-// order (a fixed order: the same bits on every run).
-__global__ void __launch_bounds__(256) k_colsum(const __nv_bfloat16* __restrict__ g, int m, int n, size_t ld,
-                                                float* __restrict__ out) {
-    __shared__ float part[8][32];
+// Bias gradient: column sums of a BF16 m x n matrix (row stride ld) into FP32, in
+// two fixed-order passes (the same bits on every run). k_colsum_part: block
+// (x, y) sums rows [128 y, 128 y + 128) of columns [32 x, 32 x + 32), warp p its
+// 16 rows 16 p .. 16 p + 15 in order (all 16 loads in flight), the eight warps'
+// sums then in warp order, into part[y][col]. k_colsum_final adds the parts of
+// a column in y order.
+constexpr int kColsumRows = 128;
+__global__ void __launch_bounds__(256) k_colsum_part(const __nv_bfloat16* __restrict__ g, int m, int n, size_t ld,
+                                                     float* __restrict__ part) {
+    __shared__ float ws[8][32];
     const int lane = threadIdx.x & 31, p = threadIdx.x >> 5;
     const int c = blockIdx.x * 32 + lane;
+    const int r0 = blockIdx.y * kColsumRows + p * 16;
+    float v[16];
+#pragma unroll
+    for (int q = 0; q < 16; q++)
+        v[q] = (c < n && r0 + q < m) ? __bfloat162float(g[(size_t)(r0 + q) * ld + c]) : 0.0f;
     float s = 0.0f;
-    if (c < n)
-        for (int r = p; r < m; r += 8) s += __bfloat162float(g[(size_t)r * ld + c]);
-    part[p][lane] = s;
+#pragma unroll
+    for (int q = 0; q < 16; q++) s += v[q];
+    ws[p][lane] = s;
     __syncthreads();
     if (p == 0 && c < n) {
-        float t = part[0][lane];
+        float t = ws[0][lane];
 #pragma unroll
-        for (int q = 1; q < 8; q++) t += part[q][lane];
-        out[c] = t;
+        for (int q = 1; q < 8; q++) t += ws[q][lane];
+        part[(size_t)blockIdx.y * n + c] = t;
     }
+}
+__global__ void k_colsum_final(const float* __restrict__ part, int nparts, int n, float* __restrict__ out) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= n) return;
+    float t = 0.0f;
+    for (int y = 0; y < nparts; y++) t += part[(size_t)y * n + c];
+    out[c] = t;
 }
 
 // BF16 copy of FP32 values.
