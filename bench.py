@@ -823,7 +823,7 @@ def run_c5(args):
         p = emb.B200Assigner(0, precision="bf16x1")
         p.load_rows(x)
         t0 = time.perf_counter()
-        outp = p.train_resident_proposed(k, emb.Config(nepochs=5.0), late_epochs=1,
+        outp = p.train_resident_proposed(k, emb.Config(nepochs=5.0), late_epochs=args.late_epochs,
                                          net_steps=args.late_net_steps, groups=groups, top=32, mass=0.999)
         t_late = time.perf_counter() - t0
         stp = outp.stats
@@ -833,7 +833,7 @@ def run_c5(args):
         rows_trained = sum(out.recipe.epoch_rows)
         late = {"train_rows_per_s": rows_trained / t_late, "train_s": t_late,
                 "full_search_train_rows_per_s": rows_trained / t_train, "full_search_train_s": t_train,
-                "speedup": t_train / t_late,
+                "speedup": t_train / t_late, "late_epochs": args.late_epochs, "net_steps": args.late_net_steps,
                 "final_mse_delta": float(dist_p.astype(np.float64).mean()) / mse_f - 1.0,
                 "last_pass_label_agreement": float(np.mean(outp.labels == out.labels)),
                 "late_epoch_device_ms": stp["late_epochs_ms"], "proposer_fit_ms": stp["late_fit_ms"],
@@ -890,7 +890,8 @@ def run_c5(args):
             "speedup_vs_full_search": min(t_full, t_full3) / t_mlp, "speedup_vs_fp32_path": t_fp32 / t_mlp,
             "network_roofline": {"bound": "tensor", "achieved": flops_row * n / (st_mlp["propose_ms"] / 1e3) / 1e12,
                                  "peak": peaks["bf16_tflops_sustained"], "unit": "TFLOP/s",
-                                 "kernel": "k_gemm_bf16 x3 + k_mlp_input + k_topm_groups (forward pass)"},
+                                 "kernel": "k_mlp_tc: fused tcgen05 forward pass (standardised input, three "
+                                           "layers, top-m group selection in the epilogue)"},
             "times_s": {"data": t_data, "train": t_train, "grouping": t_group, "network_fit": t_fit},
             "proposer_in_training": late,
             "fit_loss_first_last": [float(losses[:20].mean()), float(losses[-20:].mean())],
@@ -972,6 +973,8 @@ def main():
     ap.add_argument("--proposer-configs", default="32:0:0.999,32:0:0.9999,16:0:0.99,8:0:0",
                     help="c5: top:confidence:mass settings of the proposer assign; the first is the headline")
     ap.add_argument("--c5-rows", type=int, default=10_000_000, help="c5: rows of the workload")
+    ap.add_argument("--late-epochs", type=int, default=1,
+                    help="C5: last epochs of the proposer-in-training run searched through the proposer")
     ap.add_argument("--late-net-steps", type=int, default=3000,
                     help="c5: Adam steps of the network fitted inside the proposed training run")
     ap.add_argument("--proposer-training", type=int, default=1,
