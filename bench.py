@@ -975,7 +975,7 @@ def main():
     ap.add_argument("--c5-rows", type=int, default=10_000_000, help="c5: rows of the workload")
     ap.add_argument("--late-epochs", type=int, default=1,
                     help="C5: last epochs of the proposer-in-training run searched through the proposer")
-    ap.add_argument("--late-net-steps", type=int, default=3000,
+    ap.add_argument("--late-net-steps", type=int, default=1000,
                     help="c5: Adam steps of the network fitted inside the proposed training run")
     ap.add_argument("--proposer-training", type=int, default=1,
                     help="c5: also train with the proposer in the last epoch (1) or not (0)")
