@@ -484,6 +484,76 @@ __global__ void __launch_bounds__(256) k_b_research_cta(const T* __restrict__ x,
     }
 }
 
+// Certification for f32 rows with d % 16 == 0 under the AVX-512 rounding: four
+// threads per row with 16-byte loads, the 16 lanes of the reference's sums in
+// the same tree as k_certify16v (the same bits as k_b_certify), a quarter of
+// the warps. Grid (ceil(max batch * 4 / 256), count).
+__global__ void __launch_bounds__(256) k_b_certify16v(const float* __restrict__ x, BArgs a) {
+    const int i = blockIdx.y;
+    BStep st;
+    if (!b_active(a, i, &st)) return;
+    const BInst& I = a.inst[i];
+    const int lane = threadIdx.x & 31, q = lane & 3;
+    const int row = (int)(((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 2);
+    const int m = (int)st.bn;
+    if (((int)(blockIdx.x * blockDim.x) >> 2) >= m) return;  // the whole block is past the batch
+    const bool live = row < m;
+    const int r = live ? row : m - 1;  // dead quarter-warps mirror a live row and write nothing
+    const int d = a.d, k = (int)I.k;
+    const float* xr = x + (I.row0 + b_rows(a, I, st)[r]) * (size_t)d;
+    Top2 t;
+    t.init();
+    for (uint32_t s = 0; s < I.nsplit; s++) {
+        const size_t o = (I.p_off + (size_t)s * I.batch + r) * 2;
+        t.push(a.part_s[o], a.part_i[o]);
+        t.push(a.part_s[o + 1], a.part_i[o + 1]);
+    }
+    const uint32_t j1 = t.i1 < (uint32_t)k ? t.i1 : 0u;
+    const uint32_t j2 = t.i2 < (uint32_t)k ? t.i2 : j1;
+    const float* ci = a.c + I.c_off;
+    const float* c1 = ci + (size_t)j1 * d;
+    const float* c2 = ci + (size_t)j2 * d;
+    float sq[4] = {0.0f, 0.0f, 0.0f, 0.0f}, p1[4] = {0.0f, 0.0f, 0.0f, 0.0f}, p2[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+    for (int e = 4 * q; e < d; e += 16) {
+        const float4 xv = *reinterpret_cast<const float4*>(xr + e);
+        const float4 u = *reinterpret_cast<const float4*>(c1 + e);
+        const float4 w = *reinterpret_cast<const float4*>(c2 + e);
+        const float xs[4] = {xv.x, xv.y, xv.z, xv.w}, us[4] = {u.x, u.y, u.z, u.w}, ws[4] = {w.x, w.y, w.z, w.w};
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            sq[j] = __fadd_rn(sq[j], __fmul_rn(xs[j], xs[j]));
+            p1[j] = __fmaf_rn(xs[j], us[j], p1[j]);
+            p2[j] = __fmaf_rn(xs[j], ws[j], p2[j]);
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < 4; j++) {  // lane l with l^8, then l^4 of the reference's 16 lanes
+        p1[j] = __fadd_rn(p1[j], __shfl_xor_sync(kFull, p1[j], 2));
+        p2[j] = __fadd_rn(p2[j], __shfl_xor_sync(kFull, p2[j], 2));
+    }
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+        p1[j] = __fadd_rn(p1[j], __shfl_xor_sync(kFull, p1[j], 1));
+        p2[j] = __fadd_rn(p2[j], __shfl_xor_sync(kFull, p2[j], 1));
+    }
+    const float a1 = __fadd_rn(__fadd_rn(p1[0], p1[2]), __fadd_rn(p1[1], p1[3]));
+    const float a2 = __fadd_rn(__fadd_rn(p2[0], p2[2]), __fadd_rn(p2[1], p2[3]));
+    float xn = -0.0f;
+    const int base = lane & ~3;
+#pragma unroll
+    for (int qq = 0; qq < 4; qq++)
+#pragma unroll
+        for (int j = 0; j < 4; j++) xn = __fadd_rn(xn, __shfl_sync(kFull, sq[j], base + qq));
+    if (live && q == 0) {
+        float theta = 0.0f;
+        if (!certify_decide(row, t, j1, j2, a1, a2, xn, k, a.norms + I.k_off, &a.bounds[i], a.ka, a.kb,
+                            a.blabels + I.b_off, a.bdist + I.b_off, nullptr, 0.0f, 0.0f, nullptr, &theta)) {
+            const uint32_t slot = atomicAdd(&a.ctl->redo, 1u);
+            a.redo_list[slot] = ((uint32_t)i << 24) | (uint32_t)row;
+        }
+    }
+}
+
 // Certification of every active instance's batch rows (one warp per row, the
 // reference's rounding for the selected match kernel, as k_certify); rows the
 // bound cannot settle are listed for the exhaustive search.
