@@ -701,6 +701,10 @@ def run_c4(args):
         return outs, float(np.median(times)), float(np.median(dev)), choice
 
     outs, t, t_dev, choice = timed_runs(False)
+    if args.c4_lockstep_only:  # profiling: the lockstep calls alone
+        print(json.dumps({"workload": args.workload, "lockstep_ms": t * 1e3, "device_ms": t_dev,
+                          "rows_per_s": epoch_rows / t, "autotuned_search_tile": choice}), flush=True)
+        return
     outs_s, t_streams, _, _ = timed_runs(True)
     # Sequential, per-kernel launches, one instance after the other.
     b = emb.B200Assigner(0, precision="fp32", train_eager=True, batched_streams=True)
@@ -973,6 +977,8 @@ def main():
     ap.add_argument("--proposer-configs", default="32:0:0.999,32:0:0.9999,16:0:0.99,8:0:0",
                     help="c5: top:confidence:mass settings of the proposer assign; the first is the headline")
     ap.add_argument("--c5-rows", type=int, default=10_000_000, help="c5: rows of the workload")
+    ap.add_argument("--c4-lockstep-only", action="store_true",
+                    help="C4: time the lockstep calls only (no streams-mode or sequential comparison)")
     ap.add_argument("--late-epochs", type=int, default=1,
                     help="C5: last epochs of the proposer-in-training run searched through the proposer")
     ap.add_argument("--late-net-steps", type=int, default=1000,
