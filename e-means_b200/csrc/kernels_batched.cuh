@@ -386,36 +386,6 @@ __global__ void k_b_certify_small(const T* __restrict__ x, BArgs a) {
     }
 }
 
-// Exhaustive exact search for small d: one thread per listed row, the reference's
-// strict-< scan over ascending centroids (lowest index on ties, label 0 when no
-// score beats +inf) in its rounding.
-template <typename T>
-__global__ void k_b_research_small(const T* __restrict__ x, BArgs a) {
-    const uint32_t n = a.ctl->redo;
-    const int d = a.d;
-    for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
-        const uint32_t e = a.redo_list[r];
-        const int i = (int)(e >> 24), row = (int)(e & 0xFFFFFFu);
-        BStep st;
-        b_active(a, i, &st);
-        const BInst& I = a.inst[i];
-        const T* xr = x + (I.row0 + b_rows(a, I, st)[row]) * (size_t)d;
-        const float* ci = a.c + I.c_off;
-        const float* ni = a.norms + I.k_off;
-        float best = __int_as_float(0x7f800000);
-        uint32_t lab = 0;
-        for (int j = 0; j < (int)I.k; j++) {
-            const float sc = score_ref(ni[j], dot_ref(a.match, xr, ci + (size_t)j * d, d));
-            if (sc < best) {
-                best = sc;
-                lab = (uint32_t)j;
-            }
-        }
-        a.blabels[I.b_off + row] = lab;
-        a.bdist[I.b_off + row] = fmaxf(__fadd_rn(best, sqnorm_ref(xr, d)), 0.0f);
-    }
-}
-
 // Exhaustive exact search with a CTA per listed row (256 threads): warp w scans
 // the centroids [w k / 8, (w + 1) k / 8) in ascending order in groups as
 // k_b_research does, and the warps' results merge by (score, index), finite
