@@ -282,6 +282,145 @@ __global__ void __launch_bounds__(256, 1) k_b_search(const T* __restrict__ x, BA
     }
 }
 
+// The search with the item's row block resident in shared memory (f32 rows,
+// d % 4 == 0, d <= kBResMaxD): the BM gathered rows are staged once per item
+// (transposed, As[t][row]) and each BN-centroid tile once per tile (the next
+// tile's values in registers while the current one is multiplied), so an
+// item's rows are read once instead of once per centroid tile and a tile costs
+// two block barriers instead of two per 16 dimensions. Scores, the per-row
+// top-2 and the partials as k_b_search.
+constexpr int kBResMaxD = 128;
+template <int BM, int BN>
+constexpr size_t b_res_smem() { return (size_t)kBResMaxD * (BM + BN) * sizeof(float); }
+
+template <int BM, int BN>
+__global__ void __launch_bounds__(256, 1) k_b_search_res(const float* __restrict__ x, BArgs a) {
+    constexpr int TM = BM / 16, TN = BN / 16;
+    constexpr int BV = BN * kBResMaxD / 4 / 256;  // float4 per thread of a centroid tile (d = kBResMaxD)
+    extern __shared__ __align__(16) float res_smem[];
+    float* As = res_smem;                    // [d][BM]
+    float* Bs = res_smem + kBResMaxD * BM;   // [d][BN]
+    __shared__ uint32_t item_s;
+    const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+    const int d = a.d, dq = d >> 2;
+    for (;;) {
+        if (tid == 0) item_s = atomicAdd(&a.ctl->qhead, 1u);
+        __syncthreads();
+        const uint32_t it = item_s;
+        __syncthreads();
+        if (it >= a.total_items) break;
+        const int i = (int)a.item_inst[it];
+        BStep st;
+        if (!b_active(a, i, &st)) continue;  // uniform: every thread read the same item
+        const BInst& I = a.inst[i];
+        const uint32_t local = it - I.item_off;
+        const int rt = (int)(local / I.nsplit), split = (int)(local % I.nsplit);
+        const int row0 = rt * BM;
+        if (row0 >= (int)st.bn) continue;
+        const uint32_t* ids = b_rows(a, I, st);
+        const float* xi = x + I.row0 * (size_t)d;
+        const float* ci = a.c + I.c_off;
+        const float* ni = a.norms + I.k_off;
+        const int k = (int)I.k, m = (int)st.bn;
+        const int ntiles = (k + BN - 1) / BN;
+        // the row block, transposed: element e = (chunk c, row r) with r fastest
+        for (int e = tid; e < BM * dq; e += 256) {
+            const int r = e % BM, c = e / BM;
+            float4 v = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            if (row0 + r < m) v = *reinterpret_cast<const float4*>(xi + (size_t)ids[row0 + r] * d + 4 * c);
+            As[(4 * c + 0) * BM + r] = v.x;
+            As[(4 * c + 1) * BM + r] = v.y;
+            As[(4 * c + 2) * BM + r] = v.z;
+            As[(4 * c + 3) * BM + r] = v.w;
+        }
+        auto load_b = [&](int col0, float4 (&rb)[BV]) {
+#pragma unroll
+            for (int q = 0; q < BV; q++) {
+                const int e = tid + 256 * q, cc = e % BN, c = e / BN;
+                rb[q] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                if (c < dq && col0 + cc < k) rb[q] = *reinterpret_cast<const float4*>(ci + (size_t)(col0 + cc) * d + 4 * c);
+            }
+        };
+        auto store_b = [&](const float4 (&rb)[BV]) {
+#pragma unroll
+            for (int q = 0; q < BV; q++) {
+                const int e = tid + 256 * q, cc = e % BN, c = e / BN;
+                if (c < dq) {
+                    Bs[(4 * c + 0) * BN + cc] = rb[q].x;
+                    Bs[(4 * c + 1) * BN + cc] = rb[q].y;
+                    Bs[(4 * c + 2) * BN + cc] = rb[q].z;
+                    Bs[(4 * c + 3) * BN + cc] = rb[q].w;
+                }
+            }
+        };
+        Top2 top[TM];
+#pragma unroll
+        for (int q = 0; q < TM; q++) top[q].init();
+        float4 rb[BV];
+        if (split < ntiles) load_b(split * BN, rb);
+        for (int tile = split; tile < ntiles; tile += (int)I.nsplit) {
+            const int col0 = tile * BN;
+            __syncthreads();  // the previous tile's readers are done with Bs (and As is written)
+            store_b(rb);
+            __syncthreads();
+            if (tile + (int)I.nsplit < ntiles) load_b((tile + (int)I.nsplit) * BN, rb);  // in flight meanwhile
+            float acc[TM][TN];
+#pragma unroll
+            for (int q = 0; q < TM; q++)
+#pragma unroll
+                for (int j = 0; j < TN; j++) acc[q][j] = 0.0f;
+#pragma unroll 4
+            for (int kk = 0; kk < d; kk++) {
+                float av[TM], bv[TN];
+#pragma unroll
+                for (int q = 0; q < TM / 2; q++) {
+                    av[q] = As[kk * BM + ty * (TM / 2) + q];
+                    av[TM / 2 + q] = As[kk * BM + BM / 2 + ty * (TM / 2) + q];
+                }
+#pragma unroll
+                for (int j = 0; j < TN / 2; j++) {
+                    bv[j] = Bs[kk * BN + tx * (TN / 2) + j];
+                    bv[TN / 2 + j] = Bs[kk * BN + BN / 2 + tx * (TN / 2) + j];
+                }
+#pragma unroll
+                for (int q = 0; q < TM; q++)
+#pragma unroll
+                    for (int j = 0; j < TN; j++) acc[q][j] = __fmaf_rn(av[q], bv[j], acc[q][j]);
+            }
+#pragma unroll
+            for (int j = 0; j < TN; j++) {
+                const int col = col0 + (j < TN / 2 ? tx * (TN / 2) + j : BN / 2 + tx * (TN / 2) + (j - TN / 2));
+                if (col < k) {
+                    const float nj = ni[col];
+#pragma unroll
+                    for (int q = 0; q < TM; q++) top[q].push(__fmaf_rn(-2.0f, acc[q][j], nj), (uint32_t)col);
+                }
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < TM; q++) {
+            top[q].merge_shfl_xor(1);
+            top[q].merge_shfl_xor(2);
+            top[q].merge_shfl_xor(4);
+            top[q].merge_shfl_xor(8);
+        }
+        if (tx == 0) {
+#pragma unroll
+            for (int q = 0; q < TM; q++) {
+                const int row = row0 + (q < TM / 2 ? ty * (TM / 2) + q : BM / 2 + ty * (TM / 2) + (q - TM / 2));
+                if (row < m) {
+                    const size_t o = (I.p_off + (size_t)split * I.batch + row) * 2;
+                    a.part_s[o] = top[q].s1;
+                    a.part_i[o] = top[q].i1;
+                    a.part_s[o + 1] = top[q].s2;
+                    a.part_i[o + 1] = top[q].i2;
+                }
+            }
+        }
+        __syncthreads();  // As is rewritten by the next item
+    }
+}
+
 // The search for small d (d <= D <= 32): one thread per batch row, an item being
 // 256 rows against centroid chunks split, split + nsplit, ... of 512 centroids,
 // each chunk staged in shared memory 8192 / D centroids at a time (every thread
