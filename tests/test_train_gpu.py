@@ -242,6 +242,32 @@ def test_lockstep_instances_equal_single_runs(emb, dtype, closing_f64):
         assert np.array_equal(outs[i].objective, single.objective), i
 
 
+@pytest.mark.parametrize("d", [16, 40])
+def test_lockstep_every_search_variant(emb, monkeypatch, d):
+    # Every search form the autotuner can pick (forced through
+    # EMB200_BATCHED_SEARCH_VARIANT; a form that does not apply to d is ignored
+    # and the default choice runs) gives the same bits: the certification and
+    # the exact re-search settle each row whatever the search's partials were.
+    sizes = [9000, 2600, 15000, 700]
+    ks = [150, 16, 90, 40]
+    _, x, inst = _uneven_instances(emb, d, sizes, ks, 300 + d)
+    cfg = emb.Config(nepochs=2.0)
+    ref = None
+    for v in range(11):
+        monkeypatch.setenv("EMB200_BATCHED_SEARCH_VARIANT", str(v))
+        a = emb.B200Assigner(0, precision="fp32")
+        a.load_rows(x)
+        outs = a.train_batched(inst, cfg)
+        a.close()
+        if ref is None:
+            ref = outs
+            continue
+        for o, q in zip(ref, outs):
+            assert np.array_equal(o.labels, q.labels), v
+            assert same_f32(o.centroids, q.centroids), v
+            assert o.n_splits == q.n_splits, v
+
+
 def test_lockstep_graph_eager_streams_agree(emb, orc, tmp_path, monkeypatch):
     # The captured global step replayed, the same kernels launched one by one, and
     # the per-instance streams mode give the same bits; k = 5000 takes the
