@@ -243,7 +243,7 @@ def test_lockstep_instances_equal_single_runs(emb, dtype, closing_f64):
 
 
 @pytest.mark.parametrize("d", [16, 40])
-def test_lockstep_every_search_variant(emb, monkeypatch, d):
+def test_lockstep_every_search_variant(emb, monkeypatch, tmp_path, d):
     # Every search form the autotuner can pick (forced through
     # EMB200_BATCHED_SEARCH_VARIANT; a form that does not apply to d is ignored
     # and the default choice runs) gives the same bits: the certification and
@@ -252,6 +252,7 @@ def test_lockstep_every_search_variant(emb, monkeypatch, d):
     ks = [150, 16, 90, 40]
     _, x, inst = _uneven_instances(emb, d, sizes, ks, 300 + d)
     cfg = emb.Config(nepochs=2.0)
+    monkeypatch.setenv("EMB200_AUTOTUNE_CACHE", str(tmp_path / "tune.txt"))
     ref = None
     for v in range(11):
         monkeypatch.setenv("EMB200_BATCHED_SEARCH_VARIANT", str(v))
