@@ -474,7 +474,18 @@ __global__ void __launch_bounds__(256) k_b_search_small(const T* __restrict__ x,
             }
             for (int j = tid; j < nc; j += 256) ns[j] = ni[col0 + j];
             __syncthreads();
-            for (int j = 0; j < nc; j++) {
+            // four centroids' dot products at a time: independent FMA chains in flight
+            int j = 0;
+            for (; j + 4 <= nc; j += 4) {
+                float dot[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+#pragma unroll
+                for (int t = 0; t < D; t++)
+#pragma unroll
+                    for (int u = 0; u < 4; u++) dot[u] = __fmaf_rn(xr[t], cs[(j + u) * D + t], dot[u]);
+#pragma unroll
+                for (int u = 0; u < 4; u++) top.push(__fmaf_rn(-2.0f, dot[u], ns[j + u]), (uint32_t)(col0 + j + u));
+            }
+            for (; j < nc; j++) {
                 float dot = 0.0f;
 #pragma unroll
                 for (int t = 0; t < D; t++) dot = __fmaf_rn(xr[t], cs[j * D + t], dot);
