@@ -130,6 +130,17 @@ struct Top2 {
             }
         }
     }
+    // Branch-free insertion for an approximate search: strict <, so the earlier
+    // index keeps a tie and +inf / NaN scores are never inserted. The exact
+    // certification and re-search settle every row whatever the partials are,
+    // so only their values as bounds matter, not the tie order.
+    EMB_DEV void push_fast(float s, uint32_t i) {
+        const bool b1 = s < s1, b2 = s < s2;
+        s2 = b1 ? s1 : (b2 ? s : s2);
+        i2 = b1 ? i1 : (b2 ? i : i2);
+        s1 = b1 ? s : s1;
+        i1 = b1 ? i : i1;
+    }
     EMB_DEV void merge(const Top2& o) {
         push(o.s1, o.i1);
         push(o.s2, o.i2);

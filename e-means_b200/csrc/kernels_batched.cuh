@@ -255,7 +255,7 @@ __global__ void __launch_bounds__(256, 1) k_b_search(const T* __restrict__ x, BA
                 if (col < k) {
                     const float nj = ni[col];
 #pragma unroll
-                    for (int q = 0; q < TM; q++) top[q].push(__fmaf_rn(-2.0f, acc[q][j], nj), (uint32_t)col);
+                    for (int q = 0; q < TM; q++) top[q].push_fast(__fmaf_rn(-2.0f, acc[q][j], nj), (uint32_t)col);
                 }
             }
         }
@@ -393,7 +393,7 @@ __global__ void __launch_bounds__(256, 1) k_b_search_res(const float* __restrict
                 if (col < k) {
                     const float nj = ni[col];
 #pragma unroll
-                    for (int q = 0; q < TM; q++) top[q].push(__fmaf_rn(-2.0f, acc[q][j], nj), (uint32_t)col);
+                    for (int q = 0; q < TM; q++) top[q].push_fast(__fmaf_rn(-2.0f, acc[q][j], nj), (uint32_t)col);
                 }
             }
         }
@@ -483,13 +483,13 @@ __global__ void __launch_bounds__(256) k_b_search_small(const T* __restrict__ x,
 #pragma unroll
                     for (int u = 0; u < 4; u++) dot[u] = __fmaf_rn(xr[t], cs[(j + u) * D + t], dot[u]);
 #pragma unroll
-                for (int u = 0; u < 4; u++) top.push(__fmaf_rn(-2.0f, dot[u], ns[j + u]), (uint32_t)(col0 + j + u));
+                for (int u = 0; u < 4; u++) top.push_fast(__fmaf_rn(-2.0f, dot[u], ns[j + u]), (uint32_t)(col0 + j + u));
             }
             for (; j < nc; j++) {
                 float dot = 0.0f;
 #pragma unroll
                 for (int t = 0; t < D; t++) dot = __fmaf_rn(xr[t], cs[j * D + t], dot);
-                top.push(__fmaf_rn(-2.0f, dot, ns[j]), (uint32_t)(col0 + j));
+                top.push_fast(__fmaf_rn(-2.0f, dot, ns[j]), (uint32_t)(col0 + j));
             }
         }
         if (have) {
