@@ -848,7 +848,7 @@ def run_c5(args):
                         "and fitting the network on the previous epoch's labels); MSE from an exact assign of "
                         "all rows to each run's final centroids"}
     # FP64 brute force on a sample of rows: agreement of each path's labels
-    sample = np.random.default_rng(3).choice(n, 4096, replace=False)
+    sample = np.random.default_rng(3).choice(n, 32768, replace=False)
     bl, _ = orc.bruteforce_f64(x[sample], out.centroids)
     a.close()
     # the plain FP32 path on the first rows (its pass over all rows would take minutes)
