@@ -974,7 +974,7 @@ def main():
     ap.add_argument("--workload", default="c2", choices=["c2", "c1", "c3", "c4a", "c4b", "c5", "report"],
                     help="c2: the headline assign benchmark; the others: the remaining configurations")
     ap.add_argument("--proposer-steps", type=int, default=8000, help="c5: Adam steps of the network")
-    ap.add_argument("--proposer-configs", default="32:0:0.999,32:0:0.9999,16:0:0.99,8:0:0",
+    ap.add_argument("--proposer-configs", default="32:0.99:0.9995,32:0:0.999,32:0.999:0.9995,8:0:0",
                     help="c5: top:confidence:mass settings of the proposer assign; the first is the headline")
     ap.add_argument("--c5-rows", type=int, default=10_000_000, help="c5: rows of the workload")
     ap.add_argument("--c4-lockstep-only", action="store_true",
