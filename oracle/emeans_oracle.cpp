@@ -538,7 +538,7 @@ int orc_i8_assign(int bits, const int8_t* x, size_t m, size_t d, const float* c,
 }
 
 // ---------------------------------------------------------------- FP64 brute force
-// Exact nearest centroid in f64, lowest index on ties (judge of label agreement).
+// Exact nearest centroid in f64, lowest index on ties (the yardstick of label agreement).
 void orc_bruteforce_f64(int dtype, const void* x, size_t m, size_t d, const float* c, size_t k, uint32_t* labels,
                         double* dist, int threads) {
 #pragma omp parallel for schedule(dynamic, 16) num_threads(threads)

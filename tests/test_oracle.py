@@ -1,7 +1,7 @@
 """Pins the CPU oracle against the reference crate's own known-answer tests.
 
 Each test restates one of the reference's unit tests (cited) against the C++
-restatement in oracle/, so the oracle is trusted before it judges the GPU.
+restatement in oracle/, so the oracle is trusted before it checks the GPU.
 """
 import numpy as np
 import pytest
