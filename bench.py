@@ -763,6 +763,10 @@ def run_c5(args):
     t_data = time.perf_counter() - t0
     a = emb.B200Assigner(0, precision="bf16x1")
     a.load_rows(x)
+    # An untimed short run first: the process's one-time costs (kernel loading)
+    # do not fall on the timed full-search training, which the proposer-in-
+    # training run is compared with.
+    a.train_resident(k, emb.Config(nepochs=0.2))
     t0 = time.perf_counter()
     out = a.train_resident(k, emb.Config(nepochs=5.0))
     t_train = time.perf_counter() - t0
