@@ -131,6 +131,9 @@ struct emb200_handle {
     size_t kpad = 0;
     CUtensorMap map_hi{}, map_lo{};  // TMA descriptors of c_hi / c_lo (128B swizzle, 64 x 128 boxes)
     bool maps_ok = false;
+    // Half-norms split into BF16 parts for the single-term search that sums the
+    // norms inside the contraction ([whole tiles][16], k_prep_nrm16)
+    DevBuf<__nv_bfloat16> nrm16;
     DevBuf<int8_t> c8;   // I8 centroids (CpuI8Assigner)
     DevBuf<int16_t> c16; // I16 centroids: round(c * 2^ishift)
     int ishift = 0;      // I16 scale exponent (src/cpu_i8.rs:97)
@@ -250,10 +253,23 @@ int smem_attr_once(emb200_handle* h, std::atomic<uint64_t>& done, const void* fn
 size_t elt_size(int dtype) { return dtype == EMB200_F32 ? 4 : 1; }
 
 // Error-bound coefficients of the certification, E = ka |x| cmax + kb nmax
-// (see k_certify). u = 2^-24 (f32 rounding), ub = 2^-9 (bf16 rounding); the
+// (see k_certify). u = 2^-24 (f32 rounding), ub = 2^-8 (bf16 rounding: 8
+// significant bits, round to nearest); the
 // tensor-core accumulation is allowed one f32 truncation (2u) per product term.
-void bound_coefficients(int precision, int dtype, size_t d, bool packed, float* ka, float* kb) {
-    const double u = std::ldexp(1.0, -24), ub = std::ldexp(1.0, -9);
+//
+// The single-term BF16 search of f32 rows (norm_mma) sums the half-norm's three
+// BF16 parts in the same tensor-core accumulation as the d products: three more
+// truncated terms, whose magnitudes add |norm| / 2 to the sum they are relative to,
+// so the score (twice the accumulator) gains gamma(d + 5, 2u) |norm|.
+//
+// kr (single-term BF16, when the caller asks for it): the operands' rounding is
+// bounded per row instead, by kr (xr cmax + (|x| + xr) dmax) with xr = |x - bf16(x)|
+// of the row and dmax >= max_j |c_j - bf16(c_j)| (exact identity plus Cauchy-Schwarz,
+// in score units, times the same 1.25 margin), and leaves ka.
+void bound_coefficients(int precision, int dtype, size_t d, bool packed, float* ka, float* kb, bool norm_mma = false,
+                        float* kr = nullptr) {
+    if (kr) *kr = 0.0f;
+    const double u = std::ldexp(1.0, -24), ub = std::ldexp(1.0, -8);
     auto gamma = [](double n, double unit) { return n * unit / (1.0 - n * unit); };
     double g_ref = gamma((double)d + 2, u);  // reference dot vs exact
     double a;
@@ -273,9 +289,14 @@ void bound_coefficients(int precision, int dtype, size_t d, bool packed, float* 
         a = 2.0 * (rep + 1.02 * gamma(terms * (double)d + 2, 2 * u) + g_ref) + 4.02 * u;
     } else {
         double rep = dtype == EMB200_F32 ? 2.0 * ub + ub * ub : ub;
-        a = 2.0 * (rep + 1.02 * gamma((double)d + 2, 2 * u) + g_ref) + 4.02 * u;
+        if (kr) {
+            rep = 0.0;
+            *kr = 1.25f * 2.0f;
+        }
+        a = 2.0 * (rep + 1.02 * gamma((double)d + (norm_mma ? 5 : 2), 2 * u) + g_ref) + 4.02 * u;
     }
     double b = 2.0 * u;
+    if (norm_mma) b += 1.02 * gamma((double)d + 5, 2 * u);
     if (packed) {  // tensor-core top-2 keys carry the column in 5 mantissa bits: |key - s| <= 2^-18 |s|
         const double t = std::ldexp(1.0, -18);
         a += 2.01 * t;
@@ -349,6 +370,8 @@ int prepare_centroids(emb200_handle* h) {
         if (rc) return rc;
         rc = encode_bf16_map(h, &h->map_lo, lo);
         if (rc) return rc;
+        // Allocated here, outside any captured epoch; filled before each search.
+        if (h->nrm16.ensure(kp * 16)) return fail(h, EMB200_ENOMEM, "BF16 norm allocation failed");
         h->maps_ok = true;
     }
     k_prep_centroids<<<(unsigned)((k + 7) / 8), 256, 0, st>>>(h->c.p, k, d, h->norms.p, h->bounds.p, hi, lo,
@@ -579,16 +602,16 @@ int tc_nsplit(const emb200_handle* h, size_t m) {
     return best;
 }
 
-template <typename T, bool COLLECT, bool FP8>
+template <typename T, bool COLLECT, bool FP8, bool NM = false>
 int launch_tc_kernel(emb200_handle* h, const T* x, const TcParams& p, int nsplit, cudaStream_t st) {
-    const TcLayout L = tc_layout(p.kpad, p.nterms, FP8);
+    const TcLayout L = tc_layout(p.kpad, p.nterms, FP8, NM);
     // At least 120 KB so that two CTAs never share an SM: each holds all 512 TMEM columns.
     const size_t smem = std::max<size_t>(L.total + 1024, 120 * 1024);
-    SMEM_ATTR_ONCE((k_assign_tc<T, COLLECT, FP8>), 227 * 1024);  // one flag per instantiation
+    SMEM_ATTR_ONCE((k_assign_tc<T, COLLECT, FP8, NM>), 227 * 1024);  // one flag per instantiation
     // Persistent: one CTA per SM, or one per work item when there are fewer.
     const size_t items = (p.m + (size_t)kTcBM - 1) / kTcBM * (size_t)nsplit;
     const unsigned grid = (unsigned)std::max<size_t>(1, std::min(items, (size_t)h->sm_count));
-    k_assign_tc<T, COLLECT, FP8><<<grid, kTcPThreads, smem, st>>>(x, FP8 ? h->map_f8 : h->map_hi, h->map_lo, p);
+    k_assign_tc<T, COLLECT, FP8, NM><<<grid, kTcPThreads, smem, st>>>(x, FP8 ? h->map_f8 : h->map_hi, h->map_lo, p);
     CKL();
     return EMB200_OK;
 }
@@ -624,6 +647,15 @@ int launch_tc(emb200_handle* h, const T* x, const uint32_t* gather, const uint32
     p.nsplit = nsplit;
     if constexpr (!COLLECT && std::is_same<T, float>::value) {
         if (fp8) return launch_tc_kernel<T, false, true>(h, x, p, nsplit, st);
+        // Single-term BF16 search of f32 rows: norms summed inside the contraction
+        // (the certification bound allows for it whenever this mode is searched).
+        const size_t kp = (h->k + kTcBN - 1) / kTcBN * kTcBN;
+        if (nterms == 1 && h->nrm16.n >= kp * 16) {
+            k_prep_nrm16<<<(unsigned)((kp + 255) / 256), 256, 0, st>>>(h->norms.p, (int)kp, h->nrm16.p);
+            CKL();
+            p.nrm16 = h->nrm16.p;
+            return launch_tc_kernel<T, false, false, true>(h, x, p, nsplit, st);
+        }
     }
     return launch_tc_kernel<T, COLLECT, false>(h, x, p, nsplit, st);
 }
@@ -768,8 +800,9 @@ int settle_rows(emb200_handle* h, const T* x, const uint32_t* gather, size_t m, 
     if (h->redo_rows.ensure(m) || h->redo_theta.ensure(m) || h->counters.ensure(8))
         return fail(h, EMB200_ENOMEM, "scratch allocation failed for %zu rows", m);
     uint32_t* ctr = h->counters.p;
-    float ka, kb, ka2, kb2;
-    bound_coefficients(fast_prec, dtype, h->d, tc, &ka, &kb);
+    float ka, kb, ka2, kb2, kr;
+    bound_coefficients(fast_prec, dtype, h->d, tc, &ka, &kb,
+                       tc && fast_prec == EMB200_PREC_BF16X1 && dtype == EMB200_F32, &kr);
     bound_coefficients(EMB200_PREC_BF16, dtype, h->d, false, &ka2, &kb2);
     const int match = h->opts.match_kernel;
     bool vec4 = false;
@@ -779,18 +812,18 @@ int settle_rows(emb200_handle* h, const T* x, const uint32_t* gather, size_t m, 
         k_certify16v<<<(unsigned)((m + 63) / 64), 256, 0, st>>>(
             (const float*)x, gather, (int)m, d, h->c.p, h->norms.p, k, h->part_s.p, h->part_i.p, nsplit, h->bounds.p,
             ka, kb, labels, dist, h->redo_rows.p, ctr, ctr + 1, tc ? (const int*)(ctr + 2) : nullptr, h->redo_theta.p,
-            ka2, kb2, row_bounds);
+            ka2, kb2, row_bounds, kr);
     } else if (match == kMatchAvx512) {
         k_certify16<T><<<(unsigned)((m + 15) / 16), 256, 0, st>>>(
             x, gather, (int)m, d, h->c.p, h->norms.p, k, h->part_s.p, h->part_i.p, nsplit, h->bounds.p, ka, kb, labels,
             dist, h->redo_rows.p, ctr, ctr + 1, tc ? (const int*)(ctr + 2) : nullptr, h->redo_theta.p, ka2, kb2,
-            row_bounds);
+            row_bounds, kr);
     } else {
         k_certify<T><<<(unsigned)((m + 7) / 8), 256, 0, st>>>(x, gather, (int)m, d, h->c.p, h->norms.p, k, h->part_s.p,
                                                                h->part_i.p, nsplit, h->bounds.p, ka, kb, match, labels,
                                                                dist, h->redo_rows.p, ctr, ctr + 1,
                                                                tc ? (const int*)(ctr + 2) : nullptr, h->redo_theta.p,
-                                                               ka2, kb2, row_bounds);
+                                                               ka2, kb2, row_bounds, kr);
     }
     CKL();
     if (graph) {
@@ -970,7 +1003,7 @@ int emb200_destroy(emb200_handle* h) {
     if (!h) return EMB200_OK;
     cudaSetDevice(h->device);
     if (h->stream) cudaStreamSynchronize(h->stream);
-    h->c.release(); h->norms.release(); h->bias.release(); h->bounds.release();
+    h->c.release(); h->norms.release(); h->bias.release(); h->bounds.release(); h->nrm16.release();
     h->c_hi.release(); h->c_lo.release(); h->c8.release(); h->c16.release(); h->off8.release();
     h->rows.release(); h->res_labels.release(); h->res_dist.release();
     h->stage.release(); h->st_labels.release(); h->st_dist.release();

@@ -13,8 +13,14 @@ struct Bounds {
     float cmax;  // >= max_j |c_j| (upper-rounded)
     float nmax;  // >= max_j |norms_j| (norms include the bias)
     float cmax_hi;  // >= max_j |bf16(c_j)| (three-term split bound)
-    float pad;
+    float dmax;     // >= max_j |c_j - bf16(c_j)| (single-term residual bound)
 };
+
+// Upper bound of |v - bf16(v)|^2 summed into acc (v - bf16(v) is exact in f32).
+EMB_DEV float bf16_resid_sq(float v, float acc) {
+    const float r = v - __bfloat162float(__float2bfloat16_rn(v));
+    return __fmaf_ru(r, r, acc);
+}
 
 EMB_DEV void atomic_max_pos(float* addr, float v) {
     // Non-negative floats order like their bit patterns.
@@ -99,10 +105,11 @@ __global__ void k_prep_centroids(const float* __restrict__ c, int k, int d, floa
     if (warp >= k) return;
     const float* cj = c + (size_t)warp * d;
     float nrm = warp_sqnorm_ref(cj, d, lane);
-    float ss = 0.0f, ssh = 0.0f;
+    float ss = 0.0f, ssh = 0.0f, ssd = 0.0f;
     for (int i = lane; i < kpad; i += 32) {
         float v = i < d ? cj[i] : 0.0f;
         ss = __fmaf_ru(v, v, ss);
+        ssd = bf16_resid_sq(v, ssd);
         if (hi) {
             __nv_bfloat16 h = __float2bfloat16_rn(v);
             float hf = __bfloat162float(h);
@@ -115,12 +122,14 @@ __global__ void k_prep_centroids(const float* __restrict__ c, int k, int d, floa
     for (int o = 16; o; o >>= 1) {
         ss = __fadd_ru(ss, __shfl_xor_sync(kFull, ss, o));
         ssh = __fadd_ru(ssh, __shfl_xor_sync(kFull, ssh, o));
+        ssd = __fadd_ru(ssd, __shfl_xor_sync(kFull, ssd, o));
     }
     if (lane == 0) {
         norms[warp] = nrm;
         atomic_max_pos(&bounds->cmax, __fmul_ru(__fsqrt_ru(ss), 1.0000005f));
         atomic_max_pos(&bounds->nmax, fabsf(nrm));
         atomic_max_pos(&bounds->cmax_hi, __fmul_ru(__fsqrt_ru(ssh), 1.0000005f));
+        atomic_max_pos(&bounds->dmax, __fmul_ru(__fsqrt_ru(ssd), 1.0000005f));
     }
 }
 
@@ -145,7 +154,8 @@ EMB_DEV bool certify_decide(int row, const Top2& t, uint32_t j1, uint32_t j2, fl
                             const float* __restrict__ norms, const Bounds* __restrict__ bounds, float ka, float kb,
                             uint32_t* __restrict__ labels, float* __restrict__ dist,
                             const int* __restrict__ fast_err, float ka2, float kb2,
-                            const float2* __restrict__ row_bounds, float* theta_out) {
+                            const float2* __restrict__ row_bounds, float* theta_out, float kr = 0.0f,
+                            float xr = 0.0f) {
     bool ok = t.i1 < (uint32_t)k && (k < 2 || t.i2 < (uint32_t)k);
     const float s1 = score_ref(norms[j1], a1);
     float sb = s1;
@@ -159,8 +169,13 @@ EMB_DEV bool certify_decide(int row, const Top2& t, uint32_t j1, uint32_t j2, fl
     }
     if (ok && k > 2) {
         const float xnorm = __fmul_ru(__fsqrt_ru(fmaxf(xn, 0.0f)), 1.0000005f);
-        const float E = __fadd_ru(__fmul_ru(__fmul_ru(ka, xnorm), row_bounds ? row_bounds[row].x : bounds->cmax),
-                                  __fmul_ru(kb, row_bounds ? row_bounds[row].y : bounds->nmax));
+        const float cm = row_bounds ? row_bounds[row].x : bounds->cmax;
+        float E = __fadd_ru(__fmul_ru(__fmul_ru(ka, xnorm), cm),
+                            __fmul_ru(kb, row_bounds ? row_bounds[row].y : bounds->nmax));
+        // Single-term BF16: x.c - bf16(x).bf16(c) = (x - bf16(x)).c + bf16(x).(c - bf16(c)),
+        // at most xr cmax + (|x| + xr) dmax, with xr = |x - bf16(x)| of this row.
+        if (kr > 0.0f)
+            E = __fadd_ru(E, __fmul_ru(kr, __fadd_ru(__fmul_ru(xr, cm), __fmul_ru(__fadd_ru(xnorm, xr), bounds->dmax))));
         const float thr = __fsub_rd(t.s2, E);
         ok = isfinite(E) && sb < thr;  // NaN-safe: any NaN fails
     }
@@ -201,7 +216,7 @@ __global__ void k_certify(const T* __restrict__ x, const uint32_t* __restrict__ 
                           uint32_t* __restrict__ redo_rows, uint32_t* __restrict__ redo_count,
                           uint32_t* __restrict__ cert_count, const int* __restrict__ fast_err,
                           float* __restrict__ redo_theta, float ka2, float kb2,
-                          const float2* __restrict__ row_bounds = nullptr) {
+                          const float2* __restrict__ row_bounds = nullptr, float kr = 0.0f) {
     int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     int lane = threadIdx.x & 31;
     if (row >= m) return;
@@ -224,10 +239,17 @@ __global__ void k_certify(const T* __restrict__ x, const uint32_t* __restrict__ 
     float dg = group_dot_ref(match, xr, c + (size_t)jg * d, d, lane);
     float d1 = __shfl_sync(kFull, dg, 0);
     float d2 = __shfl_sync(kFull, dg, gsz);
+    float xres = 0.0f;  // |x - bf16(x)|, upper-rounded (single-term BF16 bound)
+    if (kr > 0.0f) {
+        float acc = 0.0f;
+        for (int i = lane; i < d; i += 32) acc = bf16_resid_sq(to_f32(xr[i]), acc);
+        for (int o = 16; o; o >>= 1) acc = __fadd_ru(acc, __shfl_xor_sync(kFull, acc, o));
+        xres = __fmul_ru(__fsqrt_ru(acc), 1.0000005f);
+    }
     if (lane != 0) return;
     float theta = 0.0f;
     if (certify_decide(row, t, j1, j2, d1, d2, xn, k, norms, bounds, ka, kb, labels, dist, fast_err, ka2, kb2,
-                       row_bounds, &theta)) {
+                       row_bounds, &theta, kr, xres)) {
         atomicAdd(cert_count, 1u);
     } else {
         const uint32_t slot = atomicAdd(redo_count, 1u);
@@ -272,7 +294,7 @@ __global__ void k_certify16(const T* __restrict__ x, const uint32_t* __restrict_
                             uint32_t* __restrict__ redo_rows, uint32_t* __restrict__ redo_count,
                             uint32_t* __restrict__ cert_count, const int* __restrict__ fast_err,
                             float* __restrict__ redo_theta, float ka2, float kb2,
-                            const float2* __restrict__ row_bounds = nullptr) {
+                            const float2* __restrict__ row_bounds = nullptr, float kr = 0.0f) {
     const int lane = threadIdx.x & 31, l = lane & 15, half = lane >> 4;
     const int row = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 2 + half;
     const bool live = row < m;
@@ -291,11 +313,12 @@ __global__ void k_certify16(const T* __restrict__ x, const uint32_t* __restrict_
     const float* c1 = c + (size_t)j1 * d;
     const float* c2 = c + (size_t)j2 * d;
     const int body = d & ~15, dr = (d + 15) & ~15;
-    float sq = 0.0f, a1 = 0.0f, a2 = 0.0f;
+    float sq = 0.0f, a1 = 0.0f, a2 = 0.0f, rs = 0.0f;
     for (int i = l; i < dr; i += 16) {
         const bool in = i < d;
         const float xv = in ? to_f32(xr[i]) : 0.0f;
         if (i < body) sq = __fadd_rn(sq, __fmul_rn(xv, xv));
+        if (kr > 0.0f) rs = bf16_resid_sq(xv, rs);
         a1 = __fmaf_rn(xv, in ? c1[i] : 0.0f, a1);
         a2 = __fmaf_rn(xv, in ? c2[i] : 0.0f, a2);
     }
@@ -303,6 +326,7 @@ __global__ void k_certify16(const T* __restrict__ x, const uint32_t* __restrict_
     for (int o = 8; o; o >>= 1) {
         a1 = __fadd_rn(a1, __shfl_xor_sync(kFull, a1, o));
         a2 = __fadd_rn(a2, __shfl_xor_sync(kFull, a2, o));
+        rs = __fadd_ru(rs, __shfl_xor_sync(kFull, rs, o));
     }
     float xn = -0.0f;
     const int base = half * 16;
@@ -318,7 +342,7 @@ __global__ void k_certify16(const T* __restrict__ x, const uint32_t* __restrict_
     float theta = 0.0f;
     if (live && l == 0) {
         ok = certify_decide(row, t, j1, j2, a1, a2, xn, k, norms, bounds, ka, kb, labels, dist, fast_err, ka2, kb2,
-                              row_bounds, &theta);
+                              row_bounds, &theta, kr, __fmul_ru(__fsqrt_ru(rs), 1.0000005f));
         redo = !ok;
     }
     certify_tally(ok, redo, row, theta, cert_count, redo_count, redo_rows, redo_theta);
@@ -336,7 +360,7 @@ __global__ void k_certify16v(const float* __restrict__ x, const uint32_t* __rest
                              float* __restrict__ dist, uint32_t* __restrict__ redo_rows,
                              uint32_t* __restrict__ redo_count, uint32_t* __restrict__ cert_count,
                              const int* __restrict__ fast_err, float* __restrict__ redo_theta, float ka2, float kb2,
-                             const float2* __restrict__ row_bounds = nullptr) {
+                             const float2* __restrict__ row_bounds = nullptr, float kr = 0.0f) {
     const int lane = threadIdx.x & 31, q = lane & 3;
     const int row = (int)(((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 2);
     const bool live = row < m;
@@ -355,6 +379,7 @@ __global__ void k_certify16v(const float* __restrict__ x, const uint32_t* __rest
     const float* c1 = c + (size_t)j1 * d;
     const float* c2 = c + (size_t)j2 * d;
     float sq[4] = {0.0f, 0.0f, 0.0f, 0.0f}, p1[4] = {0.0f, 0.0f, 0.0f, 0.0f}, p2[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+    float rs = 0.0f;
     for (int i = 4 * q; i < d; i += 16) {
         const float4 xv = *reinterpret_cast<const float4*>(xr + i);
         const float4 u = *reinterpret_cast<const float4*>(c1 + i);
@@ -365,8 +390,11 @@ __global__ void k_certify16v(const float* __restrict__ x, const uint32_t* __rest
             sq[j] = __fadd_rn(sq[j], __fmul_rn(xs[j], xs[j]));
             p1[j] = __fmaf_rn(xs[j], us[j], p1[j]);
             p2[j] = __fmaf_rn(xs[j], ws[j], p2[j]);
+            if (kr > 0.0f) rs = bf16_resid_sq(xs[j], rs);
         }
     }
+    rs = __fadd_ru(rs, __shfl_xor_sync(kFull, rs, 2));
+    rs = __fadd_ru(rs, __shfl_xor_sync(kFull, rs, 1));
 #pragma unroll
     for (int j = 0; j < 4; j++) {  // lane l with l^8, then l^4
         p1[j] = __fadd_rn(p1[j], __shfl_xor_sync(kFull, p1[j], 2));
@@ -390,7 +418,7 @@ __global__ void k_certify16v(const float* __restrict__ x, const uint32_t* __rest
     float theta = 0.0f;
     if (live && q == 0) {
         ok = certify_decide(row, t, j1, j2, a1, a2, xn, k, norms, bounds, ka, kb, labels, dist, fast_err, ka2, kb2,
-                              row_bounds, &theta);
+                              row_bounds, &theta, kr, __fmul_ru(__fsqrt_ru(rs), 1.0000005f));
         redo = !ok;
     }
     certify_tally(ok, redo, row, theta, cert_count, redo_count, redo_rows, redo_theta);

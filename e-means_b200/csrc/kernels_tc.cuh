@@ -19,7 +19,7 @@
 // and stays resident in shared memory for the whole centroid walk.
 //
 // Three-term products (hi*hi + hi*lo + lo*hi, FP32 accumulation) give scores
-// within ~3 2^-18 |x||c| of exact, which certifies nearly every row's top-2; the
+// within ~3 2^-16 |x||c| of exact, which certifies nearly every row's top-2; the
 // exact re-score happens in kernels_exact.cuh.
 #pragma once
 #include <cuda.h>
@@ -51,6 +51,14 @@ constexpr int kTcLoadWarps = 2;
 constexpr int kTcEpi0 = 2 + kTcLoadWarps;
 constexpr int kTcPThreads = 32 * (kTcEpi0 + kTcEpiWarps);
 constexpr int kTcRowScaleSlots = 4;  // FP8 per-row scales, a ring over work items
+// Norms inside the contraction (single-term BF16 search of f32 rows): each tile
+// starts with one K = 16 MMA of a constant row operand [1, 1, 1, 0, ...] against
+// the tile's half-norms split into three BF16 parts, so the accumulator holds
+// norm / 2 - x . c (the rows enter negated), half the score, and the epilogue
+// scores without loading norms or multiplying. A ring of two 8 KB slices.
+constexpr int kTcNmSlots = 2;
+constexpr uint32_t kTcNmSlotBytes = (uint32_t)kTcBN * 32;  // 256 centroids x 16 BF16
+constexpr uint32_t kTcNmConstBytes = (uint32_t)kTcBM * 32;  // 128 rows x 16 BF16
 
 struct TcParams {
     int m, d, k, kpad;   // kpad: d rounded up to 64 (one 128-byte swizzle atom per 64 BF16)
@@ -84,6 +92,9 @@ struct TcParams {
     // centroid; wf8[j] = -2 / (centroid j's scale), 0 past k (score = norm + acc r w).
     const float* wf8;
     int nsplit;  // column splits of the search (work item = row tile x split)
+    // Norms inside the contraction: [tiles * 256][16] BF16, row j = the three BF16
+    // parts of norms[j] / 2, then zeros (k_prep_nrm16).
+    const __nv_bfloat16* nrm16;
 };
 
 // ---- PTX wrappers -----------------------------------------------------------
@@ -187,6 +198,19 @@ EMB_DEV uint64_t sw128_desc(uint32_t saddr) {
     return d;
 }
 
+// Same for a K-major operand of 16 BF16 per row (32-byte rows), 32-byte swizzle:
+// 8-row groups 256 B apart. The swizzle only exchanges the two 16-byte halves of
+// a row, which the norm operands are built to be indifferent to (see kTcNmSlots).
+EMB_DEV uint64_t sw32_desc(uint32_t saddr) {
+    uint64_t d = 0;
+    d |= (uint64_t)((saddr >> 4) & 0x3FFF);        // start address
+    d |= (uint64_t)1 << 16;                         // leading byte offset (unused for swizzled K-major)
+    d |= (uint64_t)(256 >> 4) << 32;                // stride byte offset: 8 rows x 32 B
+    d |= (uint64_t)1 << 46;                         // descriptor version (sm_100)
+    d |= (uint64_t)6 << 61;                         // SWIZZLE_32B
+    return d;
+}
+
 // Instruction descriptor, kind::f16: BF16 x BF16 -> F32, both K-major, M x N.
 __host__ __device__ constexpr uint32_t idesc_bf16(int M, int N) {
     return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
@@ -238,22 +262,27 @@ struct TcLayout {
     uint32_t a_buf;        // bytes of one row-tile buffer (hi, then lo for three terms)
     uint32_t a_lo;         // offset of the lo part inside a buffer
     uint32_t b0, stage_bytes, term_bytes;
-    uint32_t norms, nrm_slot_bytes;  // ring of per-tile norms (FP8: norms, then column factors)
+    uint32_t norms, nrm_slot_bytes;  // ring of per-tile norms (FP8: norms, then column factors;
+                                     // norms in the contraction: kTcNmSlots BF16 slices)
+    uint32_t nconst;       // norms in the contraction: the constant row operand
     uint32_t rscale;       // FP8: ring of per-row scales [kTcRowScaleSlots][128]
     uint32_t merge, bars, pub, total;
     int stages, nbuf;
 };
 
-__host__ __device__ inline TcLayout tc_layout(int kpad, int nterms, bool fp8) {
+// nm: norms inside the contraction (kTcNmSlots), which also needs 512 bytes of
+// barriers instead of 256.
+__host__ __device__ inline TcLayout tc_layout(int kpad, int nterms, bool fp8, bool nm = false) {
     TcLayout s;
     const uint32_t a_term = (uint32_t)kTcBM * (uint32_t)kpad * (fp8 ? 1u : 2u);
     s.a_buf = a_term * ((!fp8 && nterms == 3) ? 2u : 1u);
     s.a_lo = a_term;
     s.term_bytes = (uint32_t)kTcBN * 128;  // one K atom of 256 centroids
     s.stage_bytes = s.term_bytes * ((fp8 || nterms == 1) ? 1u : 2u);
-    s.nrm_slot_bytes = (uint32_t)kTcBN * 4 * (fp8 ? 2u : 1u);
-    const uint32_t fixed = kTcNormSlots * s.nrm_slot_bytes + kTcRowScaleSlots * kTcBM * 4 + 3 * kTcBM * 16 + 256 +
-                           4 * kTcBM * 4 + 1024;
+    s.nrm_slot_bytes = nm ? kTcNmSlotBytes : (uint32_t)kTcBN * 4 * (fp8 ? 2u : 1u);
+    const uint32_t nrm_bytes = nm ? kTcNmSlots * kTcNmSlotBytes + kTcNmConstBytes : kTcNormSlots * s.nrm_slot_bytes;
+    const uint32_t bar_bytes = nm ? 512u : 256u;
+    const uint32_t fixed = nrm_bytes + kTcRowScaleSlots * kTcBM * 4 + 3 * kTcBM * 16 + bar_bytes + 4 * kTcBM * 4 + 1024;
     // Two row-tile buffers (the next tile's rows load while the current one is
     // searched) when they leave room for three stages, else one.
     s.nbuf = 2 * s.a_buf + 3 * s.stage_bytes + fixed <= (uint32_t)kTcSmemLimit ? 2 : 1;
@@ -262,10 +291,11 @@ __host__ __device__ inline TcLayout tc_layout(int kpad, int nterms, bool fp8) {
     s.stages = st;
     s.b0 = s.nbuf * s.a_buf;
     s.norms = s.b0 + st * s.stage_bytes;
-    s.rscale = s.norms + kTcNormSlots * s.nrm_slot_bytes;
+    s.nconst = s.norms + (nm ? kTcNmSlots * kTcNmSlotBytes : 0u);
+    s.rscale = s.norms + nrm_bytes;
     s.merge = s.rscale + kTcRowScaleSlots * kTcBM * 4;
     s.bars = s.merge + 3 * kTcBM * 16;
-    s.pub = s.bars + 256;                  // [4 column quarters][128 rows] published best key
+    s.pub = s.bars + bar_bytes;            // [4 column quarters][128 rows] published best key
     s.total = s.pub + 4 * kTcBM * 4;
     return s;
 }
@@ -288,10 +318,12 @@ EMB_DEV size_t tc_src_row(const TcParams& p, int g) {
 // Row tile -> BF16 hi (and lo for three terms) in the K-major 128B-swizzled layout,
 // by threads tid = 0 .. nthr-1: 128 rows x (kpad / 8) chunks of 8 elements. Each
 // thread issues the loads of up to four chunks before converting any of them, so
-// that the gathered rows' latencies overlap.
+// that the gathered rows' latencies overlap. neg: the rows negated (exact; BF16
+// rounding to nearest is symmetric), for the norms-in-the-contraction search.
 template <typename T>
 EMB_DEV void tc_load_rows(uint8_t* a_hi, uint8_t* a_lo, const T* __restrict__ x, const TcParams& p, int row0, int m,
-                          int tid, int nthr) {
+                          int tid, int nthr, bool neg = false) {
+    const float sg = neg ? -1.0f : 1.0f;
     constexpr int kBatch = 4;
     const int nchunk = p.kpad / 8;
     const int total = kTcBM * nchunk;
@@ -326,9 +358,10 @@ EMB_DEV void tc_load_rows(uint8_t* a_hi, uint8_t* a_lo, const T* __restrict__ x,
             uint32_t hw[4], lw[4];
 #pragma unroll
             for (int i = 0; i < 4; i++) {
-                __nv_bfloat16 h0 = __float2bfloat16_rn(v[u][2 * i]), h1 = __float2bfloat16_rn(v[u][2 * i + 1]);
-                __nv_bfloat16 l0 = __float2bfloat16_rn(v[u][2 * i] - __bfloat162float(h0));
-                __nv_bfloat16 l1 = __float2bfloat16_rn(v[u][2 * i + 1] - __bfloat162float(h1));
+                const float v0 = sg * v[u][2 * i], v1 = sg * v[u][2 * i + 1];
+                __nv_bfloat16 h0 = __float2bfloat16_rn(v0), h1 = __float2bfloat16_rn(v1);
+                __nv_bfloat16 l0 = __float2bfloat16_rn(v0 - __bfloat162float(h0));
+                __nv_bfloat16 l1 = __float2bfloat16_rn(v1 - __bfloat162float(h1));
                 hw[i] = (uint32_t)__bfloat16_as_ushort(h0) | ((uint32_t)__bfloat16_as_ushort(h1) << 16);
                 lw[i] = (uint32_t)__bfloat16_as_ushort(l0) | ((uint32_t)__bfloat16_as_ushort(l1) << 16);
             }
@@ -620,6 +653,29 @@ EMB_DEV void mma_e4m3(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t 
         ::"r"(d_tmem), "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate));
 }
 
+// Norms inside the contraction: row j of `out` (16 BF16) holds the three BF16
+// parts of h = norms[j] / 2 (p1 = bf16(h), p2 = bf16(h - p1), p3 = bf16(h - p1 - p2);
+// both differences are exact in f32 and p3 is exact in BF16, so p1 + p2 + p3 = h
+// for every h in the normal range), then zeros. A non-finite h keeps p1 = h and
+// zeros after it, so the MMA sums the same +-inf or NaN the epilogue's
+// norm - 2 acc would give. Rows up to kp (whole tiles): the padding's 3e38 too.
+__global__ void k_prep_nrm16(const float* __restrict__ norms, int kp, __nv_bfloat16* __restrict__ out) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= kp) return;
+    const float h = 0.5f * norms[j];
+    const __nv_bfloat16 p1 = __float2bfloat16_rn(h);
+    __nv_bfloat16 p2 = __float2bfloat16_rn(0.0f), p3 = p2;
+    if (isfinite(h)) {
+        const float r1 = h - __bfloat162float(p1);
+        p2 = __float2bfloat16_rn(r1);
+        p3 = __float2bfloat16_rn(r1 - __bfloat162float(p2));
+    }
+    uint4* o = reinterpret_cast<uint4*>(out + (size_t)j * 16);
+    o[0] = make_uint4((uint32_t)__bfloat16_as_ushort(p1) | ((uint32_t)__bfloat16_as_ushort(p2) << 16),
+                      (uint32_t)__bfloat16_as_ushort(p3), 0u, 0u);
+    o[1] = make_uint4(0u, 0u, 0u, 0u);
+}
+
 // Scores of 16 accumulator columns (in place): s = norm - 2 acc (BF16), or
 // s = norm + (acc r) w (FP8: acc r undoes the row's power-of-two scale exactly,
 // w = -2 / the centroid's scale), one rounding each.
@@ -706,13 +762,14 @@ struct TcBest {
 // COLLECT = false: per-row (best key, column, lower bound of the rest) to part_s/part_i.
 // COLLECT = true : every centroid with approximate score <= theta[row] is appended
 //                  to cand[row][*] (cand_count[row] counts all, capped storage).
-template <typename T, bool COLLECT, bool FP8>
+template <typename T, bool COLLECT, bool FP8, bool NM = false>
 __global__ void __launch_bounds__(kTcPThreads, 1)
 k_assign_tc(const T* __restrict__ x, const __grid_constant__ CUtensorMap map_hi,
             const __grid_constant__ CUtensorMap map_lo, const TcParams p) {
+    static_assert(!NM || (!COLLECT && !FP8), "norms in the contraction: single-term BF16 fast search only");
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     uint8_t* smem = smem_align1024(smem_raw);
-    const TcLayout L = tc_layout(p.kpad, p.nterms, FP8);
+    const TcLayout L = tc_layout(p.kpad, p.nterms, FP8, NM);
     const int S = L.stages, NB = L.nbuf;
     uint64_t* full = (uint64_t*)(smem + L.bars);          // [kTcMaxStages]
     uint64_t* empty = full + kTcMaxStages;                // [kTcMaxStages]
@@ -724,7 +781,10 @@ k_assign_tc(const T* __restrict__ x, const __grid_constant__ CUtensorMap map_hi,
     uint64_t* rs_full = a_empty + 2;                      // [kTcRowScaleSlots] FP8 row scales written
     uint64_t* mma_done = rs_full + kTcRowScaleSlots;      // every issued MMA completed (teardown)
     uint64_t* stall_bar = mma_done + 1;                   // never completed (abort-path test)
-    uint32_t* tmem_slot = (uint32_t*)(stall_bar + 1);     // 30 barriers: 240 of the 256 bytes
+    uint64_t* nm_full = stall_bar + 1;                    // NM: [kTcNmSlots] norm slice loaded
+    uint64_t* nm_empty = nm_full + kTcNmSlots;            // NM: [kTcNmSlots] the MMA reading it completed
+    // 30 barriers: 240 of the 256 bytes; with NM 34 barriers: 272 of 512 bytes.
+    uint32_t* tmem_slot = (uint32_t*)(NM ? nm_empty + kTcNmSlots : stall_bar + 1);
     volatile int* abort_flag = (volatile int*)(tmem_slot + 1);
     float* norms_s = (float*)(smem + L.norms);
     float* rscale_s = (float*)(smem + L.rscale);
@@ -760,6 +820,12 @@ k_assign_tc(const T* __restrict__ x, const __grid_constant__ CUtensorMap map_hi,
         for (int i = 0; i < kTcRowScaleSlots; i++) mbar_init(&rs_full[i], kTcLoadWarps * 32);
         mbar_init(mma_done, 1);
         mbar_init(stall_bar, 1);
+        if (NM) {
+            for (int i = 0; i < kTcNmSlots; i++) {
+                mbar_init(&nm_full[i], 1);
+                mbar_init(&nm_empty[i], 1);
+            }
+        }
         *abort_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
@@ -767,6 +833,15 @@ k_assign_tc(const T* __restrict__ x, const __grid_constant__ CUtensorMap map_hi,
     {  // published best keys start at +inf
         float* pub = (float*)(smem + L.pub);
         for (int i = threadIdx.x; i < 4 * kTcBM; i += blockDim.x) pub[i] = INFINITY;
+    }
+    if (NM) {
+        // The constant row operand of the norm MMA: every row [1, 1, 1, 0, 0, 0, 0, 0]
+        // in both 16-byte halves (BF16 one = 0x3F80), so whichever half the 32-byte
+        // swizzle pairs with the norm slice's parts, the product is p1 + p2 + p3.
+        uint4* nc = reinterpret_cast<uint4*>(smem + L.nconst);
+        for (int i = threadIdx.x; i < (int)(kTcNmConstBytes / 16); i += blockDim.x)
+            nc[i] = make_uint4(0x3F803F80u, 0x00003F80u, 0u, 0u);
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // visible to the tensor cores
     }
     tc_fence_before();
     __syncthreads();
@@ -789,16 +864,32 @@ k_assign_tc(const T* __restrict__ x, const __grid_constant__ CUtensorMap map_hi,
                             ok = false;
                             break;
                         }
+                        // NM: the tile's norm slice goes into slot tg % kTcNmSlots once the
+                        // MMA of tile tg - kTcNmSlots has read it (waited before any copy
+                        // of this unit is issued, so an abort here leaves none untracked).
+                        if (NM && a == 0 && tg >= kTcNmSlots &&
+                            !mbar_wait(&nm_empty[tg % kTcNmSlots], ((uint32_t)(tg / kTcNmSlots) & 1u) ^ 1u, abort_flag,
+                                       kTcCtlSleepNs)) {
+                            ok = false;
+                            break;
+                        }
                         uint8_t* stage = smem + L.b0 + s * L.stage_bytes;
                         mbar_expect_tx(&full[s], L.stage_bytes);
                         tma_load_2d(stage, &map_hi, &full[s], a * (FP8 ? 128 : 64), col);
                         if (!FP8 && p.nterms > 1) tma_load_2d(stage + L.term_bytes, &map_lo, &full[s], a * 64, col);
                         if (a == 0) {
-                            const int ns = tg % kTcNormSlots;
-                            float* dst = norms_s + ns * (L.nrm_slot_bytes / 4);
-                            mbar_expect_tx(&norms_full[ns], L.nrm_slot_bytes);
-                            bulk_load(dst, p.norms + (size_t)col, kTcBN * 4, &norms_full[ns]);
-                            if (FP8) bulk_load(dst + kTcBN, p.wf8 + (size_t)col, kTcBN * 4, &norms_full[ns]);
+                            if (NM) {
+                                const int ns = tg % kTcNmSlots;
+                                mbar_expect_tx(&nm_full[ns], kTcNmSlotBytes);
+                                bulk_load(smem + L.norms + ns * kTcNmSlotBytes, p.nrm16 + (size_t)col * 16,
+                                          kTcNmSlotBytes, &nm_full[ns]);
+                            } else {
+                                const int ns = tg % kTcNormSlots;
+                                float* dst = norms_s + ns * (L.nrm_slot_bytes / 4);
+                                mbar_expect_tx(&norms_full[ns], L.nrm_slot_bytes);
+                                bulk_load(dst, p.norms + (size_t)col, kTcBN * 4, &norms_full[ns]);
+                                if (FP8) bulk_load(dst + kTcBN, p.wf8 + (size_t)col, kTcBN * 4, &norms_full[ns]);
+                            }
                             nissued = tg + 1;
                         }
                     }
@@ -808,8 +899,10 @@ k_assign_tc(const T* __restrict__ x, const __grid_constant__ CUtensorMap map_hi,
             // exits; bounded like every wait.
             if (*abort_flag) {
                 for (int v = u > S ? u - S : 0; v < u; v++) mbar_drain(&full[v % S], (uint32_t)(v / S) & 1u);
-                for (int t = nissued > kTcNormSlots ? nissued - kTcNormSlots : 0; t < nissued; t++)
-                    mbar_drain(&norms_full[t % kTcNormSlots], (uint32_t)(t / kTcNormSlots) & 1u);
+                const int nslots = NM ? kTcNmSlots : kTcNormSlots;
+                uint64_t* nbar = NM ? nm_full : norms_full;
+                for (int t = nissued > nslots ? nissued - nslots : 0; t < nissued; t++)
+                    mbar_drain(&nbar[t % nslots], (uint32_t)(t / nslots) & 1u);
             }
         }
     } else if (warp == 1) {
@@ -829,12 +922,18 @@ k_assign_tc(const T* __restrict__ x, const __grid_constant__ CUtensorMap map_hi,
                 const uint64_t a_lo0 = sw128_desc(smem_u32(smem + ab * L.a_buf + L.a_lo));
                 for (int t = 0; t < nt && ok; t++, tg++) {
                     const int b = tg & 1;
-                    if (!mbar_wait(&acc_empty[b], ((uint32_t)(tg >> 1) & 1u) ^ 1u, abort_flag, kTcCtlSleepNs)) {
+                    if (!mbar_wait(&acc_empty[b], ((uint32_t)(tg >> 1) & 1u) ^ 1u, abort_flag, kTcCtlSleepNs) ||
+                        (NM && !mbar_wait(&nm_full[tg % kTcNmSlots], (uint32_t)(tg / kTcNmSlots) & 1u, abort_flag,
+                                          kTcCtlSleepNs))) {
                         ok = false;
                         break;
                     }
                     tc_fence_after();
                     const uint32_t d_tmem = tmem_base + (uint32_t)(b * kTcBN);
+                    // NM: the accumulator starts as the half-norms (one K = 16 MMA).
+                    if (NM)
+                        mma_bf16(d_tmem, sw32_desc(smem_u32(smem + L.nconst)),
+                                 sw32_desc(smem_u32(smem + L.norms + (tg % kTcNmSlots) * kTcNmSlotBytes)), idesc, 0u);
                     for (int a = 0; a < natoms; a++, u++) {
                         const int s = u % S;
                         if (!mbar_wait(&full[s], (uint32_t)(u / S) & 1u, abort_flag, kTcCtlSleepNs)) {
@@ -847,7 +946,7 @@ k_assign_tc(const T* __restrict__ x, const __grid_constant__ CUtensorMap map_hi,
                         const uint64_t ah = a_hi0 + (uint64_t)(a * a_atom), al = a_lo0 + (uint64_t)(a * a_atom);
 #pragma unroll
                         for (int kk = 0; kk < 4; kk++) {  // 32 bytes of K per MMA = 2 descriptor units
-                            const uint32_t acc = (a > 0 || kk > 0) ? 1u : 0u;
+                            const uint32_t acc = (NM || a > 0 || kk > 0) ? 1u : 0u;
                             if (FP8) mma_e4m3(d_tmem, ah + 2 * kk, bh + 2 * kk, idesc, acc);
                             else mma_bf16(d_tmem, ah + 2 * kk, bh + 2 * kk, idesc, acc);
                         }
@@ -861,7 +960,10 @@ k_assign_tc(const T* __restrict__ x, const __grid_constant__ CUtensorMap map_hi,
                         }
                         mma_commit(&empty[s]);
                     }
-                    if (ok) mma_commit(&acc_full[b]);
+                    if (ok) {
+                        if (NM) mma_commit(&nm_empty[tg % kTcNmSlots]);
+                        mma_commit(&acc_full[b]);
+                    }
                 }
                 if (ok) mma_commit(&a_empty[ab]);  // the row buffer is free once these MMAs complete
             }
@@ -881,7 +983,7 @@ k_assign_tc(const T* __restrict__ x, const __grid_constant__ CUtensorMap map_hi,
             if (FP8)
                 tc_load_rows_fp8(a, rscale_s + (i % kTcRowScaleSlots) * kTcBM, x, p, (w / nsplit) * kTcBM, m, ltid);
             else
-                tc_load_rows(a, a + L.a_lo, x, p, (w / nsplit) * kTcBM, m, ltid, kTcLoadWarps * 32);
+                tc_load_rows(a, a + L.a_lo, x, p, (w / nsplit) * kTcBM, m, ltid, kTcLoadWarps * 32, NM);
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // visible to the tensor cores
             mbar_arrive(&a_full[ab]);
             // The epilogue reads slot i % 4 of the row scales at item i. The loader
@@ -910,7 +1012,7 @@ k_assign_tc(const T* __restrict__ x, const __grid_constant__ CUtensorMap map_hi,
             for (int t = 0; t < nt && ok; t++, tg++) {
                 const int b = tg & 1;
                 if (!mbar_wait(&acc_full[b], (uint32_t)(tg >> 1) & 1u, abort_flag, 20000) ||
-                    !mbar_wait(&norms_full[tg % kTcNormSlots], (uint32_t)(tg / kTcNormSlots) & 1u, abort_flag) ||
+                    (!NM && !mbar_wait(&norms_full[tg % kTcNormSlots], (uint32_t)(tg / kTcNormSlots) & 1u, abort_flag)) ||
                     (p.stall_ns && t == p.stall_tile && warp == kTcEpi0 &&
                      !mbar_wait(stall_bar, 0, abort_flag, 0, p.stall_ns))) {
                     ok = false;
@@ -948,7 +1050,14 @@ k_assign_tc(const T* __restrict__ x, const __grid_constant__ CUtensorMap map_hi,
                 float sc4[4][16], mnh[4];
 #pragma unroll
                 for (int h = 0; h < 4; h++) {
-                    tc_scores16<FP8>(v4[h], nrm + h * 16, nrm + kTcBN + h * 16, rs, sc4[h]);
+                    if constexpr (NM) {
+                        // The accumulator is the half-score: keys and bounds stay in those
+                        // units (every comparison is scale-free) until they are written.
+#pragma unroll
+                        for (int j = 0; j < 16; j++) sc4[h][j] = __uint_as_float(v4[h][j]);
+                    } else {
+                        tc_scores16<FP8>(v4[h], nrm + h * 16, nrm + kTcBN + h * 16, rs, sc4[h]);
+                    }
                     mnh[h] = tc_min16s(sc4[h]);
                 }
                 if (!COLLECT) {
@@ -1033,9 +1142,10 @@ k_assign_tc(const T* __restrict__ x, const __grid_constant__ CUtensorMap map_hi,
                     // the final best key); were it ever violated, raising s2 to s1
                     // leaves no margin, so the row goes to the refine pass.
                     const size_t oo = ((size_t)split * p.m + row) * 2;
-                    p.part_s[oo] = s1;
+                    const float unit = NM ? 2.0f : 1.0f;  // NM: half-scores back to scores (exact)
+                    p.part_s[oo] = unit * s1;
                     p.part_i[oo] = i1;
-                    p.part_s[oo + 1] = fmaxf(s2, s1);
+                    p.part_s[oo + 1] = unit * fmaxf(s2, s1);
                     p.part_i[oo + 1] = i1;
                 }
                 pub[cq * kTcBM + r] = INFINITY;  // the next item starts afresh

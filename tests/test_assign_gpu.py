@@ -135,6 +135,31 @@ def test_ties_go_to_lowest_index(orc, assigners, precision):
     assert np.all(lab < 40)
 
 
+@pytest.mark.parametrize("precision", PRECISIONS)
+def test_adversarial_bf16_rounding(orc, assigners, precision):
+    # Every element of the rows and of centroid 1 is 1 + 2^-8 - 2^-12, which BF16
+    # rounds down to 1 with a relative error of almost 2^-8 (its unit roundoff);
+    # centroid 0 is all ones, exact in BF16. Centroid 1 is the reference's label
+    # (by d e^2, e the excess over 1), yet the single-term BF16 scores put centroid
+    # 0 ahead by about 4 d e: a bound that took the unit roundoff for 2^-9 would
+    # certify the wrong label. The other centroids have small norms (so the bound's
+    # max |c| is the two close ones') and scores far above theirs.
+    d = 128
+    e = np.float32(2.0 ** -8 - 2.0 ** -12)
+    v = np.float32(1.0) + e
+    rng = np.random.default_rng(8)
+    x = np.full((512, d), v, dtype=np.float32)
+    x[256:] += rng.integers(0, 4, (256, d)).astype(np.float32) * np.float32(2.0 ** -20)  # still rounds down
+    far = rng.standard_normal((62, d)).astype(np.float32) * np.float32(0.01) - np.float32(0.05)  # small norms
+    c = np.concatenate([np.ones((1, d), np.float32), np.full((1, d), v, np.float32), far])
+    a = assigners(precision)
+    a.set_centroids(c)
+    lab, dist = a.assign(x)
+    ref_l, ref_d = orc.cpu_assign(x, c, emulate=True)
+    assert np.all(ref_l == 1)
+    assert np.array_equal(lab, ref_l) and same_f32(dist, ref_d)
+
+
 def test_edge_cases(orc, assigners):
     a = assigners("fp32")
     # k = 1, d = 1
