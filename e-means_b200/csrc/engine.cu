@@ -265,7 +265,7 @@ size_t elt_size(int dtype) { return dtype == EMB200_F32 ? 4 : 1; }
 // kr (single-term BF16, when the caller asks for it): the operands' rounding is
 // bounded per row instead, by kr (xr cmax + (|x| + xr) dmax) with xr = |x - bf16(x)|
 // of the row and dmax >= max_j |c_j - bf16(c_j)| (exact identity plus Cauchy-Schwarz,
-// in score units, times the same 1.25 margin), and leaves ka.
+// in score units), and leaves ka.
 void bound_coefficients(int precision, int dtype, size_t d, bool packed, float* ka, float* kb, bool norm_mma = false,
                         float* kr = nullptr) {
     if (kr) *kr = 0.0f;
@@ -290,8 +290,10 @@ void bound_coefficients(int precision, int dtype, size_t d, bool packed, float* 
     } else {
         double rep = dtype == EMB200_F32 ? 2.0 * ub + ub * ub : ub;
         if (kr) {
+            // The identity is exact and the norms it uses are rounded up; the
+            // 2^-10 margin covers |x| from the reference's rounded sqnorm.
             rep = 0.0;
-            *kr = 1.25f * 2.0f;
+            *kr = 2.0f * (1.0f + 0x1p-10f);
         }
         a = 2.0 * (rep + 1.02 * gamma((double)d + (norm_mma ? 5 : 2), 2 * u) + g_ref) + 4.02 * u;
     }
