@@ -985,7 +985,7 @@ def main():
                     help="C4: time the lockstep calls only (no streams-mode or sequential comparison)")
     ap.add_argument("--late-epochs", type=int, default=1,
                     help="C5: last epochs of the proposer-in-training run searched through the proposer")
-    ap.add_argument("--late-net-steps", type=int, default=1000,
+    ap.add_argument("--late-net-steps", type=int, default=500,
                     help="c5: Adam steps of the network fitted inside the proposed training run")
     ap.add_argument("--proposer-training", type=int, default=1,
                     help="c5: also train with the proposer in the last epoch (1) or not (0)")

@@ -621,7 +621,8 @@ int launch_tc_kernel(emb200_handle* h, const T* x, const TcParams& p, int nsplit
 template <typename T, bool COLLECT>
 int launch_tc(emb200_handle* h, const T* x, const uint32_t* gather, const uint32_t* gather2, size_t m, int nterms,
               const float* theta, uint32_t* cand, uint32_t* cand_count, int cap, int* err, cudaStream_t st,
-              const uint32_t* m_dev = nullptr, int nsplit_override = 0, bool fp8 = false) {
+              const uint32_t* m_dev = nullptr, int nsplit_override = 0, bool fp8 = false,
+              const TcParams* fuse = nullptr, bool* fused = nullptr) {
     TcParams p{};
     p.m = (int)m;
     p.d = (int)h->d;
@@ -656,6 +657,23 @@ int launch_tc(emb200_handle* h, const T* x, const uint32_t* gather, const uint32
             k_prep_nrm16<<<(unsigned)((kp + 255) / 256), 256, 0, st>>>(h->norms.p, (int)kp, h->nrm16.p);
             CKL();
             p.nrm16 = h->nrm16.p;
+            if (fuse && nsplit == 1) {  // certification at the end of each item
+                p.fuse = 1;
+                p.cx = fuse->cx;
+                p.bounds = fuse->bounds;
+                p.ka = fuse->ka;
+                p.kb = fuse->kb;
+                p.kr = fuse->kr;
+                p.ka2 = fuse->ka2;
+                p.kb2 = fuse->kb2;
+                p.labels = fuse->labels;
+                p.dist = fuse->dist;
+                p.redo_rows = fuse->redo_rows;
+                p.redo_theta = fuse->redo_theta;
+                p.redo_count = fuse->redo_count;
+                p.cert_count = fuse->cert_count;
+                if (fused) *fused = true;
+            }
             return launch_tc_kernel<T, false, false, true>(h, x, p, nsplit, st);
         }
     }
@@ -686,7 +704,7 @@ int finish_counters(emb200_handle* h, cudaStream_t st, bool refined) {
 template <typename T>
 int settle_rows(emb200_handle* h, const T* x, const uint32_t* gather, size_t m, uint32_t* labels, float* dist,
                 cudaStream_t st, bool graph, int nsplit, int fast_prec, bool tc,
-                const float2* row_bounds = nullptr);
+                const float2* row_bounds = nullptr, bool certified = false);
 
 template <typename T>
 int assign_rows_dev(emb200_handle* h, const T* x, const uint32_t* gather, size_t m, uint32_t* labels, float* dist,
@@ -755,9 +773,31 @@ int assign_rows_dev(emb200_handle* h, const T* x, const uint32_t* gather, size_t
     CK(cudaMemsetAsync(ctr, 0, 8 * sizeof(uint32_t), st));
     h->stats.fast_kernel = fp8 ? 4 : tc ? 1 : 0;
     if (!graph) CK(cudaEventRecord(h->evk0, st));
+    bool fused = false;
     if (tc) {
+        // Single-term search of aligned f32 rows in the AVX-512 rounding: the fast
+        // kernel certifies each row tile itself (when it also sums the norms in its
+        // contraction and searches all columns in one split).
+        TcParams fz{};
+        const TcParams* fzp = nullptr;
+        if constexpr (std::is_same<T, float>::value) {
+            if (!fp8 && fast_terms == 1 && h->opts.match_kernel == kMatchAvx512 && d % 16 == 0 &&
+                ((uintptr_t)x & 15) == 0 && ((uintptr_t)h->c.p & 15) == 0) {
+                bound_coefficients(prec, dtype, h->d, true, &fz.ka, &fz.kb, prec == EMB200_PREC_BF16X1, &fz.kr);
+                bound_coefficients(EMB200_PREC_BF16, dtype, h->d, false, &fz.ka2, &fz.kb2);
+                fz.cx = h->c.p;
+                fz.bounds = h->bounds.p;
+                fz.labels = labels;
+                fz.dist = dist;
+                fz.redo_rows = h->redo_rows.p;
+                fz.redo_theta = h->redo_theta.p;
+                fz.redo_count = ctr;
+                fz.cert_count = ctr + 1;
+                fzp = &fz;
+            }
+        }
         int rc = launch_tc<T, false>(h, x, gather, nullptr, m, fast_terms, nullptr, nullptr, nullptr, 0,
-                                     (int*)(ctr + 2), st, nullptr, 0, fp8);
+                                     (int*)(ctr + 2), st, nullptr, 0, fp8, fzp, &fused);
         if (rc) return rc;
     } else {
         dim3 grid(row_tiles, nsplit);
@@ -767,7 +807,8 @@ int assign_rows_dev(emb200_handle* h, const T* x, const uint32_t* gather, size_t
         CKL();
     }
     if (!graph) CK(cudaEventRecord(h->evk1, st));
-    return settle_rows(h, x, gather, m, labels, dist, st, graph, nsplit, tc ? prec : EMB200_PREC_FP32, tc);
+    return settle_rows(h, x, gather, m, labels, dist, st, graph, nsplit, tc ? prec : EMB200_PREC_FP32, tc, nullptr,
+                       fused);
 }
 
 // Exhaustive exact search of the rows listed in rows[0 .. *count) (count on the
@@ -795,7 +836,8 @@ int launch_research(emb200_handle* h, const T* x, const uint32_t* gather, size_t
 // the fast kernel (which may have set the abort flag, counter 2).
 template <typename T>
 int settle_rows(emb200_handle* h, const T* x, const uint32_t* gather, size_t m, uint32_t* labels, float* dist,
-                cudaStream_t st, bool graph, int nsplit, int fast_prec, bool tc, const float2* row_bounds) {
+                cudaStream_t st, bool graph, int nsplit, int fast_prec, bool tc, const float2* row_bounds,
+                bool certified) {
     const int dtype = std::is_same<T, float>::value ? EMB200_F32 : (std::is_same<T, int8_t>::value ? EMB200_I8 : EMB200_U8);
     const int k = (int)h->k, d = (int)h->d;
     const int refine_terms = tc_terms(EMB200_PREC_BF16, dtype);
@@ -810,7 +852,9 @@ int settle_rows(emb200_handle* h, const T* x, const uint32_t* gather, size_t m, 
     bool vec4 = false;
     if constexpr (std::is_same<T, float>::value)
         vec4 = d % 16 == 0 && ((uintptr_t)x & 15) == 0 && ((uintptr_t)h->c.p & 15) == 0;
-    if (match == kMatchAvx512 && vec4) {
+    if (certified) {
+        // the fast kernel certified its rows itself (TcParams::fuse)
+    } else if (match == kMatchAvx512 && vec4) {
         k_certify16v<<<(unsigned)((m + 63) / 64), 256, 0, st>>>(
             (const float*)x, gather, (int)m, d, h->c.p, h->norms.p, k, h->part_s.p, h->part_i.p, nsplit, h->bounds.p,
             ka, kb, labels, dist, h->redo_rows.p, ctr, ctr + 1, tc ? (const int*)(ctr + 2) : nullptr, h->redo_theta.p,

@@ -26,6 +26,7 @@
 #include <cuda_bf16.h>
 
 #include "common.cuh"
+#include "kernels_exact.cuh"
 
 namespace emb {
 
@@ -95,6 +96,20 @@ struct TcParams {
     // Norms inside the contraction: [tiles * 256][16] BF16, row j = the three BF16
     // parts of norms[j] / 2, then zeros (k_prep_nrm16).
     const __nv_bfloat16* nrm16;
+    // Certification at the end of each work item (norms inside the contraction,
+    // one column split, f32 rows with d % 16 == 0 and 16-byte aligned rows and
+    // centroids, AVX-512 rounding): the decisions of k_certify16v, taken by the
+    // epilogue warps from the row tile's merged top-2, in place of that kernel.
+    int fuse;
+    const float* cx;  // f32 centroids [k][d]
+    const Bounds* bounds;
+    float ka, kb, kr, ka2, kb2;
+    uint32_t* labels;
+    float* dist;
+    uint32_t* redo_rows;
+    float* redo_theta;
+    uint32_t* redo_count;
+    uint32_t* cert_count;
 };
 
 // ---- PTX wrappers -----------------------------------------------------------
@@ -265,6 +280,7 @@ struct TcLayout {
     uint32_t norms, nrm_slot_bytes;  // ring of per-tile norms (FP8: norms, then column factors;
                                      // norms in the contraction: kTcNmSlots BF16 slices)
     uint32_t nconst;       // norms in the contraction: the constant row operand
+    uint32_t fin;          // norms in the contraction: an item's merged top-2 for the certification
     uint32_t rscale;       // FP8: ring of per-row scales [kTcRowScaleSlots][128]
     uint32_t merge, bars, pub, total;
     int stages, nbuf;
@@ -280,7 +296,8 @@ __host__ __device__ inline TcLayout tc_layout(int kpad, int nterms, bool fp8, bo
     s.term_bytes = (uint32_t)kTcBN * 128;  // one K atom of 256 centroids
     s.stage_bytes = s.term_bytes * ((fp8 || nterms == 1) ? 1u : 2u);
     s.nrm_slot_bytes = nm ? kTcNmSlotBytes : (uint32_t)kTcBN * 4 * (fp8 ? 2u : 1u);
-    const uint32_t nrm_bytes = nm ? kTcNmSlots * kTcNmSlotBytes + kTcNmConstBytes : kTcNormSlots * s.nrm_slot_bytes;
+    const uint32_t nrm_bytes =
+        nm ? kTcNmSlots * kTcNmSlotBytes + kTcNmConstBytes + kTcBM * 16 : kTcNormSlots * s.nrm_slot_bytes;
     const uint32_t bar_bytes = nm ? 512u : 256u;
     const uint32_t fixed = nrm_bytes + kTcRowScaleSlots * kTcBM * 4 + 3 * kTcBM * 16 + bar_bytes + 4 * kTcBM * 4 + 1024;
     // Two row-tile buffers (the next tile's rows load while the current one is
@@ -292,6 +309,7 @@ __host__ __device__ inline TcLayout tc_layout(int kpad, int nterms, bool fp8, bo
     s.b0 = s.nbuf * s.a_buf;
     s.norms = s.b0 + st * s.stage_bytes;
     s.nconst = s.norms + (nm ? kTcNmSlots * kTcNmSlotBytes : 0u);
+    s.fin = s.nconst + (nm ? kTcNmConstBytes : 0u);
     s.rscale = s.norms + nrm_bytes;
     s.merge = s.rscale + kTcRowScaleSlots * kTcBM * 4;
     s.bars = s.merge + 3 * kTcBM * 16;
@@ -762,6 +780,76 @@ struct TcBest {
 // COLLECT = false: per-row (best key, column, lower bound of the rest) to part_s/part_i.
 // COLLECT = true : every centroid with approximate score <= theta[row] is appended
 //                  to cand[row][*] (cand_count[row] counts all, capped storage).
+// Certification of one work item's 128 rows by the two row-loader warps, 16 rows
+// at a time with four threads per row (k_certify16v's decisions, so every value
+// has the same bits). fin[r]: the row's merged (best key, column, bound of the
+// rest) as scores. valid = false (the item's results never completed: the CTA
+// gave up): every row is listed for the exhaustive search instead. valid must
+// be the same across each warp.
+EMB_DEV void tc_fused_certify(const TcParams& p, const float* __restrict__ x, const uint32_t* __restrict__ fin,
+                              int row0, int m, bool valid) {
+    const int lt = (int)threadIdx.x - 32 * (kTcEpi0 - kTcLoadWarps);  // 0 .. 63
+    const int q = lt & 3, lane = (int)threadIdx.x & 31;
+    const int d = p.d, k = p.k;
+    for (int r0 = 0; r0 < kTcBM; r0 += 8 * kTcLoadWarps) {
+        const int r = r0 + (lt >> 2);
+        const int row = row0 + r;
+        const bool live = row < m;
+        bool ok = false, redo = false;
+        float theta = __int_as_float(0x7fc00000);
+        if (valid) {
+            const int rr = live ? row : m - 1;  // dead rows mirror a live one and write nothing
+            Top2 t;
+            t.init();
+            if (live) {
+                const uint32_t* e = fin + r * 4;
+                t.push(__uint_as_float(e[0]), e[1]);
+                t.push(__uint_as_float(e[2]), e[1]);
+            }
+            const uint32_t j1 = t.i1 < (uint32_t)k ? t.i1 : 0u;
+            const float* xr = x + tc_src_row(p, rr) * (size_t)d;
+            const float* c1 = p.cx + (size_t)j1 * d;
+            float sq[4] = {0.0f, 0.0f, 0.0f, 0.0f}, p1[4] = {0.0f, 0.0f, 0.0f, 0.0f}, rs = 0.0f;
+            for (int i = 4 * q; i < d; i += 16) {
+                const float4 xv = *reinterpret_cast<const float4*>(xr + i);
+                const float4 u = *reinterpret_cast<const float4*>(c1 + i);
+                const float xs[4] = {xv.x, xv.y, xv.z, xv.w}, us[4] = {u.x, u.y, u.z, u.w};
+#pragma unroll
+                for (int j = 0; j < 4; j++) {
+                    sq[j] = __fadd_rn(sq[j], __fmul_rn(xs[j], xs[j]));
+                    p1[j] = __fmaf_rn(xs[j], us[j], p1[j]);
+                    rs = bf16_resid_sq(xs[j], rs);
+                }
+            }
+            rs = __fadd_ru(rs, __shfl_xor_sync(kFull, rs, 2));
+            rs = __fadd_ru(rs, __shfl_xor_sync(kFull, rs, 1));
+#pragma unroll
+            for (int j = 0; j < 4; j++) p1[j] = __fadd_rn(p1[j], __shfl_xor_sync(kFull, p1[j], 2));
+#pragma unroll
+            for (int j = 0; j < 4; j++) p1[j] = __fadd_rn(p1[j], __shfl_xor_sync(kFull, p1[j], 1));
+            const float a1 = __fadd_rn(__fadd_rn(p1[0], p1[2]), __fadd_rn(p1[1], p1[3]));
+            float xn = -0.0f;
+            const int base = lane & ~3;
+#pragma unroll
+            for (int qq = 0; qq < 4; qq++)
+#pragma unroll
+                for (int j = 0; j < 4; j++) xn = __fadd_rn(xn, __shfl_sync(kFull, sq[j], base + qq));
+            if (live && q == 0) {
+                // The second candidate is the first's column again (the written
+                // pair), so one exact dot product serves both.
+                const int no_abort = 0;
+                ok = certify_decide(row, t, j1, j1, a1, a1, xn, k, p.norms, p.bounds, p.ka, p.kb, p.labels, p.dist,
+                                    &no_abort, p.ka2, p.kb2, nullptr, &theta, p.kr,
+                                    __fmul_ru(__fsqrt_ru(rs), 1.0000005f));
+                redo = !ok;
+            }
+        } else {
+            redo = live && q == 0;
+        }
+        certify_tally(ok, redo, row, theta, p.cert_count, p.redo_count, p.redo_rows, p.redo_theta);
+    }
+}
+
 template <typename T, bool COLLECT, bool FP8, bool NM = false>
 __global__ void __launch_bounds__(kTcPThreads, 1)
 k_assign_tc(const T* __restrict__ x, const __grid_constant__ CUtensorMap map_hi,
@@ -783,8 +871,11 @@ k_assign_tc(const T* __restrict__ x, const __grid_constant__ CUtensorMap map_hi,
     uint64_t* stall_bar = mma_done + 1;                   // never completed (abort-path test)
     uint64_t* nm_full = stall_bar + 1;                    // NM: [kTcNmSlots] norm slice loaded
     uint64_t* nm_empty = nm_full + kTcNmSlots;            // NM: [kTcNmSlots] the MMA reading it completed
-    // 30 barriers: 240 of the 256 bytes; with NM 34 barriers: 272 of 512 bytes.
-    uint32_t* tmem_slot = (uint32_t*)(NM ? nm_empty + kTcNmSlots : stall_bar + 1);
+    uint64_t* fin_full = nm_empty + kTcNmSlots;           // NM: an item's merged top-2 written (fused certify)
+    uint64_t* fin_empty = fin_full + 1;                   // NM: the row loaders are done with it
+    // 30 barriers: 240 of the 256 bytes; with NM 36 barriers: 288 of 512 bytes.
+    uint32_t* tmem_slot = (uint32_t*)(NM ? fin_empty + 1 : stall_bar + 1);
+    uint32_t* fin = (uint32_t*)(smem + L.fin);            // NM: [128 rows][4]
     volatile int* abort_flag = (volatile int*)(tmem_slot + 1);
     float* norms_s = (float*)(smem + L.norms);
     float* rscale_s = (float*)(smem + L.rscale);
@@ -825,6 +916,8 @@ k_assign_tc(const T* __restrict__ x, const __grid_constant__ CUtensorMap map_hi,
                 mbar_init(&nm_full[i], 1);
                 mbar_init(&nm_empty[i], 1);
             }
+            mbar_init(fin_full, 1);
+            mbar_init(fin_empty, kTcLoadWarps * 32);
         }
         *abort_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -975,22 +1068,48 @@ k_assign_tc(const T* __restrict__ x, const __grid_constant__ CUtensorMap map_hi,
         // ---- row loaders: item i's row tile into buffer i % NB once the MMAs of
         // item i - NB have completed
         const int ltid = threadIdx.x - 64;
+        // Fused certification (NM, TcParams::fuse): after loading item i's rows the
+        // loaders certify item i - 1 (its merged top-2 is complete once the
+        // epilogue finishes that item, while item i is searched), and the last item
+        // after the loop. After an abort they load nothing more, but still list the
+        // rows of every item whose results never completed for the exact search.
+        // Once a wait has failed, no later item counts as complete either (its
+        // barrier phases no longer line up with the items).
+        const bool fuse = NM && p.fuse;
+        bool fin_ok = true;
+        auto certify_item = [&](int j) {
+            bool valid = fin_ok && mbar_wait(fin_full, (uint32_t)(j & 1), abort_flag, kTcCtlSleepNs);
+            valid = __all_sync(0xffffffffu, valid);
+            fin_ok = valid;
+            if constexpr (std::is_same<T, float>::value)
+                tc_fused_certify(p, x, fin, (item_of(j) / nsplit) * kTcBM, m, valid);
+            mbar_arrive(fin_empty);
+        };
+        bool loading = true;
         for (int i = 0; i < my_items; i++) {
             const int w = item_of(i);
             const int ab = i % NB;
-            if (!mbar_wait(&a_empty[ab], ((uint32_t)(i / NB) & 1u) ^ 1u, abort_flag, kTcCtlSleepNs)) break;
-            uint8_t* a = smem + ab * L.a_buf;
-            if (FP8)
-                tc_load_rows_fp8(a, rscale_s + (i % kTcRowScaleSlots) * kTcBM, x, p, (w / nsplit) * kTcBM, m, ltid);
-            else
-                tc_load_rows(a, a + L.a_lo, x, p, (w / nsplit) * kTcBM, m, ltid, kTcLoadWarps * 32, NM);
-            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // visible to the tensor cores
-            mbar_arrive(&a_full[ab]);
-            // The epilogue reads slot i % 4 of the row scales at item i. The loader
-            // cannot be four items ahead of it: item i + 4 needs the MMAs of item
-            // i + 2 done, which need the epilogue to have released tiles of item i.
-            if (FP8) mbar_arrive(&rs_full[i % kTcRowScaleSlots]);
+            if (loading && !mbar_wait(&a_empty[ab], ((uint32_t)(i / NB) & 1u) ^ 1u, abort_flag, kTcCtlSleepNs))
+                loading = false;
+            if (loading) {
+                uint8_t* a = smem + ab * L.a_buf;
+                if (FP8)
+                    tc_load_rows_fp8(a, rscale_s + (i % kTcRowScaleSlots) * kTcBM, x, p, (w / nsplit) * kTcBM, m,
+                                     ltid);
+                else
+                    tc_load_rows(a, a + L.a_lo, x, p, (w / nsplit) * kTcBM, m, ltid, kTcLoadWarps * 32, NM);
+                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // visible to the tensor cores
+                mbar_arrive(&a_full[ab]);
+                // The epilogue reads slot i % 4 of the row scales at item i. The loader
+                // cannot be four items ahead of it: item i + 4 needs the MMAs of item
+                // i + 2 done, which need the epilogue to have released tiles of item i.
+                if (FP8) mbar_arrive(&rs_full[i % kTcRowScaleSlots]);
+            } else if (!fuse) {
+                break;
+            }
+            if (fuse && i > 0) certify_item(i - 1);
         }
+        if (fuse && my_items > 0) certify_item(my_items - 1);
     } else {
         // ---- epilogue: warps 4..19. Thread = row (TMEM lane); warp w takes the
         // 64-column quarter (w - 4) / 4 of every tile, as four 16-column halves.
@@ -1141,15 +1260,29 @@ k_assign_tc(const T* __restrict__ x, const __grid_constant__ CUtensorMap map_hi,
                     // holds by construction (every value folded into s2 is at least
                     // the final best key); were it ever violated, raising s2 to s1
                     // leaves no margin, so the row goes to the refine pass.
-                    const size_t oo = ((size_t)split * p.m + row) * 2;
                     const float unit = NM ? 2.0f : 1.0f;  // NM: half-scores back to scores (exact)
-                    p.part_s[oo] = unit * s1;
-                    p.part_i[oo] = i1;
-                    p.part_s[oo + 1] = unit * fmaxf(s2, s1);
-                    p.part_i[oo + 1] = i1;
+                    if (NM && p.fuse) {
+                        // For the row loaders' certification, once they are done with
+                        // the previous item's (never after a wait that gave up).
+                        if (i == 0 || mbar_wait(fin_empty, (uint32_t)((i - 1) & 1), abort_flag, kTcCtlSleepNs)) {
+                            uint32_t* e = fin + r * 4;
+                            e[0] = __float_as_uint(unit * s1);
+                            e[1] = i1;
+                            e[2] = __float_as_uint(unit * fmaxf(s2, s1));
+                        }
+                    } else {
+                        const size_t oo = ((size_t)split * p.m + row) * 2;
+                        p.part_s[oo] = unit * s1;
+                        p.part_i[oo] = i1;
+                        p.part_s[oo + 1] = unit * fmaxf(s2, s1);
+                        p.part_i[oo + 1] = i1;
+                    }
                 }
                 pub[cq * kTcBM + r] = INFINITY;  // the next item starts afresh
                 asm volatile("bar.sync 1, %0;" ::"n"(kTcEpiWarps * 32) : "memory");
+                // The item's results are complete unless some role gave up (every failed
+                // wait raises the abort flag): hand them to the row loaders.
+                if (NM && p.fuse && warp == kTcEpi0 && lane == 0 && !*abort_flag) mbar_arrive(fin_full);
             }
         }
     }

@@ -551,8 +551,25 @@ EMB_DEV void revive_cta(int k, int d, float* __restrict__ c, float* __restrict__
             const int n = min(cap, k - c0);
             for (int i = tid; i < n; i += blockDim.x) stage[i] = usage[c0 + i];
             __syncthreads();
-            if (tid == 0)
-                for (int i = 0; i < n; i++) total = __fadd_rn(total, stage[i]);
+            if (tid == 0) {
+                // Eight values per 2 vector loads, issued ahead of their adds (the
+                // adds stay one chain in index order).
+                const float4* s4 = reinterpret_cast<const float4*>(stage);
+                int i = 0;
+#pragma unroll 4
+                for (; i + 8 <= n; i += 8) {
+                    const float4 a = s4[i >> 2], b = s4[(i >> 2) + 1];
+                    total = __fadd_rn(total, a.x);
+                    total = __fadd_rn(total, a.y);
+                    total = __fadd_rn(total, a.z);
+                    total = __fadd_rn(total, a.w);
+                    total = __fadd_rn(total, b.x);
+                    total = __fadd_rn(total, b.y);
+                    total = __fadd_rn(total, b.z);
+                    total = __fadd_rn(total, b.w);
+                }
+                for (; i < n; i++) total = __fadd_rn(total, stage[i]);
+            }
             __syncthreads();
         }
         if (tid == 0) thr_s = __fdiv_rn(__fmul_rn(total, tau), (float)k);

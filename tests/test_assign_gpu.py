@@ -353,17 +353,39 @@ def test_i8_mode_c3_like_exact(emb, orc, assigners):
     assert np.array_equal(lab, rl) and same_f32(dist, rd)
 
 
-@pytest.mark.parametrize("precision,bits", [("bf16x1", 0), ("bf16", 0), ("fp32", 8)])
+@pytest.mark.parametrize("n,k", [(94_720, 4096), (76_000, 300)])
+def test_certified_in_the_fast_kernel(emb, orc, assigners, n, k):
+    # Row tiles in whole waves of 148 SMs, so the search takes one column split
+    # (on a 148-SM B200): the single-term search certifies
+    # each row tile in its own row-loader warps (no separate certify kernel).
+    # Labels and distances must still be the reference's bit for bit, and the
+    # certified and refined counts must cover every row.
+    x = emb.datasets.embeddings(n, 128, latent=32, seed=17)
+    c = x[np.random.default_rng(18).choice(n, k, replace=False)] * np.float32(0.97)
+    a = assigners("bf16x1")
+    a.set_centroids(c)
+    lab, dist = a.assign(x)
+    st = a.stats()
+    rl, rd = orc.cpu_assign(x, c, emulate=not orc.has_kernel("avx512"))
+    assert np.array_equal(lab, rl) and same_f32(dist, rd)
+    assert st["rows_certified"] + st["rows_refined"] == n and st["rows_refined"] > 0, st
+    assert st["fast_aborted"] == 0, st
+
+
+@pytest.mark.parametrize("precision,bits,n", [("bf16x1", 0, 9_000), ("bf16", 0, 9_000), ("fp32", 8, 9_000),
+                                              ("bf16x1", 0, 75_776)])
 @pytest.mark.parametrize("stall_tile", [0, 2])
-def test_bounded_wait_abort_path(emb, orc, precision, bits, stall_tile):
+def test_bounded_wait_abort_path(emb, orc, precision, bits, n, stall_tile):
     # One epilogue warp of every CTA of the fast tensor-core kernel waits, at a
     # given centroid tile, on a barrier that nothing completes, with a 2 ms limit.
     # The wait runs out while copies and MMAs are in flight: the kernel drains
     # them, frees TMEM and flags the abort, and the call settles every row with
     # the exact search. Labels and distances must still be the oracle's, and the
-    # GPU must serve the next call normally.
+    # GPU must serve the next call normally. With 75,776 rows the search runs in
+    # one column split and certifies in its row-loader warps, which must list the
+    # rows of every unfinished row tile.
     rng = np.random.default_rng(40 + stall_tile)
-    n, k, d = 9_000, 2_000, 96
+    k, d = 2_000, 96
     a = emb.B200Assigner(0, precision=precision, centroid_bits=bits)
     if bits:
         x = rng.integers(-128, 128, (n, d), dtype=np.int8)
