@@ -343,7 +343,7 @@ def run_ours(args):
         "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                      "frac": achieved / peak, "peak_note": f"bf16 burst {peaks['source']} (kernel timed in a "
                                                            f"loop of {r['ms_total'] / 1e3:.2f} s)",
-                     "kernel": "k_assign_tc (fast contraction)",
+                     "kernel": "k_assign_tc (fast contraction; with one column split its row-loader warps also certify the rows)",
                      "algorithmic_flops_per_launch": flops_per_launch,
                      "executed_flops_per_launch": flops_per_launch * {"bf16": 3, "bf16x1": 1, "fp8": 1, "fp32": 1}[head],
                      "traffic": None if tpr is None else tpr * N_ROWS},
