@@ -372,6 +372,25 @@ def test_certified_in_the_fast_kernel(emb, orc, assigners, n, k):
     assert st["fast_aborted"] == 0, st
 
 
+def test_certified_in_the_fast_kernel_with_bias(emb, orc, assigners):
+    # The same one-split search with a per-centroid bias (norms and their bound
+    # include it), then reset by set_centroids.
+    n, k = 75_776, 2_000
+    x = emb.datasets.embeddings(n, 64, latent=16, seed=19)
+    c = x[np.random.default_rng(20).choice(n, k, replace=False)] * np.float32(0.97)
+    bias = np.random.default_rng(21).uniform(0, 0.05, k).astype(np.float32)
+    a = assigners("bf16x1")
+    a.set_centroids(c)
+    a.set_bias(bias)
+    lab, dist = a.assign(x)
+    rl, rd = orc.cpu_assign(x, c, bias=bias, emulate=not orc.has_kernel("avx512"))
+    assert np.array_equal(lab, rl) and same_f32(dist, rd)
+    a.set_centroids(c)
+    lab, dist = a.assign(x)
+    rl, rd = orc.cpu_assign(x, c, emulate=not orc.has_kernel("avx512"))
+    assert np.array_equal(lab, rl) and same_f32(dist, rd)
+
+
 @pytest.mark.parametrize("precision,bits,n", [("bf16x1", 0, 9_000), ("bf16", 0, 9_000), ("fp32", 8, 9_000),
                                               ("bf16x1", 0, 75_776)])
 @pytest.mark.parametrize("stall_tile", [0, 2])

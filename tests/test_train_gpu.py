@@ -60,6 +60,16 @@ def test_blob_mixture_bit_exact(emb, orc, precision):
     assert st["fast_aborted"] == 0
 
 
+def test_large_batches_single_term_bit_exact(emb, orc):
+    # Batches of 98,304 rows (whole waves of row tiles on 148 SMs, one centroid
+    # tile): the single-term search certifies each row tile inside its own kernel,
+    # also in the captured epochs. Training must still equal the oracle's.
+    x = emb.datasets.blobs(196_608, 32, n_blobs=300, seed=6)
+    out, ref, st = run_both(emb, orc, x, 200, "bf16x1", nepochs=2.0, batch_size=98_304)
+    check_same(out, ref)
+    assert st["fast_aborted"] == 0
+
+
 @pytest.mark.parametrize("d", [100, 36])
 def test_crowded_clusters_bit_exact(emb, orc, d):
     # Most rows in one tight blob: a batch puts hundreds of rows in a few clusters
