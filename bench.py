@@ -830,6 +830,10 @@ def run_c5(args):
     if args.proposer_training:
         p = emb.B200Assigner(0, precision="bf16x1")
         p.load_rows(x)
+        # Untimed first, as for the full-search run: the handle's allocations and
+        # the first captures of its kernels stay out of the timed training.
+        p.train_resident_proposed(k, emb.Config(nepochs=2.0), late_epochs=1, net_steps=args.late_net_steps,
+                                  groups=groups, top=32, mass=0.999)
         t0 = time.perf_counter()
         outp = p.train_resident_proposed(k, emb.Config(nepochs=5.0), late_epochs=args.late_epochs,
                                          net_steps=args.late_net_steps, groups=groups, top=32, mass=0.999)
